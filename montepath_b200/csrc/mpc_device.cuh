@@ -1,0 +1,312 @@
+// mpc_device.cuh -- device-side generators, inverse CDF and reductions of the
+// B200 Monte Carlo backend.  Everything here is evaluated in registers inside
+// the fused pricing kernels; no sample is materialised unless the request is
+// an FP64-plain one.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mpc_types.h"
+
+namespace mpc {
+
+// ----------------------------------------------------------- xorshift64* --
+// MonteCarloRng (crates/mc-core/src/runtime/cpu.rs:2955-3007) replayed on the
+// device.  The state transition x -> x^(x>>12), ^(x<<25), ^(x>>27) is linear
+// over GF(2), so T^k is a 64x64 bit matrix.  The host tabulates
+// T^(2^b) for b = 0..63 in nibble form: jump[b][q][v] = T^(2^b) applied to
+// the nibble value v placed at bit position 4q.  Jumping k draws ahead costs
+// popcount(k) * 16 table lookups.
+struct JumpTables {
+  const uint64_t* nibble;  // [64][16][16]
+};
+
+__device__ __forceinline__ uint64_t gf2_apply(const uint64_t* __restrict__ table, uint64_t x) {
+  uint64_t y = 0;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) y ^= __ldg(table + q * 16 + ((x >> (4 * q)) & 0xF));
+  return y;
+}
+
+__device__ __forceinline__ uint64_t xorshift_jump(const uint64_t* __restrict__ nibble, uint64_t state,
+                                                  uint64_t k) {
+  while (k) {
+    int b = __ffsll((long long)k) - 1;
+    state = gf2_apply(nibble + (size_t)b * 256, state);
+    k &= k - 1;
+  }
+  return state;
+}
+
+// Sequential MonteCarloRng positioned at an arbitrary normal index.
+struct XorshiftStream {
+  uint64_t state;
+  double cached;
+  bool has_cached;
+
+  __device__ __forceinline__ uint64_t next_u64() {
+    uint64_t x = state;
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    state = x;
+    return x * 0x2545F4914F6CDD1Dull;
+  }
+  __device__ __forceinline__ double next_open01() {
+    uint64_t raw = next_u64() >> 11;
+    double v = (double)raw * (1.0 / 9007199254740992.0);
+    return fmax(v, 2.2250738585072014e-308);
+  }
+  // Box-Muller in FP64 (cpu.rs:2992-3006): returns cos branch, caches sin branch.
+  __device__ __forceinline__ double normal_f64() {
+    if (has_cached) {
+      has_cached = false;
+      return cached;
+    }
+    double u1 = next_open01();
+    double u2 = next_open01();
+    double radius = sqrt(-2.0 * log(u1));
+    double s, c;
+    sincos(6.283185307179586 * u2, &s, &c);
+    cached = radius * s;
+    has_cached = true;
+    return radius * c;
+  }
+  // Same draw with the Box-Muller transform evaluated in FP32: the integer
+  // stream and the uniforms (rounded to f32) are the reference's.
+  __device__ __forceinline__ float normal_f32() {
+    if (has_cached) {
+      has_cached = false;
+      return (float)cached;
+    }
+    float u1 = (float)next_open01();
+    float u2 = (float)next_open01();
+    float radius = sqrtf(-2.0f * logf(u1));
+    float s, c;
+    sincospif(2.0f * u2, &s, &c);
+    cached = (double)(radius * s);
+    has_cached = true;
+    return radius * c;
+  }
+  // Position the stream of `seed` so that the next normal is normal number
+  // `normal_index` of the sequential stream.
+  __device__ __forceinline__ void seek(const uint64_t* __restrict__ nibble, uint64_t seed,
+                                       uint64_t normal_index, bool fp32) {
+    uint64_t s0 = seed == 0 ? 0x9E3779B97F4A7C15ull : seed;
+    uint64_t pair = normal_index >> 1;
+    state = xorshift_jump(nibble, s0, 2 * pair);
+    has_cached = false;
+    if (normal_index & 1) {
+      if (fp32)
+        (void)normal_f32();
+      else
+        (void)normal_f64();
+    }
+  }
+};
+
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  uint64_t z = x;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// derive_chunk_seed (cpu.rs:8922-8924)
+__host__ __device__ __forceinline__ uint64_t derive_chunk_seed(uint64_t base, uint64_t idx) {
+  return splitmix64(base + idx * 0x9E3779B97F4A7C15ull);
+}
+
+// The reference's CPU thread split (cpu.rs:6232-6276): `chunks` streams of
+// base or base+1 units, the first `rem` chunks one larger.  Maps a global
+// unit index to (chunk seed, index inside the chunk).
+__device__ __forceinline__ void chunk_of(const DevReq& q, uint64_t unit, uint64_t* seed, uint64_t* local) {
+  if (q.n_chunks <= 1) {
+    *seed = q.seed;
+    *local = unit;
+    return;
+  }
+  uint64_t big = q.chunk_rem * (q.chunk_base + 1);
+  uint64_t c;
+  if (unit < big) {
+    c = unit / (q.chunk_base + 1);
+    *local = unit - c * (q.chunk_base + 1);
+  } else {
+    c = q.chunk_rem + (unit - big) / q.chunk_base;
+    *local = unit - big - (c - q.chunk_rem) * q.chunk_base;
+  }
+  *seed = derive_chunk_seed(q.seed, c);
+}
+
+// --------------------------------------------------------- counter hash ---
+// hash_u32 / stateless_open01_f32 / stateless_standard_normal_f32
+// (cpu.rs:5626-5652, european_call_stepwise_v1.metal:6-28).
+__host__ __device__ __forceinline__ uint32_t hash_u32(uint32_t x) {
+  x += 0x9E3779B9u;
+  x ^= x >> 16;
+  x *= 0x85EBCA6Bu;
+  x ^= x >> 13;
+  x *= 0xC2B2AE35u;
+  return x ^ (x >> 16);
+}
+__host__ __device__ __forceinline__ uint32_t counter_mix(uint32_t seed, uint32_t path, uint32_t step,
+                                                         uint32_t lane) {
+  return seed ^ (path * 747796405u) ^ (step * 2891336453u) ^ (lane * 277803737u);
+}
+// f32((h + 1) / 4294967297.0): the quotient lies within one unit of 2^-32
+// below (h+1)/2^32, so the correctly rounded f64 quotient rounds to the same
+// f32 as (h+1)/2^32 rounded to nearest with ties toward zero.  Evaluated
+// exactly in integer arithmetic, no FP64 division.
+__device__ __forceinline__ float counter_open01(uint32_t h) {
+  if (h == 0xFFFFFFFFu) return 1.0f;
+  uint32_t m = h + 1u;
+  int bits = 32 - __clz(m);
+  if (bits <= 24) return (float)m * 2.3283064365386963e-10f;  // exact
+  int s = bits - 24;
+  uint32_t q = m >> s;
+  uint32_t rem = m & ((1u << s) - 1u);
+  uint32_t half = 1u << (s - 1);
+  if (rem > half) q += 1u;  // ties go down
+  return __uint2float_rn(q) * __int_as_float((127 + s - 32) << 23);
+}
+__device__ __forceinline__ float counter_normal_f32(uint32_t seed, uint32_t path, uint32_t step) {
+  float u1 = counter_open01(hash_u32(counter_mix(seed, path, step, 0u)));
+  float u2 = counter_open01(hash_u32(counter_mix(seed, path, step, 1u)));
+  float radius = sqrtf(-2.0f * logf(u1));
+  float theta = 2.0f * 3.14159265358979323846f * u2;
+  return radius * cosf(theta);
+}
+
+// ---------------------------------------------------------------- Sobol ---
+// Burley 2020 hash-based Owen scrambling (the algorithm of the `sobol_burley`
+// crate called at cpu.rs:5399-5431): Owen-shuffled index, Sobol matrix
+// product, Owen-scrambled output.  The matrix product uses per-dimension
+// nibble tables sob[dim][q][v] = XOR of V[dim][4q + j] over the bits j of v,
+// 8 lookups per sample instead of 32 conditional XORs.
+__host__ __device__ __forceinline__ uint32_t lk_permute(uint32_t x, uint32_t seed) {
+  x += seed;
+  x ^= x * 0x6c50b47cu;
+  x ^= x * 0xb82f1e52u;
+  x ^= x * 0xc7afe638u;
+  x ^= x * 0x8d22f6e6u;
+  return x;
+}
+__device__ __forceinline__ uint32_t nested_uniform_scramble(uint32_t x, uint32_t seed) {
+  return __brev(lk_permute(__brev(x), seed));
+}
+__host__ __device__ __forceinline__ uint32_t hash_combine(uint32_t seed, uint32_t v) {
+  return seed ^ (v + 0x9e3779b9u + (seed << 6) + (seed >> 2));
+}
+__device__ __forceinline__ uint32_t sobol_product(const uint32_t* __restrict__ table_dim, uint32_t index) {
+  // table_dim: 8 x 16 words for this dimension (bit 0 of the index = MSB direction)
+  uint32_t x = 0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) x ^= table_dim[q * 16 + ((index >> (4 * q)) & 0xFu)];
+  return x;
+}
+// Sobol sample of (point, normal_index) with the reference's block and
+// dimension-wrap seeding (ScrambledSobol::standard_normal, cpu.rs:5665-5677).
+__device__ __forceinline__ uint32_t sobol_point(const uint32_t* __restrict__ table, uint64_t point,
+                                                uint32_t normal_index, uint32_t seed32) {
+  uint32_t block = (uint32_t)(point >> 16);
+  uint32_t local = (uint32_t)(point & 0xFFFFu);
+  uint32_t dim = normal_index & (MPC_SOBOL_TABLE_DIMS - 1);
+  uint32_t seed = seed32 + (normal_index / MPC_SOBOL_TABLE_DIMS) + block * 0x9E3779B9u;
+  uint32_t shuffled = nested_uniform_scramble(local, seed);
+  uint32_t x = sobol_product(table + dim * 128, shuffled);
+  return nested_uniform_scramble(x, hash_combine(seed, dim));
+}
+// 23-bit midpoint uniform: exact in both precisions, never 0 or 1.
+__device__ __forceinline__ float sobol_unit_f32(uint32_t x) {
+  return ((float)(x >> 9) + 0.5f) * 1.1920928955078125e-07f;
+}
+__device__ __forceinline__ double sobol_unit_f64(uint32_t x) {
+  return ((double)(x >> 9) + 0.5) * 1.1920928955078125e-07;
+}
+
+// ------------------------------------------------------- Acklam inverse ---
+// inverse_standard_normal (cpu.rs:6012-6061): the reference rational in FP64,
+// and the same rational evaluated in FP32 for the fused path.
+__device__ __forceinline__ double icdf_f64(double p) {
+  const double a0 = -3.969683028665376e1, a1 = 2.209460984245205e2, a2 = -2.759285104469687e2,
+               a3 = 1.38357751867269e2, a4 = -3.066479806614716e1, a5 = 2.506628277459239;
+  const double b0 = -5.447609879822406e1, b1 = 1.615858368580409e2, b2 = -1.556989798598866e2,
+               b3 = 6.680131188771972e1, b4 = -1.328068155288572e1;
+  const double c0 = -7.784894002430293e-3, c1 = -3.223964580411365e-1, c2 = -2.400758277161838,
+               c3 = -2.549732539343734, c4 = 4.374664141464968, c5 = 2.938163982698783;
+  const double d0 = 7.784695709041462e-3, d1 = 3.224671290700398e-1, d2 = 2.445134137142996,
+               d3 = 3.754408661907416;
+  p = fmin(fmax(p, 2.2250738585072014e-308), 1.0 - 2.220446049250313e-16);
+  if (p < 0.02425) {
+    double q = sqrt(-2.0 * log(p));
+    return (((((c0 * q + c1) * q + c2) * q + c3) * q + c4) * q + c5) /
+           ((((d0 * q + d1) * q + d2) * q + d3) * q + 1.0);
+  }
+  if (p <= 1.0 - 0.02425) {
+    double q = p - 0.5;
+    double r = q * q;
+    return (((((a0 * r + a1) * r + a2) * r + a3) * r + a4) * r + a5) * q /
+           (((((b0 * r + b1) * r + b2) * r + b3) * r + b4) * r + 1.0);
+  }
+  double q = sqrt(-2.0 * log(1.0 - p));
+  return -(((((c0 * q + c1) * q + c2) * q + c3) * q + c4) * q + c5) /
+         ((((d0 * q + d1) * q + d2) * q + d3) * q + 1.0);
+}
+
+__device__ __forceinline__ float icdf_f32(float p) {
+  if (p >= 0.02425f && p <= 0.97575f) {
+    float q = p - 0.5f;
+    float r = q * q;
+    float num = (((((-3.969683028665376e1f * r + 2.209460984245205e2f) * r - 2.759285104469687e2f) * r +
+                   1.38357751867269e2f) * r - 3.066479806614716e1f) * r + 2.506628277459239f) * q;
+    float den = ((((-5.447609879822406e1f * r + 1.615858368580409e2f) * r - 1.556989798598866e2f) * r +
+                  6.680131188771972e1f) * r - 1.328068155288572e1f) * r + 1.0f;
+    return __fdividef(num, den);
+  }
+  float tail = p < 0.5f ? p : 1.0f - p;
+  float q = sqrtf(-2.0f * __logf(tail));
+  float num = ((((-7.784894002430293e-3f * q - 3.223964580411365e-1f) * q - 2.400758277161838f) * q -
+                2.549732539343734f) * q + 4.374664141464968f) * q + 2.938163982698783f;
+  float den = (((7.784695709041462e-3f * q + 3.224671290700398e-1f) * q + 2.445134137142996f) * q +
+               3.754408661907416f) * q + 1.0f;
+  float z = __fdividef(num, den);
+  return p < 0.5f ? z : -z;
+}
+
+// --------------------------------------------------------------- Halton ---
+// halton / halton_with_shift (cpu.rs:6063-6077), evaluated in FP64 exactly as
+// the reference (IEEE division and accumulation order).
+__device__ __forceinline__ double halton_shifted(uint64_t index, uint32_t base, double shift) {
+  double f = 1.0 / (double)base;
+  double value = 0.0;
+  while (index > 0) {
+    uint64_t next = index / base;
+    value += f * (double)(index - next * base);
+    index = next;
+    f /= (double)base;
+  }
+  value = fmax(value, 2.2250738585072014e-308);
+  double shifted = value + shift;
+  return shifted - floor(shifted);
+}
+
+__device__ __forceinline__ double open01_from_u64(uint64_t v) {
+  return fmax((double)(v >> 11) * (1.0 / 9007199254740992.0), 2.2250738585072014e-308);
+}
+// LatinHypercube::standard_normal's uniform (cpu.rs:5764-5780).
+__device__ __forceinline__ double lhs_uniform(const LhsDim& d, uint64_t point, uint64_t n_paths) {
+  uint64_t stratum = (d.multiplier * point + d.offset) % n_paths;
+  double jitter = open01_from_u64(splitmix64(d.jitter_seed ^ (point * 0xBF58476D1CE4E5B9ull)));
+  double u = ((double)stratum + jitter) / (double)n_paths;
+  return fmin(fmax(u, 2.2250738585072014e-308), 1.0 - 2.220446049250313e-16);
+}
+
+// ------------------------------------------------------------- reductions -
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  return v;
+}
+
+}  // namespace mpc

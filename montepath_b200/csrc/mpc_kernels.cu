@@ -1,0 +1,1302 @@
+// mpc_kernels.cu -- sm_100a kernels of the B200 Monte Carlo pricing backend.
+//
+// Fused path (FP32 path arithmetic, FP64 accumulation): samples are generated
+// in registers, stepped through the model, turned into a payoff and reduced
+// warp -> block -> tile partial; the block that completes a request's last
+// tile sums the tile partials in tile order (deterministic, independent of
+// which requests share the launch).  One persistent kernel walks a tile work
+// list, so a single request, a heterogeneous book and a serving wave all use
+// the same launch.
+//
+// Plain path (FP64, one request per launch sequence): samples materialised
+// in HBM, a stepping kernel writing per-path payoffs (the contract of the
+// reference's mc_cuda_european_call_stepwise_v1), and a reduction kernel.
+//
+// Longstaff-Schwartz: one cooperative launch.  Paths are written date-major,
+// each date's ITM basis moments are reduced block -> grid (FP64), every block
+// solves the 4x4 normal equations redundantly after a bounded grid barrier,
+// and exercise decisions are applied in registers.
+
+#include <atomic>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mpc_device.cuh"
+#include "mpc_launch.h"
+#include "mpc_types.h"
+
+namespace mpc {
+
+static std::atomic<uint64_t> g_launches{0};
+uint64_t kernel_launch_count() { return g_launches.load(); }
+static inline void count_launch() { g_launches.fetch_add(1); }
+
+enum Workload : int32_t {
+  W_EURO = 0,
+  W_ASIAN = 1,
+  W_DAO = 2,
+  W_UAO = 3,
+  W_LOOKBACK = 4,
+};
+
+struct SrcCtx {
+  const uint32_t* sobol;
+  const uint64_t* jump;
+};
+
+// ------------------------------------------------------------- sources ----
+// A Source yields the samples of one unit (path or antithetic pair) by
+// dimension index.  n32/n64: standard normal in FP32 / FP64; u64: the raw
+// uniform (Merton's Poisson dimension).
+template <int S>
+struct Source;
+
+template <>
+struct Source<SMP_COUNTER> {
+  uint32_t seed, unit;
+  template <bool FP64>
+  __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx&, uint64_t u) {
+    seed = q.seed32;
+    unit = (uint32_t)u;
+  }
+  __device__ __forceinline__ float n32(uint32_t d) { return counter_normal_f32(seed, unit, d); }
+  __device__ __forceinline__ double n64(uint32_t d) { return (double)counter_normal_f32(seed, unit, d); }
+  __device__ __forceinline__ double u64(uint32_t d) {
+    return (double)counter_open01(hash_u32(counter_mix(seed, unit, d, 0u)));
+  }
+};
+
+template <>
+struct Source<SMP_SOBOL> {
+  const uint32_t* table;
+  uint64_t point;
+  uint32_t seed;
+  template <bool FP64>
+  __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
+    table = c.sobol;
+    point = u;
+    seed = q.seed32;
+  }
+  __device__ __forceinline__ float n32(uint32_t d) { return icdf_f32(sobol_unit_f32(sobol_point(table, point, d, seed))); }
+  __device__ __forceinline__ double n64(uint32_t d) {
+    return icdf_f64(sobol_unit_f64(sobol_point(table, point, d, seed)));
+  }
+  __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sobol_point(table, point, d, seed)); }
+};
+
+template <>
+struct Source<SMP_HALTON> {
+  uint64_t index;
+  const uint32_t* primes;
+  const double* shifts;
+  template <bool FP64>
+  __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx&, uint64_t u) {
+    index = u + 1;
+    primes = q.halton_primes;
+    shifts = q.halton_shifts;
+  }
+  __device__ __forceinline__ double u64(uint32_t d) { return halton_shifted(index, __ldg(primes + d), __ldg(shifts + d)); }
+  __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
+  __device__ __forceinline__ float n32(uint32_t d) {
+    float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
+    return icdf_f32(u);
+  }
+};
+
+template <>
+struct Source<SMP_LHS> {
+  uint64_t point, n_paths;
+  const LhsDim* dims;
+  template <bool FP64>
+  __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx&, uint64_t u) {
+    point = u;
+    n_paths = q.n_paths;
+    dims = q.lhs;
+  }
+  __device__ __forceinline__ double u64(uint32_t d) {
+    LhsDim ld;
+    ld.multiplier = __ldg(&dims[d].multiplier);
+    ld.offset = __ldg(&dims[d].offset);
+    ld.jitter_seed = __ldg(&dims[d].jitter_seed);
+    return lhs_uniform(ld, point, n_paths);
+  }
+  __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
+  __device__ __forceinline__ float n32(uint32_t d) {
+    float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
+    return icdf_f32(u);
+  }
+};
+
+template <>
+struct Source<SMP_XORSHIFT> {
+  XorshiftStream st;
+  template <bool FP64>
+  __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
+    uint64_t seed, local;
+    chunk_of(q, u, &seed, &local);
+    st.seek(c.jump, seed, local * q.normals_per_unit, !FP64);
+  }
+  // Sequential stream: dimensions must be requested in increasing order.
+  __device__ __forceinline__ float n32(uint32_t) { return st.normal_f32(); }
+  __device__ __forceinline__ double n64(uint32_t) { return st.normal_f64(); }
+  __device__ __forceinline__ double u64(uint32_t) { return st.next_open01(); }
+};
+
+// Reads materialised samples [dim][unit] (FP64 plain path).
+struct BufSource {
+  const double* buf;
+  uint64_t n_units, unit;
+  __device__ __forceinline__ double n64(uint32_t d) { return buf[(uint64_t)d * n_units + unit]; }
+  __device__ __forceinline__ double u64(uint32_t d) { return buf[(uint64_t)d * n_units + unit]; }
+  __device__ __forceinline__ float n32(uint32_t d) { return (float)n64(d); }
+};
+
+template <class Real, class Src>
+__device__ __forceinline__ Real normal(Src& s, uint32_t d) {
+  if constexpr (sizeof(Real) == 4)
+    return s.n32(d);
+  else
+    return s.n64(d);
+}
+
+template <class Real>
+__device__ __forceinline__ Real ex(Real x) {
+  if constexpr (sizeof(Real) == 4)
+    return __expf(x);
+  else
+    return exp(x);
+}
+template <class Real>
+__device__ __forceinline__ Real sq_root(Real x) {
+  if constexpr (sizeof(Real) == 4)
+    return sqrtf(x);
+  else
+    return sqrt(x);
+}
+
+// sample_poisson by inversion with the uniform supplied (cpu.rs:932-953).
+__device__ __forceinline__ uint32_t poisson_inverse(double u, double mean) {
+  if (mean == 0.0) return 0;
+  double prob = exp(-mean), cum = prob;
+  uint32_t k = 0;
+  while (u > cum && k < 4095u) {
+    ++k;
+    prob *= mean / (double)k;
+    cum += prob;
+  }
+  return k;
+}
+
+// ------------------------------------------------------------- models -----
+// GBM stepwise with the payoff observer of workload W (cpu.rs:6443-6591,
+// 7973-8009, 8324-8354; up-and-out mirrors down-and-out).  FP32 compares the
+// barrier in log space; FP64 compares exp(log S) with the barrier as the
+// reference does.
+template <class Real, int W, class Src>
+__device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double& pay, double& ctl) {
+  const Real drift = (Real)q.drift_dt, vol = (Real)q.vol_dt, kk = (Real)q.k, disc = (Real)q.discount;
+  const Real lbar = (Real)q.log_barrier, bar = (Real)q.barrier;
+  const bool anti = q.anti != 0;
+  Real ls0 = (Real)q.log_s0, ls1 = ls0;
+  Real acc0 = (W == W_LOOKBACK) ? (Real)q.s0 : (Real)0, acc1 = acc0;
+  bool ko0 = (W == W_DAO && q.s0 <= q.barrier) || (W == W_UAO && q.s0 >= q.barrier), ko1 = ko0;
+  const uint32_t n = q.n_steps;
+  for (uint32_t s = 0; s < n; ++s) {
+    const Real z = normal<Real>(src, s);
+    ls0 += drift + vol * z;
+    if (anti) ls1 += drift - vol * z;
+    if constexpr (W == W_ASIAN) {
+      acc0 += ex<Real>(ls0);
+      if (anti) acc1 += ex<Real>(ls1);
+    } else if constexpr (W == W_LOOKBACK) {
+      acc0 = acc0 > ex<Real>(ls0) ? acc0 : ex<Real>(ls0);
+      if (anti) acc1 = acc1 > ex<Real>(ls1) ? acc1 : ex<Real>(ls1);
+    } else if constexpr (W == W_DAO) {
+      if constexpr (sizeof(Real) == 4) {
+        ko0 |= ls0 <= lbar;
+        if (anti) ko1 |= ls1 <= lbar;
+      } else {
+        ko0 |= ex<Real>(ls0) <= bar;
+        if (anti) ko1 |= ex<Real>(ls1) <= bar;
+      }
+    } else if constexpr (W == W_UAO) {
+      if constexpr (sizeof(Real) == 4) {
+        ko0 |= ls0 >= lbar;
+        if (anti) ko1 |= ls1 >= lbar;
+      } else {
+        ko0 |= ex<Real>(ls0) >= bar;
+        if (anti) ko1 |= ex<Real>(ls1) >= bar;
+      }
+    }
+  }
+  auto payoff = [&](Real ls, Real acc, bool ko) -> Real {
+    Real v;
+    if constexpr (W == W_ASIAN) {
+      if constexpr (sizeof(Real) == 4)
+        v = acc * (Real)(1.0 / (double)n) - kk;
+      else
+        v = acc / (Real)n - kk;
+    } else if constexpr (W == W_LOOKBACK) {
+      v = acc - kk;
+    } else {
+      v = ex<Real>(ls) - kk;
+      if (ko) v = 0;
+    }
+    return (v > (Real)0 ? v : (Real)0) * disc;
+  };
+  Real p0 = payoff(ls0, acc0, ko0);
+  if (anti) {
+    Real p1 = payoff(ls1, acc1, ko1);
+    pay = 0.5 * ((double)p0 + (double)p1);
+  } else {
+    pay = (double)p0;
+  }
+  ctl = (double)(disc * ex<Real>(ls0));
+}
+
+// GBM terminal European (european_call_payoff_from_shock, cpu.rs:7773-7783).
+template <class Real, class Src>
+__device__ __forceinline__ void unit_gbm_terminal(const DevReq& q, Src& src, double& pay, double& ctl) {
+  const Real z = normal<Real>(src, 0);
+  const Real s0 = (Real)q.s0, drift = (Real)q.drift_dt, vol = (Real)q.vol_dt, kk = (Real)q.k,
+             disc = (Real)q.discount;
+  Real st = s0 * ex<Real>(drift + vol * z);
+  Real p = (st - kk > (Real)0 ? st - kk : (Real)0) * disc;
+  if (q.anti) {
+    Real sb = s0 * ex<Real>(drift + vol * (-z));
+    Real pb = (sb - kk > (Real)0 ? sb - kk : (Real)0) * disc;
+    pay = 0.5 * ((double)p + (double)pb);
+  } else {
+    pay = (double)p;
+  }
+  ctl = (double)(disc * st);
+}
+
+// Heston Euler with the variance floored after every step (heston_path_terminal, cpu.rs:8667-8686).
+template <class Real, class Src>
+__device__ __forceinline__ void unit_heston(const DevReq& q, Src& src, double& pay, double& ctl) {
+  const Real kappa = (Real)q.kappa, theta = (Real)q.theta, xi = (Real)q.xi, rho = (Real)q.rho,
+             rho_perp = (Real)q.rho_perp, dt = (Real)q.dt, sqdt = (Real)q.sqrt_dt, rate = (Real)q.rate;
+  const bool anti = q.anti != 0;
+  Real ls0 = (Real)q.log_s0, ls1 = ls0, v0 = (Real)q.v0, v1 = v0;
+  const uint32_t n = q.n_steps;
+  for (uint32_t s = 0; s < n; ++s) {
+    const Real zv = normal<Real>(src, 2 * s);
+    const Real zi = normal<Real>(src, 2 * s + 1);
+    {
+      Real vp = v0 > (Real)0 ? v0 : (Real)0;
+      Real sv = sq_root<Real>(vp);
+      Real zp = rho * zv + rho_perp * zi;
+      ls0 += (rate - (Real)0.5 * vp) * dt + sv * sqdt * zp;
+      v0 = v0 + kappa * (theta - vp) * dt + xi * sv * sqdt * zv;
+      v0 = v0 > (Real)0 ? v0 : (Real)0;
+    }
+    if (anti) {
+      Real vp = v1 > (Real)0 ? v1 : (Real)0;
+      Real sv = sq_root<Real>(vp);
+      Real zp = rho * (-zv) + rho_perp * (-zi);
+      ls1 += (rate - (Real)0.5 * vp) * dt + sv * sqdt * zp;
+      v1 = v1 + kappa * (theta - vp) * dt + xi * sv * sqdt * (-zv);
+      v1 = v1 > (Real)0 ? v1 : (Real)0;
+    }
+  }
+  const Real kk = (Real)q.k, disc = (Real)q.discount;
+  Real st = ex<Real>(ls0);
+  Real p = (st - kk > (Real)0 ? st - kk : (Real)0) * disc;
+  if (anti) {
+    Real sb = ex<Real>(ls1);
+    Real pb = (sb - kk > (Real)0 ? sb - kk : (Real)0) * disc;
+    pay = 0.5 * ((double)p + (double)pb);
+  } else {
+    pay = (double)p;
+  }
+  ctl = (double)(st * disc);
+}
+
+// Merton: stepwise extension (z, u, z_J per step) and the reference terminal
+// form (cpu.rs:6408-6441) with dims (z, u, z_J).
+template <class Real, bool STEP, class Src>
+__device__ __forceinline__ void unit_merton(const DevReq& q, Src& src, double& pay, double& ctl) {
+  const Real drift = (Real)q.drift_dt, vol = (Real)q.vol_dt, jm = (Real)q.jump_mean, jv = (Real)q.jump_vol;
+  const double lam = q.lam_dt;
+  Real ls = (Real)q.log_s0;
+  const uint32_t n = STEP ? q.n_steps : 1;
+  for (uint32_t s = 0; s < n; ++s) {
+    const Real z = normal<Real>(src, 3 * s);
+    const uint32_t jumps = poisson_inverse(src.u64(3 * s + 1), lam);
+    ls += drift + vol * z;
+    if (jumps > 0) {
+      const Real zj = normal<Real>(src, 3 * s + 2);
+      ls += (Real)jumps * jm + jv * sq_root<Real>((Real)jumps) * zj;
+    }
+  }
+  const Real kk = (Real)q.k, disc = (Real)q.discount;
+  Real st = ex<Real>(ls);
+  pay = (double)((st - kk > (Real)0 ? st - kk : (Real)0) * disc);
+  ctl = (double)(st * disc);
+}
+
+// d-asset basket, terminal or stepwise (basket_terminal_payoff, cpu.rs:7616-7635).
+template <class Real, class Src>
+__device__ __forceinline__ void unit_basket(const DevReq& q, Src& src, double& pay, double& ctl) {
+  const uint32_t d = q.n_assets, n = q.n_steps;
+  const bool anti = q.anti != 0;
+  Real x0[8], x1[8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) x0[a] = x1[a] = (Real)0;
+  uint32_t dim = 0;
+  for (uint32_t s = 0; s < n; ++s) {
+    Real z[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+      if (a < (int)d) z[a] = normal<Real>(src, dim++);
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      if (a >= (int)d) break;
+      Real zc = (Real)0;
+#pragma unroll
+      for (int b = 0; b < 8; ++b)
+        if (b <= a) zc += (Real)q.chol[a * d + b] * z[b];
+      const Real dr = (Real)q.b_drift[a], vo = (Real)q.b_vol[a];
+      x0[a] += dr + vo * zc;
+      if (anti) x1[a] += dr + vo * (-zc);
+    }
+  }
+  Real b0 = 0, b1 = 0;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    if (a >= (int)d) break;
+    b0 += (Real)q.weights[a] * ((Real)q.spots[a] * ex<Real>(x0[a]));
+    if (anti) b1 += (Real)q.weights[a] * ((Real)q.spots[a] * ex<Real>(x1[a]));
+  }
+  const Real kk = (Real)q.k, disc = (Real)q.discount;
+  Real p = (b0 - kk > (Real)0 ? b0 - kk : (Real)0) * disc;
+  if (anti) {
+    Real pb = (b1 - kk > (Real)0 ? b1 - kk : (Real)0) * disc;
+    pay = 0.5 * ((double)p + (double)pb);
+  } else {
+    pay = (double)p;
+  }
+  ctl = (double)(b0 * disc);
+}
+
+// Coupled MLMC level of the arithmetic Asian (cpu.rs:6641-6894): level 0 is
+// the plain Asian with the base steps; level l couples M fine normals per
+// coarse step with a coarse path driven by sum(z)/sqrt(M).
+template <class Real, class Src>
+__device__ __forceinline__ void unit_mlmc(const DevReq& q, Src& src, double& pay, double& ctl) {
+  const Real kk = (Real)q.k, disc = (Real)q.discount;
+  ctl = 0.0;
+  if (q.level == 0) {
+    const Real drift = (Real)q.f_drift, vol = (Real)q.f_vol;
+    Real ls = (Real)q.log_s0, acc = 0;
+    for (uint32_t s = 0; s < q.n_steps; ++s) {
+      ls += drift + vol * normal<Real>(src, s);
+      acc += ex<Real>(ls);
+    }
+    Real avg;
+    if constexpr (sizeof(Real) == 4)
+      avg = acc * (Real)q.inv_fine;
+    else
+      avg = acc / (Real)q.n_steps;
+    pay = (double)((avg - kk > (Real)0 ? avg - kk : (Real)0) * disc);
+    return;
+  }
+  const Real fd = (Real)q.f_drift, fv = (Real)q.f_vol, cd = (Real)q.c_drift, cv = (Real)q.c_vol;
+  const uint32_t M = q.refinement;
+  Real fl = (Real)q.log_s0, cl = fl, fs = 0, cs = 0;
+  uint32_t j = 0;
+  for (uint64_t c = 0; c < q.coarse_steps; ++c) {
+    Real zsum = 0;
+    for (uint32_t m = 0; m < M; ++m) {
+      const Real z = normal<Real>(src, j++);
+      zsum += z;
+      fl += fd + fv * z;
+      fs += ex<Real>(fl);
+    }
+    Real zc;
+    if constexpr (sizeof(Real) == 4)
+      zc = zsum * (Real)q.inv_sqrt_m;
+    else
+      zc = zsum / sqrt((double)M);
+    cl += cd + cv * zc;
+    cs += ex<Real>(cl);
+  }
+  Real fa, ca;
+  if constexpr (sizeof(Real) == 4) {
+    fa = fs * (Real)q.inv_fine;
+    ca = cs * (Real)q.inv_coarse;
+  } else {
+    fa = fs / (Real)q.n_steps;
+    ca = cs / (Real)q.coarse_steps;
+  }
+  Real pf = (fa - kk > (Real)0 ? fa - kk : (Real)0) * disc;
+  Real pc = (ca - kk > (Real)0 ? ca - kk : (Real)0) * disc;
+  pay = (double)pf - (double)pc;
+}
+
+template <class Real, int FAM, class Src>
+__device__ __forceinline__ void run_family(const DevReq& q, Src& src, double& p, double& c) {
+  if constexpr (FAM == FAM_GBM_STEP) {
+    switch (q.workload) {
+      case W_ASIAN:
+        unit_gbm_step<Real, W_ASIAN>(q, src, p, c);
+        break;
+      case W_DAO:
+        unit_gbm_step<Real, W_DAO>(q, src, p, c);
+        break;
+      case W_UAO:
+        unit_gbm_step<Real, W_UAO>(q, src, p, c);
+        break;
+      case W_LOOKBACK:
+        unit_gbm_step<Real, W_LOOKBACK>(q, src, p, c);
+        break;
+      default:
+        unit_gbm_step<Real, W_EURO>(q, src, p, c);
+        break;
+    }
+  } else if constexpr (FAM == FAM_GBM_TERMINAL) {
+    unit_gbm_terminal<Real>(q, src, p, c);
+  } else if constexpr (FAM == FAM_HESTON) {
+    unit_heston<Real>(q, src, p, c);
+  } else if constexpr (FAM == FAM_MERTON_STEP) {
+    unit_merton<Real, true>(q, src, p, c);
+  } else if constexpr (FAM == FAM_MERTON_TERMINAL) {
+    unit_merton<Real, false>(q, src, p, c);
+  } else if constexpr (FAM == FAM_BASKET) {
+    unit_basket<Real>(q, src, p, c);
+  } else {
+    unit_mlmc<Real>(q, src, p, c);
+  }
+}
+
+template <int FAM, int SMP>
+__device__ __forceinline__ void fused_unit(const DevReq& q, const SrcCtx& ctx, uint64_t u, double& p, double& c) {
+  Source<SMP> src;
+  src.template begin<false>(q, ctx, u);
+  run_family<float, FAM>(q, src, p, c);
+}
+
+template <int SMP>
+__device__ __forceinline__ void fused_unit_any(const DevReq& q, const SrcCtx& ctx, uint64_t u, double& p,
+                                               double& c) {
+  switch (q.family) {
+    case FAM_GBM_STEP:
+      fused_unit<FAM_GBM_STEP, SMP>(q, ctx, u, p, c);
+      break;
+    case FAM_GBM_TERMINAL:
+      fused_unit<FAM_GBM_TERMINAL, SMP>(q, ctx, u, p, c);
+      break;
+    case FAM_HESTON:
+      fused_unit<FAM_HESTON, SMP>(q, ctx, u, p, c);
+      break;
+    case FAM_BASKET:
+      fused_unit<FAM_BASKET, SMP>(q, ctx, u, p, c);
+      break;
+    case FAM_MLMC_LEVEL:
+      fused_unit<FAM_MLMC_LEVEL, SMP>(q, ctx, u, p, c);
+      break;
+    default:
+      if constexpr (SMP != SMP_XORSHIFT) {
+        if (q.family == FAM_MERTON_STEP)
+          fused_unit<FAM_MERTON_STEP, SMP>(q, ctx, u, p, c);
+        else
+          fused_unit<FAM_MERTON_TERMINAL, SMP>(q, ctx, u, p, c);
+      } else {
+        p = c = 0.0;
+      }
+      break;
+  }
+}
+
+// ----------------------------------------------------- block reduction ----
+constexpr int kFusedBlock = 256;
+constexpr int kWarps = kFusedBlock / 32;
+
+// Reduces v[0..4] over the block in a fixed order; result valid in thread 0.
+// The leading barrier keeps a previous call's reader of `red` safe, so calls
+// may follow each other directly.
+__device__ __forceinline__ void block_reduce5(double v[5], double (*red)[5]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) v[i] = warp_sum(v[i]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) red[warp][i] = v[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int warps = (blockDim.x + 31) >> 5;
+    for (int i = 0; i < 5; ++i) {
+      double s = 0.0;
+      for (int w = 0; w < warps; ++w) s += red[w][i];
+      v[i] = s;
+    }
+  }
+}
+
+// Sums the request's tile partials in tile order (strided per thread, then a
+// fixed block tree) into q.moments.  Called by the block that finished the
+// request's last tile.
+__device__ void finalize_request(DevReq& q, double (*red)[5]) {
+  double acc[5] = {0, 0, 0, 0, 0};
+  double cnt = 0.0;
+  for (uint32_t t = threadIdx.x; t < q.n_tiles; t += blockDim.x) {
+    const double* pt = q.partials + (size_t)t * MPC_MOMENTS;
+    cnt += __ldcg(pt + 0);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) acc[i] += __ldcg(pt + 1 + i);
+  }
+  double v[5] = {acc[0], acc[1], acc[2], acc[3], acc[4]};
+  block_reduce5(v, red);
+  double c6[5] = {cnt, 0, 0, 0, 0};
+  block_reduce5(c6, red);
+  if (threadIdx.x == 0) {
+    q.moments[0] = c6[0];
+    for (int i = 0; i < 5; ++i) q.moments[1 + i] = v[i];
+    q.moments[6] = 0.0;
+    q.moments[7] = 0.0;
+    *q.tiles_done = 0u;  // reusable without a memset
+  }
+}
+
+// --------------------------------------------------------- fused kernel ---
+// FAM >= 0: every request in the list has that family; FAM < 0: switch per tile.
+template <int FAM, int SMP>
+__global__ void __launch_bounds__(kFusedBlock) fused_kernel(const DevReq* __restrict__ reqs,
+                                                            const Tile* __restrict__ tiles, uint32_t n_tiles,
+                                                            uint32_t* __restrict__ counter, SrcCtx ctx) {
+  __shared__ DevReq sq;
+  __shared__ double red[kWarps][5];
+  __shared__ uint32_t s_tile;
+  __shared__ int s_last;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= n_tiles) break;
+    const Tile tl = tiles[t];
+    {  // stage the request descriptor in shared memory
+      const uint4* src = reinterpret_cast<const uint4*>(reqs + tl.req);
+      uint4* dst = reinterpret_cast<uint4*>(&sq);
+      for (uint32_t i = threadIdx.x; i < sizeof(DevReq) / sizeof(uint4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const uint64_t first = (uint64_t)tl.tile * sq.tile_units;
+    const uint64_t last = min(first + (uint64_t)sq.tile_units, sq.n_units);
+    double v[5] = {0, 0, 0, 0, 0};
+    const bool cv = sq.cv != 0;
+    double* per_unit = sq.per_unit;
+    for (uint64_t u = first + threadIdx.x; u < last; u += blockDim.x) {
+      double p, c;
+      if constexpr (FAM >= 0)
+        fused_unit<FAM, SMP>(sq, ctx, u, p, c);
+      else
+        fused_unit_any<SMP>(sq, ctx, u, p, c);
+      v[0] += p;
+      v[1] += p * p;
+      if (cv) {
+        v[2] += c;
+        v[3] += c * c;
+        v[4] += p * c;
+      }
+      if (per_unit) per_unit[u] = p;
+    }
+    block_reduce5(v, red);
+    if (threadIdx.x == 0) {
+      double* pt = sq.partials + (size_t)tl.tile * MPC_MOMENTS;
+      pt[0] = (double)(last - first);
+      for (int i = 0; i < 5; ++i) pt[1 + i] = v[i];
+      __threadfence();
+      s_last = (atomicAdd(sq.tiles_done, 1u) == sq.n_tiles - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      finalize_request(sq, red);
+    }
+    __syncthreads();
+  }
+}
+
+template <int FAM, int SMP>
+static cudaError_t launch_fused_t(const DevReq* reqs, const Tile* tiles, uint32_t n_tiles, uint32_t* counter,
+                                  const SrcCtx& ctx, int grid, int block, cudaStream_t stream) {
+  fused_kernel<FAM, SMP><<<grid, block, 0, stream>>>(reqs, tiles, n_tiles, counter, ctx);
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <int SMP>
+static cudaError_t launch_fused_s(int family, const DevReq* reqs, const Tile* tiles, uint32_t n_tiles,
+                                  uint32_t* counter, const SrcCtx& ctx, int grid, int block, cudaStream_t stream) {
+  switch (family) {
+    case FAM_GBM_STEP:
+      return launch_fused_t<FAM_GBM_STEP, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+    case FAM_GBM_TERMINAL:
+      return launch_fused_t<FAM_GBM_TERMINAL, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+    case FAM_HESTON:
+      return launch_fused_t<FAM_HESTON, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+    case FAM_BASKET:
+      return launch_fused_t<FAM_BASKET, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+    case FAM_MLMC_LEVEL:
+      return launch_fused_t<FAM_MLMC_LEVEL, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+    case FAM_MERTON_STEP:
+      if constexpr (SMP != SMP_XORSHIFT)
+        return launch_fused_t<FAM_MERTON_STEP, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+      return cudaErrorInvalidValue;
+    case FAM_MERTON_TERMINAL:
+      if constexpr (SMP != SMP_XORSHIFT)
+        return launch_fused_t<FAM_MERTON_TERMINAL, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+      return cudaErrorInvalidValue;
+    default:
+      return launch_fused_t<-1, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+  }
+}
+
+cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_tiles, uint32_t* d_tile_counter,
+                         int family, int sampler, const DeviceTables& tabs, int grid, int block,
+                         cudaStream_t stream) {
+  SrcCtx ctx{tabs.sobol, tabs.jump};
+  if (block != kFusedBlock) return cudaErrorInvalidValue;
+  switch (sampler) {
+    case SMP_XORSHIFT:
+      return launch_fused_s<SMP_XORSHIFT>(family, d_reqs, d_tiles, n_tiles, d_tile_counter, ctx, grid, block, stream);
+    case SMP_HALTON:
+      return launch_fused_s<SMP_HALTON>(family, d_reqs, d_tiles, n_tiles, d_tile_counter, ctx, grid, block, stream);
+    case SMP_LHS:
+      return launch_fused_s<SMP_LHS>(family, d_reqs, d_tiles, n_tiles, d_tile_counter, ctx, grid, block, stream);
+    case SMP_SOBOL:
+      return launch_fused_s<SMP_SOBOL>(family, d_reqs, d_tiles, n_tiles, d_tile_counter, ctx, grid, block, stream);
+    case SMP_COUNTER:
+      return launch_fused_s<SMP_COUNTER>(family, d_reqs, d_tiles, n_tiles, d_tile_counter, ctx, grid, block, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <int FAM, int SMP>
+static int occ_t(int block) {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fused_kernel<FAM, SMP>, block, 0);
+  return n;
+}
+template <int SMP>
+static int occ_s(int family, int block) {
+  switch (family) {
+    case FAM_GBM_STEP:
+      return occ_t<FAM_GBM_STEP, SMP>(block);
+    case FAM_GBM_TERMINAL:
+      return occ_t<FAM_GBM_TERMINAL, SMP>(block);
+    case FAM_HESTON:
+      return occ_t<FAM_HESTON, SMP>(block);
+    case FAM_BASKET:
+      return occ_t<FAM_BASKET, SMP>(block);
+    case FAM_MLMC_LEVEL:
+      return occ_t<FAM_MLMC_LEVEL, SMP>(block);
+    case FAM_MERTON_STEP:
+      if constexpr (SMP != SMP_XORSHIFT) return occ_t<FAM_MERTON_STEP, SMP>(block);
+      return 1;
+    case FAM_MERTON_TERMINAL:
+      if constexpr (SMP != SMP_XORSHIFT) return occ_t<FAM_MERTON_TERMINAL, SMP>(block);
+      return 1;
+    default:
+      return occ_t<-1, SMP>(block);
+  }
+}
+int fused_max_blocks_per_sm(int family, int sampler, int block) {
+  switch (sampler) {
+    case SMP_XORSHIFT:
+      return occ_s<SMP_XORSHIFT>(family, block);
+    case SMP_HALTON:
+      return occ_s<SMP_HALTON>(family, block);
+    case SMP_LHS:
+      return occ_s<SMP_LHS>(family, block);
+    case SMP_SOBOL:
+      return occ_s<SMP_SOBOL>(family, block);
+    default:
+      return occ_s<SMP_COUNTER>(family, block);
+  }
+}
+
+// ------------------------------------------------------ FP64 plain path ---
+__device__ __forceinline__ bool is_uniform_dim(const DevReq& q, uint32_t d) {
+  return (q.family == FAM_MERTON_STEP || q.family == FAM_MERTON_TERMINAL) && (d % 3u) == 1u;
+}
+
+template <int SMP>
+__global__ void __launch_bounds__(256) plain_generate_kernel(DevReq q, double* __restrict__ buf, SrcCtx ctx) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint32_t dims = (uint32_t)q.normals_per_unit;
+  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < q.n_units; u += stride) {
+    Source<SMP> src;
+    src.template begin<true>(q, ctx, u);
+    for (uint32_t d = 0; d < dims; ++d) buf[(uint64_t)d * q.n_units + u] = is_uniform_dim(q, d) ? src.u64(d) : src.n64(d);
+  }
+}
+
+cudaError_t launch_plain_generate(const DevReq& q, double* d_buf, int sampler, const DeviceTables& tabs,
+                                  cudaStream_t stream) {
+  SrcCtx ctx{tabs.sobol, tabs.jump};
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  uint64_t want = (q.n_units + 255) / 256;
+  int grid = (int)(want < (uint64_t)sms * 8 ? want : (uint64_t)sms * 8);
+  if (grid < 1) grid = 1;
+  switch (sampler) {
+    case SMP_XORSHIFT:
+      plain_generate_kernel<SMP_XORSHIFT><<<grid, 256, 0, stream>>>(q, d_buf, ctx);
+      break;
+    case SMP_HALTON:
+      plain_generate_kernel<SMP_HALTON><<<grid, 256, 0, stream>>>(q, d_buf, ctx);
+      break;
+    case SMP_LHS:
+      plain_generate_kernel<SMP_LHS><<<grid, 256, 0, stream>>>(q, d_buf, ctx);
+      break;
+    case SMP_SOBOL:
+      plain_generate_kernel<SMP_SOBOL><<<grid, 256, 0, stream>>>(q, d_buf, ctx);
+      break;
+    case SMP_COUNTER:
+      plain_generate_kernel<SMP_COUNTER><<<grid, 256, 0, stream>>>(q, d_buf, ctx);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <int FAM>
+__global__ void __launch_bounds__(256) plain_simulate_kernel(const DevReq* __restrict__ qp,
+                                                             const double* __restrict__ buf,
+                                                             double* __restrict__ payoff,
+                                                             double* __restrict__ control) {
+  const DevReq& q = *qp;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t u = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; u < q.n_units; u += stride) {
+    BufSource src{buf, q.n_units, u};
+    double p, c;
+    run_family<double, FAM>(q, src, p, c);
+    payoff[u] = p;
+    if (control) control[u] = c;
+  }
+}
+
+cudaError_t launch_plain_simulate(const DevReq& q, const DevReq* d_req, const double* d_buf, double* d_payoff,
+                                  double* d_control, cudaStream_t stream) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  uint64_t want = (q.n_units + 255) / 256;
+  int grid = (int)(want < (uint64_t)sms * 8 ? want : (uint64_t)sms * 8);
+  if (grid < 1) grid = 1;
+  switch (q.family) {
+    case FAM_GBM_STEP:
+      plain_simulate_kernel<FAM_GBM_STEP><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+    case FAM_GBM_TERMINAL:
+      plain_simulate_kernel<FAM_GBM_TERMINAL><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+    case FAM_HESTON:
+      plain_simulate_kernel<FAM_HESTON><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+    case FAM_MERTON_STEP:
+      plain_simulate_kernel<FAM_MERTON_STEP><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+    case FAM_MERTON_TERMINAL:
+      plain_simulate_kernel<FAM_MERTON_TERMINAL><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+    case FAM_BASKET:
+      plain_simulate_kernel<FAM_BASKET><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+    default:
+      plain_simulate_kernel<FAM_MLMC_LEVEL><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+// Deterministic FP64 reduction of the payoff (and control) buffers in tiles
+// of q.tile_units, finalized by the last tile.
+__global__ void __launch_bounds__(kFusedBlock) plain_reduce_kernel(DevReq* __restrict__ qp,
+                                                                   const double* __restrict__ payoff,
+                                                                   const double* __restrict__ control) {
+  __shared__ double red[kWarps][5];
+  __shared__ int s_last;
+  DevReq& q = *qp;
+  for (uint32_t t = blockIdx.x; t < q.n_tiles; t += gridDim.x) {
+    const uint64_t first = (uint64_t)t * q.tile_units;
+    const uint64_t last = min(first + (uint64_t)q.tile_units, q.n_units);
+    double v[5] = {0, 0, 0, 0, 0};
+    for (uint64_t u = first + threadIdx.x; u < last; u += blockDim.x) {
+      const double p = payoff[u];
+      v[0] += p;
+      v[1] += p * p;
+      if (control) {
+        const double c = control[u];
+        v[2] += c;
+        v[3] += c * c;
+        v[4] += p * c;
+      }
+    }
+    block_reduce5(v, red);
+    if (threadIdx.x == 0) {
+      double* pt = q.partials + (size_t)t * MPC_MOMENTS;
+      pt[0] = (double)(last - first);
+      for (int i = 0; i < 5; ++i) pt[1 + i] = v[i];
+      __threadfence();
+      s_last = (atomicAdd(q.tiles_done, 1u) == q.n_tiles - 1) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      finalize_request(q, red);
+    }
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_plain_reduce(const DevReq* d_req, const double* d_payoff, const double* d_control,
+                                uint64_t n_units, uint32_t n_tiles, cudaStream_t stream) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int grid = (int)(n_tiles < (uint32_t)sms * 4 ? n_tiles : (uint32_t)sms * 4);
+  if (grid < 1) grid = 1;
+  plain_reduce_kernel<<<grid, kFusedBlock, 0, stream>>>(const_cast<DevReq*>(d_req), d_payoff, d_control);
+  count_launch();
+  return cudaGetLastError();
+}
+
+// ---------------------------------------- reference v1 kernel contract ----
+// Same buffers and scalars as mc_cuda_european_call_stepwise_v1
+// (european_call_stepwise_v1.cu:1-28): path-major FP64 normals, one path per
+// thread, per-path discounted payoff.  Index arithmetic in 64 bits.
+__global__ void __launch_bounds__(256) european_call_stepwise_v1_kernel(const double* __restrict__ normals,
+                                                                       double* __restrict__ payoffs,
+                                                                       int32_t n_paths, int32_t n_steps,
+                                                                       double log_s0, double strike,
+                                                                       double drift_dt, double vol_dt,
+                                                                       double discount) {
+  const int64_t path = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (path >= n_paths) return;
+  double ls = log_s0;
+  const double* z = normals + path * (int64_t)n_steps;
+  for (int32_t s = 0; s < n_steps; ++s) ls += drift_dt + vol_dt * z[s];
+  const double st = exp(ls);
+  payoffs[path] = st > strike ? (st - strike) * discount : 0.0;
+}
+
+cudaError_t launch_european_call_stepwise_v1(const double* normals, double* payoffs, int32_t n_paths,
+                                             int32_t n_steps, double log_s0, double strike, double drift_dt,
+                                             double vol_dt, double discount, cudaStream_t stream) {
+  if (n_paths <= 0) return cudaSuccess;
+  int grid = (int)((n_paths + 255) / 256);
+  european_call_stepwise_v1_kernel<<<grid, 256, 0, stream>>>(normals, payoffs, n_paths, n_steps, log_s0, strike,
+                                                              drift_dt, vol_dt, discount);
+  count_launch();
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ LSM ---
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid barrier for a cooperative launch.  The wait is bounded: after
+// timeout_ns the block records the failure in *error and every block leaves
+// the kernel at the next check.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* error, uint64_t timeout_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const uint64_t start = global_ns();
+      while (*gen == g) {
+        if (*((volatile int*)error) != 0) break;
+        if (global_ns() - start > timeout_ns) {
+          atomicExch(error, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = *((volatile int*)error) == 0;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <class Real>
+__device__ __forceinline__ void laguerre4(Real x, Real b[4]) {
+  // laguerre_lsm_basis (cpu.rs:7667-7682); degrees above `degree` are unused
+  const Real x2 = x * x, x3 = x2 * x;
+  b[0] = (Real)1;
+  b[1] = (Real)1 - x;
+  b[2] = (Real)1 - (Real)2 * x + (Real)0.5 * x2;
+  b[3] = (Real)1 - (Real)3 * x + (Real)1.5 * x2 - x3 / (Real)6;
+}
+
+// solve_lsm_normal_equations (cpu.rs:7684-7736), FP64 Gauss-Jordan.
+__device__ bool solve4(double a[4][4], double rhs[4], int dim) {
+  for (int piv = 0; piv < dim; ++piv) {
+    int best = piv;
+    double best_abs = fabs(a[piv][piv]);
+    for (int row = piv + 1; row < dim; ++row) {
+      double c = fabs(a[row][piv]);
+      if (c > best_abs) {
+        best = row;
+        best_abs = c;
+      }
+    }
+    if (best_abs <= 1e-12) return false;
+    if (best != piv) {
+      for (int c = 0; c < 4; ++c) {
+        double t = a[piv][c];
+        a[piv][c] = a[best][c];
+        a[best][c] = t;
+      }
+      double t = rhs[piv];
+      rhs[piv] = rhs[best];
+      rhs[best] = t;
+    }
+    double pv = a[piv][piv];
+    for (int c = piv; c < dim; ++c) a[piv][c] /= pv;
+    rhs[piv] /= pv;
+    for (int row = 0; row < dim; ++row) {
+      if (row == piv) continue;
+      double f = a[row][piv];
+      if (f == 0.0) continue;
+      for (int c = piv; c < dim; ++c) a[row][c] -= f * a[piv][c];
+      rhs[row] -= f * rhs[piv];
+    }
+  }
+  return true;
+}
+
+constexpr int kLsmBlock = 256;
+constexpr int kLsmMaxP = 8;
+constexpr int kLsmMom = 15;  // 10 unique A^T A, 4 A^T b, ITM count
+
+template <class Real, int SMP>
+__global__ void __launch_bounds__(kLsmBlock) lsm_kernel(LsmArgs a, SrcCtx ctx) {
+  __shared__ double red[kWarps][5];
+  __shared__ double s_mom[16];
+  __shared__ double s_beta[4];
+  __shared__ int s_ok;
+  __shared__ Real s_disc[512];
+  const uint64_t n = a.n_paths;
+  const uint32_t steps = a.n_steps;
+  for (uint32_t j = threadIdx.x; j <= steps && j < 512; j += blockDim.x) s_disc[j] = (Real)a.disc_pow[j];
+  __syncthreads();
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  Real* paths = reinterpret_cast<Real*>(a.paths);
+  const Real k = (Real)a.k, drift = (Real)a.drift, vol = (Real)a.vol, inv_k = (Real)(1.0 / fmax(a.k, 2.2250738585072014e-308));
+  const int coeffs = (int)a.degree + 1;
+  Real cash[kLsmMaxP];
+  uint32_t exd[kLsmMaxP];
+  DevReq q;  // sampler view of the request
+  q.seed = a.seed;
+  q.seed32 = a.seed32;
+  q.n_chunks = 1;
+  q.normals_per_unit = steps;
+#pragma unroll
+  for (int j = 0; j < kLsmMaxP; ++j) {
+    const uint64_t path = gtid + (uint64_t)j * nthreads;
+    cash[j] = 0;
+    exd[j] = steps;
+    if (path >= n) continue;
+    Source<SMP> src;
+    src.template begin<sizeof(Real) == 8>(q, ctx, path);
+    Real s = (Real)a.s0;
+    for (uint32_t st = 1; st <= steps; ++st) {
+      const Real z = normal<Real>(src, st - 1);
+      s *= ex<Real>(drift + vol * z);  // multiplicative update as cpu.rs:3829-3830
+      paths[(uint64_t)(st - 1) * n + path] = s;
+    }
+    cash[j] = k - s > (Real)0 ? k - s : (Real)0;
+  }
+  uint32_t regressions = 0;
+  for (int si = (int)a.n_sched - 2; si >= 0; --si) {
+    const uint32_t step = a.sched[si];
+    const int buf = si & 1;
+    double m[kLsmMom];
+#pragma unroll
+    for (int i = 0; i < kLsmMom; ++i) m[i] = 0.0;
+    Real sv[kLsmMaxP];
+#pragma unroll
+    for (int j = 0; j < kLsmMaxP; ++j) {
+      const uint64_t path = gtid + (uint64_t)j * nthreads;
+      sv[j] = (Real)0;
+      if (path >= n) continue;
+      const Real s = paths[(uint64_t)(step - 1) * n + path];
+      sv[j] = s;
+      const Real imm = k - s;
+      if (!(imm > (Real)0)) continue;
+      const Real cont = cash[j] * s_disc[exd[j] - step];
+      Real b[4];
+      laguerre4<Real>(s * inv_k, b);
+      int idx = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = r; c < 4; ++c) m[idx++] += (double)(b[r] * b[c]);
+#pragma unroll
+      for (int r = 0; r < 4; ++r) m[10 + r] += (double)(b[r] * cont);
+      m[14] += 1.0;
+    }
+    // block reduction of the 15 moments in three rounds of five
+    double* part = a.partials + ((size_t)buf * gridDim.x + blockIdx.x) * 16;
+    for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
+      double v[5] = {m[r0], m[r0 + 1], m[r0 + 2], m[r0 + 3], m[r0 + 4]};
+      block_reduce5(v, red);
+      if (threadIdx.x == 0)
+        for (int i = 0; i < 5; ++i) part[r0 + i] = v[i];
+      __syncthreads();
+    }
+    if (!grid_barrier(a.barrier, a.error, a.timeout_ns)) return;
+    // every block sums the block partials in the same fixed order (identical result everywhere)
+    {
+      double acc[kLsmMom];
+#pragma unroll
+      for (int i = 0; i < kLsmMom; ++i) acc[i] = 0.0;
+      const double* base = a.partials + (size_t)buf * gridDim.x * 16;
+      for (uint32_t blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
+#pragma unroll
+        for (int i = 0; i < kLsmMom; ++i) acc[i] += __ldcg(base + (size_t)blk * 16 + i);
+      for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
+        double v[5] = {acc[r0], acc[r0 + 1], acc[r0 + 2], acc[r0 + 3], acc[r0 + 4]};
+        block_reduce5(v, red);
+        if (threadIdx.x == 0)
+          for (int i = 0; i < 5; ++i) s_mom[r0 + i] = v[i];
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double ata[4][4] = {{0}}, atb[4] = {0};
+      int idx = 0;
+      for (int r = 0; r < 4; ++r)
+        for (int c = r; c < 4; ++c) {
+          ata[r][c] = s_mom[idx];
+          ata[c][r] = s_mom[idx];
+          ++idx;
+        }
+      for (int r = 0; r < 4; ++r) atb[r] = s_mom[10 + r];
+      // the reference zeroes rows/columns beyond the basis degree
+      for (int r = coeffs; r < 4; ++r) {
+        atb[r] = 0.0;
+        for (int c = 0; c < 4; ++c) ata[r][c] = ata[c][r] = 0.0;
+      }
+      int ok = s_mom[14] >= (double)coeffs ? 1 : 0;
+      if (ok) ok = solve4(ata, atb, coeffs) ? 1 : 0;
+      for (int r = 0; r < 4; ++r) s_beta[r] = (ok && r < coeffs) ? atb[r] : 0.0;
+      s_ok = ok;
+    }
+    __syncthreads();
+    if (s_ok) {
+      ++regressions;
+      const Real b0 = (Real)s_beta[0], b1 = (Real)s_beta[1], b2 = (Real)s_beta[2], b3 = (Real)s_beta[3];
+#pragma unroll
+      for (int j = 0; j < kLsmMaxP; ++j) {
+        const uint64_t path = gtid + (uint64_t)j * nthreads;
+        if (path >= n) continue;
+        const Real imm = k - sv[j];
+        if (!(imm > (Real)0)) continue;
+        Real b[4];
+        laguerre4<Real>(sv[j] * inv_k, b);
+        Real cont = b0 * b[0] + b1 * b[1];
+        if (coeffs > 2) cont += b2 * b[2];
+        if (coeffs > 3) cont += b3 * b[3];
+        if (imm > (cont > (Real)0 ? cont : (Real)0)) {
+          cash[j] = imm;
+          exd[j] = step;
+        }
+      }
+    }
+  }
+  // estimator: discounted cashflows, exercise counts
+  double v[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+  for (int j = 0; j < kLsmMaxP; ++j) {
+    const uint64_t path = gtid + (uint64_t)j * nthreads;
+    if (path >= n) continue;
+    const double d = (double)cash[j] * a.disc_pow[exd[j]];
+    v[0] += d;
+    v[1] += d * d;
+    if (exd[j] < steps)
+      v[2] += 1.0;
+    else if (cash[j] > (Real)0)
+      v[3] += 1.0;
+  }
+  block_reduce5(v, red);
+  if (threadIdx.x == 0) {
+    double* fp = a.final_partials + (size_t)blockIdx.x * 4;
+    for (int i = 0; i < 4; ++i) fp[i] = v[i];
+    __threadfence();
+    s_ok = atomicAdd(a.done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_ok) {
+    __threadfence();
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (uint32_t blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
+      for (int i = 0; i < 4; ++i) acc[i] += __ldcg(a.final_partials + (size_t)blk * 4 + i);
+    block_reduce5(acc, red);
+    if (threadIdx.x != 0) return;
+    a.out[0] = (double)n;
+    a.out[1] = acc[0];
+    a.out[2] = acc[1];
+    a.out[3] = acc[2];
+    a.out[4] = acc[3];
+    a.out[5] = (double)regressions;
+    *a.done = 0u;
+  }
+}
+
+template <class Real, int SMP>
+static cudaError_t launch_lsm_t(const LsmArgs& a, const SrcCtx& ctx, int* grid_used, cudaStream_t stream) {
+  int dev = 0, sms = 148, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_kernel<Real, SMP>, kLsmBlock, 0);
+  if (per_sm < 1) return cudaErrorLaunchOutOfResources;
+  uint64_t need = (a.n_paths + (uint64_t)kLsmBlock * kLsmMaxP - 1) / ((uint64_t)kLsmBlock * kLsmMaxP);
+  uint64_t cap = (uint64_t)sms * (uint64_t)per_sm;
+  if (need > cap) return cudaErrorInvalidValue;  // more paths than co-resident threads x kLsmMaxP
+  // about two blocks per SM keeps the per-date barrier and partial sums cheap
+  uint64_t grid = (uint64_t)sms * 2 < cap ? (uint64_t)sms * 2 : cap;
+  uint64_t useful = (a.n_paths + kLsmBlock - 1) / kLsmBlock;
+  if (grid > useful) grid = useful;
+  if (grid < need) grid = need;
+  if (grid < 1) grid = 1;
+  *grid_used = (int)grid;
+  LsmArgs args = a;
+  SrcCtx c = ctx;
+  void* params[] = {&args, &c};
+  cudaError_t err = cudaLaunchCooperativeKernel((const void*)lsm_kernel<Real, SMP>, dim3((unsigned)grid),
+                                                dim3(kLsmBlock), params, 0, stream);
+  count_launch();
+  return err;
+}
+
+cudaError_t launch_lsm(const LsmArgs& a, const DeviceTables& tabs, int* grid_used, cudaStream_t stream) {
+  SrcCtx ctx{tabs.sobol, tabs.jump};
+  if (a.n_steps > 511) return cudaErrorInvalidValue;
+  if (a.fp64) {
+    if (a.sampler == SMP_COUNTER) return launch_lsm_t<double, SMP_COUNTER>(a, ctx, grid_used, stream);
+    return launch_lsm_t<double, SMP_XORSHIFT>(a, ctx, grid_used, stream);
+  }
+  if (a.sampler == SMP_COUNTER) return launch_lsm_t<float, SMP_COUNTER>(a, ctx, grid_used, stream);
+  return launch_lsm_t<float, SMP_XORSHIFT>(a, ctx, grid_used, stream);
+}
+
+// ------------------------------------------------------------ generators ---
+template <int SMP>
+__global__ void __launch_bounds__(256) generate_kernel(DevReq q, int fp32, void* out, uint64_t n_points,
+                                                       uint32_t dims, SrcCtx ctx) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n_points; p += stride) {
+    Source<SMP> src;
+    if (fp32) {
+      src.template begin<false>(q, ctx, p);
+      float* o = reinterpret_cast<float*>(out) + p * dims;
+      for (uint32_t d = 0; d < dims; ++d) o[d] = src.n32(d);
+    } else {
+      src.template begin<true>(q, ctx, p);
+      double* o = reinterpret_cast<double*>(out) + p * dims;
+      for (uint32_t d = 0; d < dims; ++d) o[d] = src.n64(d);
+    }
+  }
+}
+
+cudaError_t launch_generate_normals(const DevReq& q, int sampler, int fp32, void* d_out, uint64_t n_points,
+                                    uint32_t dims, const DeviceTables& tabs, cudaStream_t stream) {
+  SrcCtx ctx{tabs.sobol, tabs.jump};
+  uint64_t want = (n_points + 255) / 256;
+  int grid = (int)(want < 4096 ? want : 4096);
+  if (grid < 1) grid = 1;
+  switch (sampler) {
+    case SMP_XORSHIFT:
+      generate_kernel<SMP_XORSHIFT><<<grid, 256, 0, stream>>>(q, fp32, d_out, n_points, dims, ctx);
+      break;
+    case SMP_HALTON:
+      generate_kernel<SMP_HALTON><<<grid, 256, 0, stream>>>(q, fp32, d_out, n_points, dims, ctx);
+      break;
+    case SMP_LHS:
+      generate_kernel<SMP_LHS><<<grid, 256, 0, stream>>>(q, fp32, d_out, n_points, dims, ctx);
+      break;
+    case SMP_SOBOL:
+      generate_kernel<SMP_SOBOL><<<grid, 256, 0, stream>>>(q, fp32, d_out, n_points, dims, ctx);
+      break;
+    case SMP_COUNTER:
+      generate_kernel<SMP_COUNTER><<<grid, 256, 0, stream>>>(q, fp32, d_out, n_points, dims, ctx);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+__global__ void counter_hash_kernel(uint32_t seed, uint32_t n_paths, uint32_t n_steps, uint32_t* out) {
+  const uint64_t total = (uint64_t)n_paths * n_steps;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t path = (uint32_t)(i / n_steps), step = (uint32_t)(i % n_steps);
+    out[2 * i] = hash_u32(counter_mix(seed, path, step, 0u));
+    out[2 * i + 1] = hash_u32(counter_mix(seed, path, step, 1u));
+  }
+}
+
+cudaError_t launch_counter_hash(uint32_t seed, uint32_t n_paths, uint32_t n_steps, uint32_t* d_out,
+                                cudaStream_t stream) {
+  uint64_t total = (uint64_t)n_paths * n_steps;
+  int grid = (int)((total + 255) / 256 < 4096 ? (total + 255) / 256 : 4096);
+  if (grid < 1) grid = 1;
+  counter_hash_kernel<<<grid, 256, 0, stream>>>(seed, n_paths, n_steps, d_out);
+  count_launch();
+  return cudaGetLastError();
+}
+
+// Each thread emits 64 consecutive draws after one jump.
+__global__ void xorshift_kernel(uint64_t seed, uint64_t offset, uint64_t count, uint64_t* out, const uint64_t* jump) {
+  const uint64_t chunk = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t first = chunk * 64;
+  if (first >= count) return;
+  XorshiftStream st;
+  uint64_t s0 = seed == 0 ? 0x9E3779B97F4A7C15ull : seed;
+  st.state = xorshift_jump(jump, s0, offset + first);
+  st.has_cached = false;
+  const uint64_t last = first + 64 < count ? first + 64 : count;
+  for (uint64_t i = first; i < last; ++i) out[i] = st.next_u64();
+}
+
+cudaError_t launch_xorshift(uint64_t seed, uint64_t offset, uint64_t count, uint64_t* d_out,
+                            const DeviceTables& tabs, cudaStream_t stream) {
+  uint64_t chunks = (count + 63) / 64;
+  int grid = (int)((chunks + 255) / 256);
+  if (grid < 1) grid = 1;
+  xorshift_kernel<<<grid, 256, 0, stream>>>(seed, offset, count, d_out, tabs.jump);
+  count_launch();
+  return cudaGetLastError();
+}
+
+cudaError_t launch_flush(void* d_buf, size_t bytes, cudaStream_t stream) {
+  count_launch();
+  return cudaMemsetAsync(d_buf, (int)(g_launches.load() & 0xFF), bytes, stream);
+}
+
+}  // namespace mpc

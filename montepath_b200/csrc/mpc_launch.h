@@ -1,0 +1,69 @@
+// mpc_launch.h -- host-side launch wrappers of the kernels in mpc_kernels.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mpc_types.h"
+
+namespace mpc {
+
+struct DeviceTables {
+  const uint32_t* sobol;  // [256][8][16] nibble tables
+  const uint64_t* jump;   // [64][16][16] xorshift jump nibble tables
+};
+
+// Fused FP32 path: one persistent launch over a tile work list.  All
+// requests in `reqs` must share `sampler`; `family` < 0 lets each tile switch
+// on its request's family (mixed batches).
+cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_tiles, uint32_t* d_tile_counter,
+                         int family, int sampler, const DeviceTables& tabs, int grid, int block,
+                         cudaStream_t stream);
+int fused_max_blocks_per_sm(int family, int sampler, int block);
+
+// FP64 plain path: materialise samples, simulate into a payoff buffer, reduce.
+cudaError_t launch_plain_generate(const DevReq& q, double* d_buf, int sampler, const DeviceTables& tabs,
+                                  cudaStream_t stream);
+cudaError_t launch_plain_simulate(const DevReq& q, const DevReq* d_req, const double* d_buf, double* d_payoff,
+                                  double* d_control, cudaStream_t stream);
+cudaError_t launch_plain_reduce(const DevReq* d_req, const double* d_payoff, const double* d_control,
+                                uint64_t n_units, uint32_t n_tiles, cudaStream_t stream);
+
+// Reference kernel contract mc_cuda_european_call_stepwise_v1.
+cudaError_t launch_european_call_stepwise_v1(const double* normals, double* payoffs, int32_t n_paths,
+                                             int32_t n_steps, double log_s0, double strike, double drift_dt,
+                                             double vol_dt, double discount, cudaStream_t stream);
+
+// Longstaff-Schwartz: one cooperative launch (paths, backward induction, estimator).
+struct LsmArgs {
+  uint64_t n_paths;
+  uint32_t n_steps, n_sched, degree, sampler;
+  uint64_t seed;
+  uint32_t seed32, fp64;
+  double s0, k, drift, vol, disc_step;
+  const uint32_t* sched;     // exercise dates (ascending, ends with n_steps)
+  const double* disc_pow;    // disc_step^j, j = 0..n_steps
+  void* paths;               // [n_steps][n_paths] float or double
+  double* partials;          // [2][grid][16]
+  double* final_partials;    // [grid][4]
+  double* out;               // [8]: n, sum, sumsq, early, maturity, regressions
+  unsigned* barrier;         // [2]: count, generation
+  unsigned* done;            // last-block counter
+  int* error;                // barrier timeout flag
+  uint64_t timeout_ns;
+};
+cudaError_t launch_lsm(const LsmArgs& a, const DeviceTables& tabs, int* grid_used, cudaStream_t stream);
+
+// Device generators for the ABI's sampler entry points.
+cudaError_t launch_generate_normals(const DevReq& q, int sampler, int fp32, void* d_out, uint64_t n_points,
+                                    uint32_t dims, const DeviceTables& tabs, cudaStream_t stream);
+cudaError_t launch_counter_hash(uint32_t seed, uint32_t n_paths, uint32_t n_steps, uint32_t* d_out,
+                                cudaStream_t stream);
+cudaError_t launch_xorshift(uint64_t seed, uint64_t offset, uint64_t count, uint64_t* d_out,
+                            const DeviceTables& tabs, cudaStream_t stream);
+cudaError_t launch_flush(void* d_buf, size_t bytes, cudaStream_t stream);
+
+// Kernel launches issued by the wrappers above since process start.
+uint64_t kernel_launch_count();
+
+}  // namespace mpc

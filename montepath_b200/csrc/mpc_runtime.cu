@@ -1,0 +1,1560 @@
+// mpc_runtime.cu -- host runtime of the B200 Monte Carlo backend behind the
+// C ABI of include/montepath_cuda.h.
+//
+// It replaces NvidiaCudaBackend (crates/mc-core/src/backend/cuda.rs:40-203):
+// device discovery, support reports, request validation with status codes,
+// launch-shape selection, and execution of every pricing family on the GPU.
+// There is no CPU fallback: a request the device path cannot run is
+// rejected with MPC_E_UNSUPPORTED.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "mpc_device.cuh"
+#include "mpc_launch.h"
+#include "mpc_runtime.h"
+#include "sobol_directions.h"
+
+using namespace mpc;
+
+namespace mpc {
+
+int fail(mpc_context* ctx, int status, const std::string& msg) {
+  if (ctx) ctx->last_error = msg;
+  return status;
+}
+
+int cuda_fail(mpc_context* ctx, cudaError_t err, const char* what) {
+  std::string msg = std::string(what) + ": " + cudaGetErrorName(err) + " (" + cudaGetErrorString(err) + ")";
+  if (ctx) ctx->last_error = msg;
+  return err == cudaErrorMemoryAllocation ? MPC_E_OOM_BUDGET : MPC_E_CUDA;
+}
+
+#define MPC_CUDA(ctx, call)                                   \
+  do {                                                        \
+    cudaError_t _e = (call);                                  \
+    if (_e != cudaSuccess) return cuda_fail((ctx), _e, #call); \
+  } while (0)
+
+int scratch(mpc_context* ctx, const std::string& name, size_t bytes, void** out) {
+  if (bytes == 0) bytes = 16;
+  DevBuf& b = ctx->bufs[name];
+  if (b.bytes >= bytes) {
+    *out = b.ptr;
+    return MPC_OK;
+  }
+  size_t grow = std::max(bytes, b.bytes + b.bytes / 2);
+  grow = (grow + 255) & ~size_t(255);
+  uint64_t after = ctx->live_bytes - b.bytes + grow;
+  if (after > ctx->budget) {
+    grow = (bytes + 255) & ~size_t(255);
+    after = ctx->live_bytes - b.bytes + grow;
+    if (after > ctx->budget)
+      return fail(ctx, MPC_E_OOM_BUDGET,
+                  "request needs " + std::to_string(bytes) + " device bytes for '" + name +
+                      "', beyond the HBM budget of " + std::to_string(ctx->budget) + " bytes");
+  }
+  if (b.ptr) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(b.ptr);
+    ctx->live_bytes -= b.bytes;
+    b.ptr = nullptr;
+    b.bytes = 0;
+  }
+  void* p = nullptr;
+  cudaError_t err = cudaMalloc(&p, grow);
+  if (err != cudaSuccess) return cuda_fail(ctx, err, ("cudaMalloc " + name).c_str());
+  cudaMemset(p, 0, grow);
+  b.ptr = p;
+  b.bytes = grow;
+  ctx->live_bytes += grow;
+  ctx->peak_bytes = std::max(ctx->peak_bytes, ctx->live_bytes);
+  *out = p;
+  return MPC_OK;
+}
+
+static int pinned_staging(mpc_context* ctx, size_t bytes, void** out) {
+  if (ctx->pinned_bytes < bytes) {
+    if (ctx->pinned) {
+      cudaStreamSynchronize(ctx->stream);
+      cudaFreeHost(ctx->pinned);
+    }
+    size_t grow = std::max(bytes, ctx->pinned_bytes * 2);
+    cudaError_t err = cudaHostAlloc(&ctx->pinned, grow, cudaHostAllocDefault);
+    if (err != cudaSuccess) {
+      ctx->pinned = nullptr;
+      ctx->pinned_bytes = 0;
+      return cuda_fail(ctx, err, "cudaHostAlloc");
+    }
+    ctx->pinned_bytes = grow;
+  }
+  *out = ctx->pinned;
+  return MPC_OK;
+}
+
+// ------------------------------------------------------------ validation ---
+static bool finite(double x) { return std::isfinite(x); }
+
+static int invalid(std::string* msg, const std::string& m) {
+  if (msg) *msg = m;
+  return MPC_E_INVALID_CONFIG;
+}
+static int unsupported(std::string* msg, const std::string& m) {
+  if (msg) *msg = m;
+  return MPC_E_UNSUPPORTED;
+}
+
+static bool is_lsm(int w) { return w == MPC_WORKLOAD_AMERICAN_PUT || w == MPC_WORKLOAD_BERMUDAN_PUT; }
+
+// Lower Cholesky factor; returns false if the matrix is not a valid correlation matrix.
+static bool cholesky(const double* corr, uint32_t d, double* L) {
+  std::memset(L, 0, sizeof(double) * 64);
+  if (d == 2) {  // exactly the reference's rho / sqrt(1 - rho^2) split (cpu.rs:7622-7630)
+    if (corr[1] < -1.0 || corr[1] > 1.0) return false;
+    L[0] = 1.0;
+    L[2] = corr[1];
+    L[3] = std::sqrt(std::max(1.0 - corr[1] * corr[1], 0.0));
+    return true;
+  }
+  for (uint32_t i = 0; i < d; ++i) {
+    if (std::fabs(corr[i * d + i] - 1.0) > 1e-12) return false;
+    for (uint32_t j = 0; j < d; ++j)
+      if (std::fabs(corr[i * d + j] - corr[j * d + i]) > 1e-12) return false;
+  }
+  for (uint32_t i = 0; i < d; ++i) {
+    for (uint32_t j = 0; j <= i; ++j) {
+      double s = corr[i * d + j];
+      for (uint32_t k = 0; k < j; ++k) s -= L[i * d + k] * L[j * d + k];
+      if (i == j) {
+        if (s < -1e-12) return false;
+        L[i * d + i] = std::sqrt(std::max(s, 0.0));
+      } else {
+        L[i * d + j] = L[j * d + j] > 0.0 ? s / L[j * d + j] : 0.0;
+      }
+    }
+  }
+  return true;
+}
+
+// Mirrors the reference's config asserts (cpu.rs:5010-5153 and the per-entry
+// asserts such as cpu.rs:3014-3016) as status codes, plus the device limits.
+int validate(const mpc_request_t& r, std::string* msg) {
+  if (r.workload < 0 || r.workload > MPC_WORKLOAD_ASIAN_MLMC) return invalid(msg, "unknown workload");
+  if (r.model < 0 || r.model > MPC_MODEL_MERTON) return invalid(msg, "unknown model");
+  if (r.technique < 0 || r.technique > MPC_TECHNIQUE_CONTROL_VARIATE) return invalid(msg, "unknown technique");
+  if (r.sampling < 0 || r.sampling > MPC_SAMPLING_COUNTER_HASH) return invalid(msg, "unknown sampling");
+  if (r.precision != MPC_PRECISION_FP64_PLAIN && r.precision != MPC_PRECISION_FP32_PATH)
+    return invalid(msg, "unknown precision");
+  if (r.method < 0 || r.method > MPC_METHOD_STEPWISE) return invalid(msg, "unknown method");
+  for (double x : {r.s0, r.k, r.r, r.sigma, r.t})
+    if (!finite(x)) return invalid(msg, "market parameters must be finite");
+  if (r.workload == MPC_WORKLOAD_ASIAN_MLMC) {
+    if (!(r.s0 > 0.0) || !(r.k > 0.0) || !(r.t > 0.0)) return invalid(msg, "s0, k and t must be > 0");
+    if (!(r.sigma >= 0.0)) return invalid(msg, "sigma must be >= 0");
+    if (r.base_steps == 0) return invalid(msg, "base_steps must be > 0");
+    if (r.levels == 0 || r.levels > MPC_MAX_LEVELS) return invalid(msg, "levels must be in 1..=16");
+    if (r.refinement_factor < 2) return invalid(msg, "refinement_factor must be >= 2");
+    if (r.scramble_replicates == 0) return invalid(msg, "scramble_replicates must be > 0");
+    uint64_t fine = r.base_steps;
+    for (uint32_t l = 1; l < r.levels; ++l) {
+      fine *= r.refinement_factor;
+      if (fine > (1u << 20)) return unsupported(msg, "finest MLMC level exceeds 2^20 steps");
+    }
+    if (r.target_stderr > 0.0) {
+      if (!finite(r.target_stderr)) return invalid(msg, "target_stderr must be finite");
+      if (r.pilot_paths_per_level < 2) return invalid(msg, "pilot_paths_per_level must be > 1");
+      if (r.min_step_updates == 0) return invalid(msg, "min_step_updates must be > 0");
+      if (r.max_step_updates < r.min_step_updates) return invalid(msg, "max_step_updates must be >= min_step_updates");
+    } else {
+      for (uint32_t l = 0; l < r.levels; ++l)
+        if (r.paths_per_level[l] == 0) return invalid(msg, "paths_per_level values must be > 0");
+    }
+    if (r.technique != MPC_TECHNIQUE_STANDARD) return unsupported(msg, "MLMC supports the standard technique only");
+    if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE)
+      return unsupported(msg, "Brownian-bridge sampling is not implemented for MLMC levels");
+    return MPC_OK;
+  }
+  if (r.n_paths == 0) return invalid(msg, "n_paths must be > 0");
+  if (r.n_paths > (1ull << 32)) return unsupported(msg, "n_paths above 2^32 is not supported");
+  if (r.n_steps == 0) return invalid(msg, "n_steps must be > 0");
+  if (!(r.t > 0.0)) return invalid(msg, "t must be > 0");
+  if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE)
+    return unsupported(msg, "Brownian-bridge Sobol sampling runs on the CPU reference only");
+  if (is_lsm(r.workload)) {
+    if (r.n_steps < 2) return invalid(msg, "n_steps must be >= 2 for LSM regression");
+    if (r.n_steps > 511) return unsupported(msg, "LSM supports at most 511 steps");
+    if (!(r.s0 > 0.0) || !(r.k > 0.0)) return invalid(msg, "s0 and k must be > 0");
+    if (!(r.sigma >= 0.0)) return invalid(msg, "sigma must be >= 0");
+    if (r.basis_degree == 0) return invalid(msg, "basis_degree must be > 0");
+    if (r.workload == MPC_WORKLOAD_BERMUDAN_PUT) {
+      if (r.n_exercise == 0) return invalid(msg, "exercise_steps must include at least one exercise date");
+      if (r.n_exercise > MPC_MAX_EXERCISE_DATES) return invalid(msg, "at most 64 exercise dates");
+      for (uint32_t i = 0; i < r.n_exercise; ++i)
+        if (r.exercise_steps[i] == 0 || r.exercise_steps[i] > r.n_steps)
+          return invalid(msg, "exercise_steps must be in 1..=n_steps");
+    }
+    if (r.sampling != MPC_SAMPLING_PSEUDORANDOM && r.sampling != MPC_SAMPLING_COUNTER_HASH)
+      return unsupported(msg, "LSM paths use the pseudorandom or counter-hash stream");
+    if (r.technique != MPC_TECHNIQUE_STANDARD) return unsupported(msg, "LSM supports the standard technique only");
+    if (r.n_paths > 8ull * 148 * 8 * 256) return unsupported(msg, "LSM path count exceeds the co-resident capacity");
+    return MPC_OK;
+  }
+  if (r.workload == MPC_WORKLOAD_BASKET_CALL) {
+    if (r.n_assets < 1 || r.n_assets > MPC_MAX_ASSETS) return invalid(msg, "n_assets must be in 1..=8");
+    for (uint32_t a = 0; a < r.n_assets; ++a) {
+      if (!(r.spots[a] > 0.0)) return invalid(msg, "basket spots must be > 0");
+      if (!(r.sigmas[a] >= 0.0)) return invalid(msg, "basket sigmas must be >= 0");
+      if (!finite(r.weights[a])) return invalid(msg, "basket weights must be finite");
+    }
+    if (!(r.k >= 0.0)) return invalid(msg, "k must be >= 0");
+    double L[64];
+    if (!cholesky(r.corr, r.n_assets, L)) return invalid(msg, "corr must be a valid correlation matrix");
+    if (r.model != MPC_MODEL_GBM) return unsupported(msg, "baskets are simulated under GBM");
+  } else {
+    if (!(r.s0 > 0.0)) return invalid(msg, "s0 must be > 0");
+    if (!(r.k >= 0.0)) return invalid(msg, "k must be >= 0");
+    if (!(r.sigma >= 0.0)) return invalid(msg, "sigma must be >= 0");
+  }
+  if (r.workload == MPC_WORKLOAD_DOWN_AND_OUT_CALL || r.workload == MPC_WORKLOAD_UP_AND_OUT_CALL) {
+    if (!(r.barrier > 0.0)) return invalid(msg, "barrier must be > 0");
+  }
+  if (r.model == MPC_MODEL_HESTON) {
+    if (r.workload != MPC_WORKLOAD_EUROPEAN_CALL) return unsupported(msg, "Heston prices European calls");
+    if (!(r.v0 >= 0.0) || !(r.kappa >= 0.0) || !(r.theta >= 0.0) || !(r.vol_of_vol >= 0.0))
+      return invalid(msg, "v0, kappa, theta and vol_of_vol must be >= 0");
+    if (!(r.rho >= -1.0 && r.rho <= 1.0)) return invalid(msg, "rho must be in [-1, 1]");
+  }
+  if (r.model == MPC_MODEL_MERTON) {
+    if (r.workload != MPC_WORKLOAD_EUROPEAN_CALL) return unsupported(msg, "Merton prices European calls");
+    if (!(r.k > 0.0)) return invalid(msg, "k must be > 0");
+    if (!(r.jump_intensity >= 0.0)) return invalid(msg, "jump_intensity must be >= 0");
+    if (!(r.jump_volatility >= 0.0)) return invalid(msg, "jump_volatility must be >= 0");
+    if (!finite(r.jump_mean)) return invalid(msg, "jump_mean must be finite");
+    if (r.sampling == MPC_SAMPLING_PSEUDORANDOM)
+      return unsupported(msg,
+                         "Merton draws a variable number of normals per path from one sequential stream; "
+                         "use scrambled_sobol, randomized_halton, latin_hypercube or counter_hash on the GPU");
+    if (r.technique == MPC_TECHNIQUE_ANTITHETIC) return unsupported(msg, "Merton supports standard and control variate");
+  }
+  uint64_t dims_per_unit = r.n_steps;
+  if (r.model == MPC_MODEL_HESTON) dims_per_unit = 2ull * r.n_steps;
+  if (r.model == MPC_MODEL_MERTON) dims_per_unit = 3ull * (r.method == MPC_METHOD_STEPWISE ? r.n_steps : 1);
+  if (r.workload == MPC_WORKLOAD_BASKET_CALL)
+    dims_per_unit = uint64_t(r.n_assets) * (r.method == MPC_METHOD_STEPWISE ? r.n_steps : 1);
+  if (dims_per_unit > (1ull << 20)) return unsupported(msg, "more than 2^20 sample dimensions per path");
+  if (r.sampling == MPC_SAMPLING_RANDOMIZED_HALTON && dims_per_unit > 8192)
+    return unsupported(msg, "randomized Halton supports at most 8192 dimensions");
+  if (r.sampling == MPC_SAMPLING_LATIN_HYPERCUBE && dims_per_unit > 8192)
+    return unsupported(msg, "Latin hypercube supports at most 8192 dimensions");
+  return MPC_OK;
+}
+
+uint64_t estimate_bytes(const mpc_request_t& r) {
+  // Fused: tile partials only.  Plain: materialised samples + payoff buffers.
+  if (r.workload == MPC_WORKLOAD_ASIAN_MLMC) {
+    uint64_t total = 0, fine = r.base_steps;
+    for (uint32_t l = 0; l < r.levels && l < MPC_MAX_LEVELS; ++l) {
+      uint64_t paths = r.target_stderr > 0.0 ? std::max<uint64_t>(r.pilot_paths_per_level, 1) : r.paths_per_level[l];
+      if (r.precision == MPC_PRECISION_FP64_PLAIN) total = std::max(total, paths * fine * 8 + paths * 16);
+      total += (paths / 256 + 1) * 64;
+      fine *= std::max<uint32_t>(r.refinement_factor, 1);
+    }
+    return total + 4096;
+  }
+  uint64_t units = r.technique == MPC_TECHNIQUE_ANTITHETIC ? (r.n_paths + 1) / 2 : r.n_paths;
+  if (is_lsm(r.workload)) {
+    uint64_t elem = r.precision == MPC_PRECISION_FP64_PLAIN ? 8 : 4;
+    return r.n_paths * r.n_steps * elem + 2 * 8192 * 16 * 8 + 4096;
+  }
+  uint64_t dims = r.n_steps;
+  if (r.model == MPC_MODEL_HESTON) dims = 2ull * r.n_steps;
+  if (r.model == MPC_MODEL_MERTON) dims = 3ull * (r.method == MPC_METHOD_STEPWISE ? r.n_steps : 1);
+  if (r.workload == MPC_WORKLOAD_BASKET_CALL) dims = uint64_t(r.n_assets) * (r.method == MPC_METHOD_STEPWISE ? r.n_steps : 1);
+  if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.model == MPC_MODEL_GBM && r.method != MPC_METHOD_STEPWISE)
+    dims = 1;
+  uint64_t partials = (units / 256 + 1) * 64 + 1024;
+  if (r.precision == MPC_PRECISION_FP64_PLAIN) return units * dims * 8 + units * 16 + partials;
+  return partials + 2048;
+}
+
+// --------------------------------------------------------------- prepare ---
+static int sampler_of(int sampling) {
+  switch (sampling) {
+    case MPC_SAMPLING_PSEUDORANDOM:
+      return SMP_XORSHIFT;
+    case MPC_SAMPLING_RANDOMIZED_HALTON:
+      return SMP_HALTON;
+    case MPC_SAMPLING_LATIN_HYPERCUBE:
+      return SMP_LHS;
+    case MPC_SAMPLING_COUNTER_HASH:
+      return SMP_COUNTER;
+    default:
+      return SMP_SOBOL;
+  }
+}
+
+static std::vector<uint32_t> first_primes(size_t n) {
+  std::vector<uint32_t> primes;
+  uint32_t c = 2;
+  while (primes.size() < n) {
+    uint32_t lim = uint32_t(std::sqrt(double(c)));
+    bool prime = true;
+    for (uint32_t p : primes) {
+      if (p > lim) break;
+      if (c % p == 0) {
+        prime = false;
+        break;
+      }
+    }
+    if (prime) primes.push_back(c);
+    ++c;
+  }
+  return primes;
+}
+
+static double open01_u64(uint64_t v) {
+  return std::max(double(v >> 11) * (1.0 / 9007199254740992.0), 2.2250738585072014e-308);
+}
+
+static uint64_t gcd64(uint64_t a, uint64_t b) {
+  while (b) {
+    uint64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Sampler tables of a structured sampler: RandomizedHalton::new (cpu.rs:5692-5704)
+// and LatinHypercube::new (cpu.rs:5737-5761).
+static void build_sampler_tables(Prepared* p, uint64_t seed, uint64_t n_paths, uint64_t dims) {
+  if (p->sampler == SMP_HALTON) {
+    size_t count = std::max<size_t>(dims, 2);
+    p->halton_primes = first_primes(count);
+    p->halton_shifts.resize(count);
+    for (size_t d = 0; d < count; ++d)
+      p->halton_shifts[d] = open01_u64(splitmix64(seed + uint64_t(d) * 0x9E3779B97F4A7C15ull));
+  } else if (p->sampler == SMP_LHS) {
+    size_t count = std::max<size_t>(dims, 1);
+    p->lhs.resize(count);
+    for (size_t d = 0; d < count; ++d) {
+      uint64_t mixed = splitmix64(seed ^ (uint64_t(d) * 0x9E3779B97F4A7C15ull) ^ 0xD1B54A32D192ED03ull);
+      uint64_t modulus = std::max<uint64_t>(n_paths, 1), c = 1;
+      if (modulus > 1) {  // coprime_multiplier (cpu.rs:5983-6002)
+        c = std::max<uint64_t>(mixed % modulus, 1);
+        if (c % 2 == 0) c += 1;
+        while (gcd64(c, modulus) != 1) {
+          c += 2;
+          if (c >= modulus) c = 1;
+        }
+      }
+      p->lhs[d].multiplier = c;
+      p->lhs[d].offset = n_paths == 0 ? 0 : splitmix64(mixed ^ 0xA24BAED4963EE407ull) % n_paths;
+      p->lhs[d].jitter_seed = splitmix64(mixed ^ 0x9FB21C651E98DF25ull);
+    }
+  }
+}
+
+int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* msg) {
+  int st = validate(r, msg);
+  if (st != MPC_OK) return st;
+  *p = Prepared();
+  DevReq& q = p->q;
+  std::memset(&q, 0, sizeof(q));
+  p->sampler = sampler_of(r.sampling);
+  p->plain = r.precision == MPC_PRECISION_FP64_PLAIN;
+  p->lsm = is_lsm(r.workload);
+  p->mlmc = r.workload == MPC_WORKLOAD_ASIAN_MLMC;
+  q.workload = r.workload;
+  q.technique = r.technique;
+  q.sampling = r.sampling;
+  q.seed = r.seed;
+  q.seed32 = uint32_t(r.seed);
+  q.anti = r.technique == MPC_TECHNIQUE_ANTITHETIC;
+  q.cv = r.technique == MPC_TECHNIQUE_CONTROL_VARIATE;
+  q.n_paths = r.n_paths;
+  q.n_units = q.anti ? (r.n_paths + 1) / 2 : r.n_paths;
+  q.s0 = r.s0;
+  q.k = r.k;
+  q.barrier = r.barrier;
+  q.log_s0 = std::log(r.s0 > 0 ? r.s0 : 1.0);
+  q.log_barrier = r.barrier > 0.0 ? std::log(r.barrier) : -INFINITY;
+  q.discount = std::exp(-r.r * r.t);
+  q.cv_expectation = r.s0;
+  q.n_chunks = 1;
+  if (p->lsm || p->mlmc) return MPC_OK;  // driven by their own runners
+  bool chunkable = true;
+  if (r.workload == MPC_WORKLOAD_BASKET_CALL) {
+    q.family = FAM_BASKET;
+    const bool step = r.method == MPC_METHOD_STEPWISE;
+    q.n_steps = step ? r.n_steps : 1;
+    q.n_assets = r.n_assets;
+    double dt = r.t / double(q.n_steps);
+    cholesky(r.corr, r.n_assets, q.chol);
+    double expectation = 0.0;
+    for (uint32_t a = 0; a < r.n_assets; ++a) {
+      q.b_drift[a] = (r.r - 0.5 * r.sigmas[a] * r.sigmas[a]) * dt;
+      q.b_vol[a] = r.sigmas[a] * std::sqrt(dt);
+      q.spots[a] = r.spots[a];
+      q.weights[a] = r.weights[a];
+      expectation += r.weights[a] * r.spots[a];  // basket_control_expectation (cpu.rs:7637-7639)
+    }
+    q.cv_expectation = expectation;
+    q.normals_per_unit = uint64_t(r.n_assets) * q.n_steps;
+    chunkable = false;  // the reference basket runs one stream (cpu.rs:7503-7518)
+    p->path_steps = r.n_paths * q.n_steps;
+  } else if (r.model == MPC_MODEL_HESTON) {
+    q.family = FAM_HESTON;
+    q.n_steps = r.n_steps;
+    q.v0 = r.v0;
+    q.kappa = r.kappa;
+    q.theta = r.theta;
+    q.xi = r.vol_of_vol;
+    q.rho = r.rho;
+    q.rho_perp = std::sqrt(std::max(1.0 - r.rho * r.rho, 0.0));
+    q.dt = r.t / double(r.n_steps);
+    q.sqrt_dt = std::sqrt(r.t / double(r.n_steps));
+    q.rate = r.r;
+    q.normals_per_unit = 2ull * r.n_steps;
+    p->path_steps = r.n_paths * r.n_steps;
+  } else if (r.model == MPC_MODEL_MERTON) {
+    const bool step = r.method == MPC_METHOD_STEPWISE;
+    q.family = step ? FAM_MERTON_STEP : FAM_MERTON_TERMINAL;
+    q.n_steps = step ? r.n_steps : 1;
+    double kj = r.jump_intensity * (std::exp(r.jump_mean + 0.5 * r.jump_volatility * r.jump_volatility) - 1.0);
+    double dt = r.t / double(q.n_steps);
+    q.drift_dt = (r.r - kj - 0.5 * r.sigma * r.sigma) * dt;
+    q.vol_dt = r.sigma * std::sqrt(dt);
+    q.lam_dt = r.jump_intensity * dt;
+    q.jump_mean = r.jump_mean;
+    q.jump_vol = r.jump_volatility;
+    q.normals_per_unit = 3ull * q.n_steps;
+    p->path_steps = r.n_paths * q.n_steps;
+  } else if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.method != MPC_METHOD_STEPWISE) {
+    q.family = FAM_GBM_TERMINAL;  // EuropeanCallMethod::Auto == terminal (cpu.rs:3020-3025)
+    q.n_steps = 1;
+    q.drift_dt = (r.r - 0.5 * r.sigma * r.sigma) * r.t;
+    q.vol_dt = r.sigma * std::sqrt(r.t);
+    q.normals_per_unit = 1;
+    chunkable = !q.anti;  // simulate_terminal_antithetic is single-stream (cpu.rs:7785-7805)
+    p->path_steps = r.n_paths;
+  } else {
+    q.family = FAM_GBM_STEP;
+    q.n_steps = r.n_steps;
+    double dt = r.t / double(r.n_steps);
+    q.drift_dt = (r.r - 0.5 * r.sigma * r.sigma) * dt;
+    q.vol_dt = r.sigma * std::sqrt(dt);
+    q.normals_per_unit = r.n_steps;
+    // simulate_stepwise_antithetic (European) is single-stream (cpu.rs:7807-7835)
+    if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && q.anti) chunkable = false;
+    p->path_steps = r.n_paths * r.n_steps;
+  }
+  p->family = q.family;
+  p->cv_expectation = q.cv_expectation;
+  const uint64_t threads = r.n_threads <= 1 ? 1 : r.n_threads;
+  if (p->sampler == SMP_XORSHIFT && chunkable && threads > 1 && q.n_units >= threads * 2000) {
+    q.n_chunks = uint32_t(threads);
+    q.chunk_base = q.n_units / threads;
+    q.chunk_rem = q.n_units % threads;
+  }
+  build_sampler_tables(p, r.seed, r.n_paths, q.normals_per_unit);
+  (void)ctx;
+  return MPC_OK;
+}
+
+Shape choose_shape(mpc_context* ctx, const Prepared& p) {
+  // Autotuner: paths-per-thread per (family, sampler, step bucket, size
+  // bucket), picked so that a request spreads over at least four waves of
+  // resident blocks; cached per context.
+  const int steps_bucket = 32 - __builtin_clz(std::max<uint32_t>(p.q.n_steps, 1));
+  const int size_bucket = 64 - __builtin_clzll(std::max<uint64_t>(p.q.n_units, 1));
+  const uint64_t key = (uint64_t(p.family) << 48) | (uint64_t(p.sampler) << 40) | (uint64_t(steps_bucket) << 8) |
+                       uint64_t(size_bucket);
+  std::lock_guard<std::mutex> lock(ctx->tuner.mu);
+  auto it = ctx->tuner.cache.find(key);
+  if (it != ctx->tuner.cache.end()) {
+    ++ctx->tuner.hits;
+    return it->second;
+  }
+  ++ctx->tuner.misses;
+  Shape s;
+  s.block = 256;
+  int occ = std::max(1, fused_max_blocks_per_sm(p.family, p.sampler, 256));
+  uint64_t resident = uint64_t(ctx->sm_count) * occ * 256;
+  uint64_t want = p.q.n_units / std::max<uint64_t>(resident * 4, 1);
+  uint32_t ppt = 1;
+  while (ppt < 8 && uint64_t(ppt) * 2 <= want) ppt *= 2;
+  s.ppt = ppt;
+  ctx->tuner.cache[key] = s;
+  return s;
+}
+
+static void summarize(double n, double sum, double sq, double* price, double* se) {
+  double mean = sum / n;
+  double var = (sq / n) - mean * mean;
+  *price = mean;
+  *se = std::sqrt(std::max(var, 0.0)) / std::sqrt(n);
+}
+
+// summarize_payoffs / summarize_block_estimates / summarize_control_variate (cpu.rs:7641-7771).
+void summarize_moments(const Prepared& p, const double* m, mpc_result_t* out) {
+  const double n = m[0];
+  for (int i = 0; i < 6; ++i) out->moments[i] = m[i];
+  out->n_samples = uint64_t(n);
+  if (p.q.cv) {
+    double pm = m[1] / n, cm = m[3] / n;
+    double cvar = (m[4] / n) - cm * cm;
+    if (cvar <= 2.220446049250313e-16) {
+      summarize(n, m[1], m[2], &out->price, &out->stderr);
+      return;
+    }
+    double cov = (m[5] / n) - pm * cm;
+    double beta = cov / cvar;
+    double e = p.cv_expectation;
+    double adj = pm - beta * (cm - e);
+    double adj_sq = (m[2] / n) - (2.0 * beta) * ((m[5] / n) - e * pm) +
+                    (beta * beta) * ((m[4] / n) - (2.0 * e * cm) + (e * e));
+    double var = std::max(adj_sq - adj * adj, 0.0);
+    out->price = adj;
+    out->stderr = std::sqrt(var) / std::sqrt(n);
+    return;
+  }
+  summarize(n, m[1], m[2], &out->price, &out->stderr);
+}
+
+// Uploads the sampler tables of `reqs` into one aux buffer and points the descriptors at them.
+static int upload_aux(mpc_context* ctx, std::vector<Prepared*>& reqs) {
+  size_t bytes = 0;
+  for (Prepared* p : reqs) {
+    bytes += p->halton_primes.size() * 4 + 16;
+    bytes += p->halton_shifts.size() * 8 + 16;
+    bytes += p->lhs.size() * sizeof(LhsDim) + 16;
+  }
+  if (bytes <= 48 * reqs.size()) return MPC_OK;
+  void* d_aux = nullptr;
+  int st = scratch(ctx, "aux", bytes, &d_aux);
+  if (st != MPC_OK) return st;
+  std::vector<uint8_t> host(bytes);
+  size_t off = 0;
+  auto place = [&](const void* src, size_t n) -> void* {
+    off = (off + 15) & ~size_t(15);
+    std::memcpy(host.data() + off, src, n);
+    void* dev = static_cast<uint8_t*>(d_aux) + off;
+    off += n;
+    return dev;
+  };
+  for (Prepared* p : reqs) {
+    if (!p->halton_primes.empty()) {
+      p->q.halton_primes = static_cast<const uint32_t*>(place(p->halton_primes.data(), p->halton_primes.size() * 4));
+      p->q.halton_shifts = static_cast<const double*>(place(p->halton_shifts.data(), p->halton_shifts.size() * 8));
+    }
+    if (!p->lhs.empty()) p->q.lhs = static_cast<const LhsDim*>(place(p->lhs.data(), p->lhs.size() * sizeof(LhsDim)));
+  }
+  MPC_CUDA(ctx, cudaMemcpyAsync(d_aux, host.data(), off, cudaMemcpyHostToDevice, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return MPC_OK;
+}
+
+// ------------------------------------------------------------ fused path ---
+int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_result_t*>& outs,
+              double* per_unit_host, uint64_t per_unit_cap) {
+  const size_t n = reqs.size();
+  if (n == 0) return MPC_OK;
+  int st = upload_aux(ctx, reqs);
+  if (st != MPC_OK) return st;
+  // tiles: each request split into tiles of 256 * ppt units
+  std::vector<uint32_t> tile_base(n);
+  uint64_t total_tiles = 0;
+  for (size_t i = 0; i < n; ++i) {
+    Shape s = choose_shape(ctx, *reqs[i]);
+    DevReq& q = reqs[i]->q;
+    q.tile_units = s.block * s.ppt;
+    q.n_tiles = uint32_t((q.n_units + q.tile_units - 1) / q.tile_units);
+    tile_base[i] = uint32_t(total_tiles);
+    total_tiles += q.n_tiles;
+  }
+  if (total_tiles > (1ull << 31)) return fail(ctx, MPC_E_UNSUPPORTED, "batch too large (tiles)");
+  // device buffers
+  void *d_reqs, *d_tiles, *d_part, *d_mom, *d_done, *d_counter, *d_unit = nullptr;
+  size_t groups = 0;
+  if ((st = scratch(ctx, "reqs", n * sizeof(DevReq), &d_reqs))) return st;
+  if ((st = scratch(ctx, "tiles", total_tiles * sizeof(Tile), &d_tiles))) return st;
+  if ((st = scratch(ctx, "partials", total_tiles * MPC_MOMENTS * sizeof(double), &d_part))) return st;
+  if ((st = scratch(ctx, "moments", n * MPC_MOMENTS * sizeof(double), &d_mom))) return st;
+  if ((st = scratch(ctx, "done", n * sizeof(uint32_t), &d_done))) return st;
+  if ((st = scratch(ctx, "counter", 64 * sizeof(uint32_t), &d_counter))) return st;
+  if (per_unit_host) {
+    if ((st = scratch(ctx, "per_unit", per_unit_cap * sizeof(double), &d_unit))) return st;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    DevReq& q = reqs[i]->q;
+    q.partials = static_cast<double*>(d_part) + size_t(tile_base[i]) * MPC_MOMENTS;
+    q.moments = static_cast<double*>(d_mom) + i * MPC_MOMENTS;
+    q.tiles_done = static_cast<uint32_t*>(d_done) + i;
+    q.per_unit = (per_unit_host && i == 0) ? static_cast<double*>(d_unit) : nullptr;
+  }
+  // group by sampler; within a group, tiles ordered by per-tile cost (longest first)
+  struct Group {
+    int sampler, family;
+    std::vector<size_t> members;
+  };
+  std::vector<Group> gl;
+  for (size_t i = 0; i < n; ++i) {
+    Group* g = nullptr;
+    for (Group& x : gl)
+      if (x.sampler == reqs[i]->sampler) g = &x;
+    if (!g) {
+      gl.push_back({reqs[i]->sampler, reqs[i]->family, {}});
+      g = &gl.back();
+    }
+    if (g->family != reqs[i]->family) g->family = -1;
+    g->members.push_back(i);
+  }
+  groups = gl.size();
+  if (groups > 64) return fail(ctx, MPC_E_UNSUPPORTED, "too many sampler groups");
+  size_t desc_bytes = n * sizeof(DevReq);
+  size_t tile_bytes = total_tiles * sizeof(Tile);
+  size_t mom_bytes = n * MPC_MOMENTS * sizeof(double);
+  void* pin = nullptr;
+  if ((st = pinned_staging(ctx, desc_bytes + tile_bytes + mom_bytes + 256, &pin))) return st;
+  uint8_t* hp = static_cast<uint8_t*>(pin);
+  for (size_t i = 0; i < n; ++i) std::memcpy(hp + i * sizeof(DevReq), &reqs[i]->q, sizeof(DevReq));
+  Tile* ht = reinterpret_cast<Tile*>(hp + desc_bytes);
+  std::vector<uint32_t> group_first(groups), group_count(groups);
+  uint64_t cursor = 0;
+  for (size_t g = 0; g < groups; ++g) {
+    std::vector<size_t> order = gl[g].members;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      return double(reqs[a]->q.normals_per_unit + reqs[a]->q.n_steps) * reqs[a]->q.tile_units >
+             double(reqs[b]->q.normals_per_unit + reqs[b]->q.n_steps) * reqs[b]->q.tile_units;
+    });
+    group_first[g] = uint32_t(cursor);
+    for (size_t i : order)
+      for (uint32_t t = 0; t < reqs[i]->q.n_tiles; ++t) ht[cursor++] = Tile{uint32_t(i), t};
+    group_count[g] = uint32_t(cursor - group_first[g]);
+  }
+  double* hm = reinterpret_cast<double*>(hp + desc_bytes + tile_bytes);
+  uint64_t launches_before = kernel_launch_count();
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  MPC_CUDA(ctx, cudaMemcpyAsync(d_reqs, hp, desc_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  MPC_CUDA(ctx, cudaMemcpyAsync(d_tiles, ht, tile_bytes, cudaMemcpyHostToDevice, ctx->stream));
+  MPC_CUDA(ctx, cudaMemsetAsync(d_counter, 0, groups * sizeof(uint32_t), ctx->stream));
+  for (size_t g = 0; g < groups; ++g) {
+    int occ = std::max(1, fused_max_blocks_per_sm(gl[g].family, gl[g].sampler, 256));
+    uint64_t grid = std::min<uint64_t>(uint64_t(ctx->sm_count) * occ, group_count[g]);
+    if (grid < 1) grid = 1;
+    cudaError_t e = launch_fused(static_cast<DevReq*>(d_reqs), static_cast<Tile*>(d_tiles) + group_first[g],
+                                 group_count[g], static_cast<uint32_t*>(d_counter) + g, gl[g].family,
+                                 gl[g].sampler, ctx->tabs, int(grid), 256, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "fused pricing kernel launch");
+  }
+  MPC_CUDA(ctx, cudaMemcpyAsync(hm, d_mom, mom_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  ctx->last_ms = ms;
+  ctx->last_launches = kernel_launch_count() - launches_before;
+  for (size_t i = 0; i < n; ++i) {
+    summarize_moments(*reqs[i], hm + i * MPC_MOMENTS, outs[i]);
+    outs[i]->path_steps = reqs[i]->path_steps;
+    outs[i]->runtime_ms = ms;
+  }
+  if (per_unit_host) {
+    uint64_t count = std::min<uint64_t>(per_unit_cap, reqs[0]->q.n_units);
+    MPC_CUDA(ctx, cudaMemcpy(per_unit_host, d_unit, count * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return MPC_OK;
+}
+
+// ------------------------------------------------------------ plain path ---
+static int run_plain(mpc_context* ctx, Prepared* p, mpc_result_t* out, double* per_unit_host,
+                     uint64_t per_unit_cap) {
+  std::vector<Prepared*> one{p};
+  int st = upload_aux(ctx, one);
+  if (st != MPC_OK) return st;
+  DevReq& q = p->q;
+  const uint64_t units = q.n_units, dims = q.normals_per_unit;
+  void *d_buf, *d_pay, *d_ctl = nullptr, *d_req, *d_part, *d_mom, *d_done;
+  if ((st = scratch(ctx, "plain_buf", units * dims * sizeof(double), &d_buf))) return st;
+  if ((st = scratch(ctx, "plain_pay", units * sizeof(double), &d_pay))) return st;
+  if (q.cv && (st = scratch(ctx, "plain_ctl", units * sizeof(double), &d_ctl))) return st;
+  q.tile_units = 2048;
+  q.n_tiles = uint32_t((units + q.tile_units - 1) / q.tile_units);
+  if ((st = scratch(ctx, "plain_req", sizeof(DevReq), &d_req))) return st;
+  if ((st = scratch(ctx, "plain_part", size_t(q.n_tiles) * MPC_MOMENTS * sizeof(double), &d_part))) return st;
+  if ((st = scratch(ctx, "plain_mom", MPC_MOMENTS * sizeof(double), &d_mom))) return st;
+  if ((st = scratch(ctx, "plain_done", 16, &d_done))) return st;
+  q.partials = static_cast<double*>(d_part);
+  q.moments = static_cast<double*>(d_mom);
+  q.tiles_done = static_cast<uint32_t*>(d_done);
+  q.per_unit = nullptr;
+  void* pin = nullptr;
+  if ((st = pinned_staging(ctx, sizeof(DevReq) + MPC_MOMENTS * sizeof(double), &pin))) return st;
+  std::memcpy(pin, &q, sizeof(DevReq));
+  double* hm = reinterpret_cast<double*>(static_cast<uint8_t*>(pin) + sizeof(DevReq));
+  uint64_t launches_before = kernel_launch_count();
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  MPC_CUDA(ctx, cudaMemcpyAsync(d_req, pin, sizeof(DevReq), cudaMemcpyHostToDevice, ctx->stream));
+  MPC_CUDA(ctx, cudaMemsetAsync(d_done, 0, 16, ctx->stream));
+  cudaError_t e = launch_plain_generate(q, static_cast<double*>(d_buf), p->sampler, ctx->tabs, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "plain sample generation");
+  e = launch_plain_simulate(q, static_cast<DevReq*>(d_req), static_cast<double*>(d_buf), static_cast<double*>(d_pay),
+                            static_cast<double*>(d_ctl), ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "plain path simulation");
+  e = launch_plain_reduce(static_cast<DevReq*>(d_req), static_cast<double*>(d_pay), static_cast<double*>(d_ctl), units,
+                          q.n_tiles, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "plain reduction");
+  MPC_CUDA(ctx, cudaMemcpyAsync(hm, d_mom, MPC_MOMENTS * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  ctx->last_ms = ms;
+  ctx->last_launches = kernel_launch_count() - launches_before;
+  summarize_moments(*p, hm, out);
+  out->path_steps = p->path_steps;
+  out->runtime_ms = ms;
+  if (per_unit_host) {
+    uint64_t count = std::min<uint64_t>(per_unit_cap, units);
+    MPC_CUDA(ctx, cudaMemcpy(per_unit_host, d_pay, count * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return MPC_OK;
+}
+
+// ------------------------------------------------------------------- LSM ---
+static double powi(double a, int b) {  // f64::powi as compiler-rt __powidf2
+  bool recip = b < 0;
+  double r = 1.0;
+  for (;;) {
+    if (b & 1) r *= a;
+    b /= 2;
+    if (b == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0 / r : r;
+}
+
+static int run_lsm(mpc_context* ctx, const mpc_request_t& r, mpc_result_t* out, double* per_unit_host) {
+  (void)per_unit_host;
+  const uint32_t degree = std::min<uint32_t>(std::max<uint32_t>(r.basis_degree, 1), 3);
+  std::vector<uint32_t> sched;
+  bool normalised = false;
+  if (r.workload == MPC_WORKLOAD_AMERICAN_PUT) {
+    for (uint32_t s = 1; s <= r.n_steps; ++s) sched.push_back(s);
+  } else {  // normalize_bermudan_exercise_schedule (cpu.rs:5155-5183)
+    std::vector<uint32_t> in(r.exercise_steps, r.exercise_steps + r.n_exercise);
+    sched = in;
+    std::sort(sched.begin(), sched.end());
+    sched.erase(std::unique(sched.begin(), sched.end()), sched.end());
+    if (sched != in) normalised = true;
+    if (std::find(sched.begin(), sched.end(), r.n_steps) == sched.end()) {
+      sched.push_back(r.n_steps);
+      normalised = true;
+    }
+  }
+  const bool fp64 = r.precision == MPC_PRECISION_FP64_PLAIN;
+  const double dt = r.t / double(r.n_steps);
+  std::vector<double> disc_pow(r.n_steps + 1);
+  const double disc_step = std::exp(-r.r * dt);
+  for (uint32_t j = 0; j <= r.n_steps; ++j) disc_pow[j] = powi(disc_step, int(j));
+  void *d_paths, *d_sched, *d_disc, *d_part, *d_fpart, *d_out, *d_bar;
+  int st;
+  const size_t elem = fp64 ? 8 : 4;
+  if ((st = scratch(ctx, "lsm_paths", r.n_paths * r.n_steps * elem, &d_paths))) return st;
+  if ((st = scratch(ctx, "lsm_sched", sched.size() * 4, &d_sched))) return st;
+  if ((st = scratch(ctx, "lsm_disc", disc_pow.size() * 8, &d_disc))) return st;
+  if ((st = scratch(ctx, "lsm_part", 2 * 16384 * 16 * 8, &d_part))) return st;
+  if ((st = scratch(ctx, "lsm_fpart", 16384 * 4 * 8, &d_fpart))) return st;
+  if ((st = scratch(ctx, "lsm_out", 8 * 8, &d_out))) return st;
+  if ((st = scratch(ctx, "lsm_bar", 64, &d_bar))) return st;
+  LsmArgs a{};
+  a.n_paths = r.n_paths;
+  a.n_steps = r.n_steps;
+  a.n_sched = uint32_t(sched.size());
+  a.degree = degree;
+  a.sampler = uint32_t(sampler_of(r.sampling));
+  a.seed = r.seed;
+  a.seed32 = uint32_t(r.seed);
+  a.fp64 = fp64 ? 1 : 0;
+  a.s0 = r.s0;
+  a.k = r.k;
+  a.drift = (r.r - 0.5 * r.sigma * r.sigma) * dt;
+  a.vol = r.sigma * std::sqrt(dt);
+  a.disc_step = disc_step;
+  a.sched = static_cast<uint32_t*>(d_sched);
+  a.disc_pow = static_cast<double*>(d_disc);
+  a.paths = d_paths;
+  a.partials = static_cast<double*>(d_part);
+  a.final_partials = static_cast<double*>(d_fpart);
+  a.out = static_cast<double*>(d_out);
+  a.barrier = static_cast<unsigned*>(d_bar);
+  a.done = static_cast<unsigned*>(d_bar) + 4;
+  a.error = reinterpret_cast<int*>(static_cast<unsigned*>(d_bar) + 8);
+  a.timeout_ns = 2000000000ull;
+  void* pin = nullptr;
+  if ((st = pinned_staging(ctx, 256, &pin))) return st;
+  double* hout = static_cast<double*>(pin);
+  int* herr = reinterpret_cast<int*>(hout + 8);
+  uint64_t launches_before = kernel_launch_count();
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  MPC_CUDA(ctx, cudaMemcpyAsync(d_sched, sched.data(), sched.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+  MPC_CUDA(ctx, cudaMemcpyAsync(d_disc, disc_pow.data(), disc_pow.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  MPC_CUDA(ctx, cudaMemsetAsync(d_bar, 0, 64, ctx->stream));
+  int grid = 0;
+  cudaError_t e = launch_lsm(a, ctx->tabs, &grid, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "LSM cooperative launch");
+  MPC_CUDA(ctx, cudaMemcpyAsync(hout, d_out, 8 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaMemcpyAsync(herr, a.error, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  ctx->last_ms = ms;
+  ctx->last_launches = kernel_launch_count() - launches_before;
+  if (*herr != 0) return fail(ctx, MPC_E_TIMEOUT, "LSM grid barrier timed out");
+  double price, se;
+  summarize(hout[0], hout[1], hout[2], &price, &se);
+  uint32_t warnings = 0;
+  if (r.workload == MPC_WORKLOAD_AMERICAN_PUT) {  // intrinsic floor (cpu.rs:3919-3925)
+    double intrinsic = std::max(r.k - r.s0, 0.0);
+    if (intrinsic > price) {
+      price = intrinsic;
+      se = 0.0;
+      warnings |= MPC_WARN_INTRINSIC_FLOOR;
+    }
+  }
+  if (r.basis_degree != degree) warnings |= MPC_WARN_BASIS_DEGREE_CLAMPED;
+  if (normalised) warnings |= MPC_WARN_SCHEDULE_NORMALISED;
+  if (r.n_threads > 1) warnings |= MPC_WARN_THREADS_IGNORED;
+  out->price = price;
+  out->stderr = se;
+  out->n_samples = r.n_paths;
+  out->path_steps = r.n_paths * r.n_steps;
+  out->moments[0] = hout[0];
+  out->moments[1] = hout[1];
+  out->moments[2] = hout[2];
+  out->early_exercise_count = uint64_t(hout[3]);
+  out->maturity_exercise_count = uint64_t(hout[4]);
+  out->regression_steps = uint32_t(hout[5]);
+  out->basis_degree = degree;
+  out->warnings |= warnings;
+  out->runtime_ms = ms;
+  return MPC_OK;
+}
+
+// ------------------------------------------------------------------ MLMC ---
+static uint64_t fine_steps(const mpc_request_t& r, uint32_t level) {
+  uint64_t s = r.base_steps;
+  for (uint32_t l = 0; l < level; ++l) s *= r.refinement_factor;
+  return s;
+}
+
+// One MLMC level as a pricing unit family (simulate_asian_mlmc_level, cpu.rs:6641-6773).
+static void level_request(const mpc_request_t& r, uint64_t seed, uint32_t level, uint64_t paths, Prepared* p) {
+  *p = Prepared();
+  DevReq& q = p->q;
+  std::memset(&q, 0, sizeof(q));
+  const uint64_t fine = fine_steps(r, level);
+  const uint64_t level_seed = derive_chunk_seed(seed, level);
+  p->sampler = sampler_of(r.sampling);
+  p->family = FAM_MLMC_LEVEL;
+  p->plain = r.precision == MPC_PRECISION_FP64_PLAIN;
+  q.family = FAM_MLMC_LEVEL;
+  q.workload = MPC_WORKLOAD_ASIAN_MLMC;
+  q.seed = level_seed;
+  q.seed32 = uint32_t(level_seed);
+  q.n_chunks = 1;
+  q.n_paths = paths;
+  q.n_units = paths;
+  q.n_steps = uint32_t(fine);
+  q.normals_per_unit = fine;
+  q.level = level;
+  q.refinement = r.refinement_factor;
+  q.s0 = r.s0;
+  q.k = r.k;
+  q.log_s0 = std::log(r.s0);
+  q.discount = std::exp(-r.r * r.t);
+  double fdt = r.t / double(fine);
+  q.f_drift = (r.r - 0.5 * r.sigma * r.sigma) * fdt;
+  q.f_vol = r.sigma * std::sqrt(fdt);
+  q.inv_fine = 1.0 / double(fine);
+  if (level > 0) {
+    q.coarse_steps = fine / r.refinement_factor;
+    double cdt = r.t / double(q.coarse_steps);
+    q.c_drift = (r.r - 0.5 * r.sigma * r.sigma) * cdt;
+    q.c_vol = r.sigma * std::sqrt(cdt);
+    q.inv_sqrt_m = 1.0 / std::sqrt(double(r.refinement_factor));
+    q.inv_coarse = 1.0 / double(q.coarse_steps);
+  }
+  p->path_steps = paths * (fine + (level > 0 ? fine / r.refinement_factor : 0));
+  build_sampler_tables(p, level_seed, paths, fine);
+}
+
+// Runs all levels of one replicate; returns per-level (mean, variance) and cost.
+static int run_levels(mpc_context* ctx, const mpc_request_t& r, uint64_t seed, const std::vector<uint64_t>& paths,
+                      std::vector<double>* mean, std::vector<double>* var, double* device_ms) {
+  const uint32_t L = r.levels;
+  std::vector<Prepared> preps(L);
+  std::vector<mpc_result_t> res(L);
+  mean->assign(L, 0.0);
+  var->assign(L, 0.0);
+  for (uint32_t l = 0; l < L; ++l) level_request(r, seed, l, paths[l], &preps[l]);
+  if (r.precision == MPC_PRECISION_FP64_PLAIN) {
+    for (uint32_t l = 0; l < L; ++l) {
+      std::memset(&res[l], 0, sizeof(res[l]));
+      int st = run_plain(ctx, &preps[l], &res[l], nullptr, 0);
+      if (st != MPC_OK) return st;
+      *device_ms += ctx->last_ms;
+    }
+  } else {
+    std::vector<Prepared*> pp;
+    std::vector<mpc_result_t*> oo;
+    for (uint32_t l = 0; l < L; ++l) {
+      std::memset(&res[l], 0, sizeof(res[l]));
+      pp.push_back(&preps[l]);
+      oo.push_back(&res[l]);
+    }
+    int st = run_fused(ctx, pp, oo, nullptr, 0);
+    if (st != MPC_OK) return st;
+    *device_ms += ctx->last_ms;
+  }
+  for (uint32_t l = 0; l < L; ++l) {
+    double nn = res[l].moments[0];
+    double m = res[l].moments[1] / nn;
+    (*mean)[l] = m;
+    (*var)[l] = (res[l].moments[2] / nn) - m * m;
+  }
+  return MPC_OK;
+}
+
+// arithmetic_asian_call_price_mlmc_{single,replicated}_cpu (cpu.rs:3612-3751)
+// with solve_arithmetic_asian_mlmc_tolerance_cpu (cpu.rs:3352-3423) when
+// target_stderr > 0.  Level variances and the allocation are FP64 on the host.
+static int run_mlmc(mpc_context* ctx, const mpc_request_t& r_in, mpc_result_t* out) {
+  mpc_request_t r = r_in;
+  const uint32_t L = r.levels;
+  const bool pseudo = r.sampling == MPC_SAMPLING_PSEUDORANDOM || r.sampling == MPC_SAMPLING_COUNTER_HASH;
+  const uint64_t reps = pseudo ? 1 : std::max<uint32_t>(r.scramble_replicates, 1);
+  double device_ms = 0.0;
+  uint64_t launches_before = kernel_launch_count();
+  auto cost = [&](uint32_t l) { return fine_steps(r, l) + (l == 0 ? 0 : fine_steps(r, l) / r.refinement_factor); };
+  if (r.target_stderr > 0.0) {
+    std::vector<uint64_t> pilot(L, r.pilot_paths_per_level);
+    std::vector<double> pm, pv;
+    int st = run_levels(ctx, r, r.seed, pilot, &pm, &pv, &device_ms);
+    if (st != MPC_OK) return st;
+    for (uint32_t l = 0; l < L; ++l) pv[l] = std::max(pv[l], 1.0e-18);
+    auto allocate = [&](double target_variance, bool by_budget, uint64_t budget, std::vector<uint64_t>& paths) {
+      double denom = 0.0;
+      for (uint32_t l = 0; l < L; ++l) denom += std::sqrt(pv[l] * double(cost(l)));
+      uint64_t total = 0;
+      for (uint32_t l = 0; l < L; ++l) {
+        double w = std::sqrt(pv[l] / double(cost(l)));
+        double raw = by_budget ? std::ceil(double(budget) * w / denom) : std::ceil(denom * w / target_variance);
+        paths[l] = std::max<uint64_t>(uint64_t(raw), 2);
+        total += paths[l] * cost(l);
+      }
+      return total;
+    };
+    auto est_se = [&](const std::vector<uint64_t>& paths) {
+      double v = 0.0;
+      for (uint32_t l = 0; l < L; ++l) v += pv[l] / double(paths[l]);
+      return std::sqrt(v / double(reps));
+    };
+    std::vector<uint64_t> paths(L);
+    uint64_t updates = allocate(r.target_stderr * r.target_stderr * double(reps), false, 0, paths) * reps;
+    double est = est_se(paths);
+    if (updates < r.min_step_updates) {
+      uint64_t per = std::max<uint64_t>((r.min_step_updates + reps - 1) / reps, 1);
+      updates = allocate(0, true, per, paths) * reps;
+      est = est_se(paths);
+    }
+    bool hit = false;
+    if (updates > r.max_step_updates) {
+      hit = true;
+      uint64_t per = std::max<uint64_t>(r.max_step_updates / reps, 1);
+      updates = allocate(0, true, per, paths) * reps;
+      est = est_se(paths);
+    }
+    for (uint32_t l = 0; l < L; ++l) r.paths_per_level[l] = paths[l];
+    out->estimated_stderr = est;
+    out->target_met = (est <= r.target_stderr && updates <= r.max_step_updates) ? 1 : 0;
+    out->max_step_updates_hit = hit ? 1 : 0;
+  }
+  std::vector<uint64_t> paths(r.paths_per_level, r.paths_per_level + L);
+  std::vector<double> rep_price(reps);
+  std::vector<std::vector<double>> lmean(reps), lvar(reps);
+  double single_se = 0.0;
+  uint64_t total_paths = 0, total_updates = 0;
+  for (uint64_t rep = 0; rep < reps; ++rep) {
+    uint64_t seed = reps > 1 ? derive_chunk_seed(r.seed, rep) : r.seed;
+    int st = run_levels(ctx, r, seed, paths, &lmean[rep], &lvar[rep], &device_ms);
+    if (st != MPC_OK) return st;
+    double price = 0.0, varc = 0.0;
+    for (uint32_t l = 0; l < L; ++l) {
+      lvar[rep][l] = std::max(lvar[rep][l], 0.0);
+      price += lmean[rep][l];
+      varc += lvar[rep][l] / double(paths[l]);
+      total_paths += paths[l];
+      total_updates += paths[l] * cost(l);
+    }
+    rep_price[rep] = price;
+    single_se = std::sqrt(varc);
+  }
+  double price = 0.0;
+  for (double p : rep_price) price += p;
+  price /= double(reps);
+  double se = single_se;
+  if (reps > 1) {
+    double sv = 0.0;
+    for (double p : rep_price) sv += (p - price) * (p - price);
+    sv /= double(reps - 1);
+    se = std::sqrt(sv / double(reps));
+  }
+  out->price = price;
+  out->stderr = se;
+  out->n_levels = L;
+  out->total_paths = total_paths;
+  out->total_step_updates = total_updates;
+  out->path_steps = total_updates;
+  for (uint32_t l = 0; l < L; ++l) {
+    double mean = 0.0;
+    for (uint64_t rep = 0; rep < reps; ++rep) mean += lmean[rep][l];
+    mean /= double(reps);
+    double var = lvar[0][l];
+    if (reps > 1) {
+      var = 0.0;
+      for (uint64_t rep = 0; rep < reps; ++rep) var += (lmean[rep][l] - mean) * (lmean[rep][l] - mean);
+      var /= double(reps - 1);
+    }
+    out->level_mean[l] = mean;
+    out->level_variance[l] = var;
+    out->level_paths[l] = paths[l] * reps;
+    out->level_fine_steps[l] = fine_steps(r, l);
+  }
+  out->runtime_ms = device_ms;
+  ctx->last_ms = device_ms;
+  ctx->last_launches = kernel_launch_count() - launches_before;
+  return MPC_OK;
+}
+
+static int price_one(mpc_context* ctx, const mpc_request_t* req, mpc_result_t* out, double* per_unit,
+                     uint64_t cap) {
+  std::memset(out, 0, sizeof(*out));
+  std::string msg;
+  int st = validate(*req, &msg);
+  if (st != MPC_OK) {
+    out->status = st;
+    return fail(ctx, st, msg);
+  }
+  if (req->workload == MPC_WORKLOAD_ASIAN_MLMC) {
+    st = run_mlmc(ctx, *req, out);
+  } else if (is_lsm(req->workload)) {
+    st = run_lsm(ctx, *req, out, per_unit);
+  } else {
+    Prepared p;
+    st = prepare(ctx, *req, &p, &msg);
+    if (st != MPC_OK) {
+      out->status = st;
+      return fail(ctx, st, msg);
+    }
+    if (p.plain) {
+      st = run_plain(ctx, &p, out, per_unit, cap);
+    } else {
+      std::vector<Prepared*> pp{&p};
+      std::vector<mpc_result_t*> oo{out};
+      st = run_fused(ctx, pp, oo, per_unit, cap);
+    }
+  }
+  out->status = st;
+  return st;
+}
+
+// ----------------------------------------------------------- device setup ---
+static void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {
+  sob.assign(size_t(MPC_SOBOL_TABLE_DIMS) * 8 * 16, 0u);
+  for (int d = 0; d < MPC_SOBOL_TABLE_DIMS; ++d)
+    for (int q = 0; q < 8; ++q)
+      for (int v = 0; v < 16; ++v) {
+        uint32_t x = 0;
+        for (int j = 0; j < 4; ++j)
+          if ((v >> j) & 1) x ^= kSobolDirections[d][4 * q + j];
+        sob[(size_t(d) * 8 + q) * 16 + v] = x;
+      }
+  // Columns of the xorshift64* transition T (image of each basis vector), then T^(2^b).
+  auto step = [](uint64_t x) {
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    return x;
+  };
+  std::vector<uint64_t> M(64), N(64);
+  for (int i = 0; i < 64; ++i) M[i] = step(1ull << i);
+  auto apply = [](const std::vector<uint64_t>& m, uint64_t x) {
+    uint64_t y = 0;
+    for (int i = 0; i < 64; ++i)
+      if ((x >> i) & 1) y ^= m[i];
+    return y;
+  };
+  jump.assign(64 * 256, 0ull);
+  for (int b = 0; b < 64; ++b) {
+    for (int q = 0; q < 16; ++q)
+      for (int v = 0; v < 16; ++v) {
+        uint64_t y = 0;
+        for (int j = 0; j < 4; ++j)
+          if ((v >> j) & 1) y ^= M[4 * q + j];
+        jump[size_t(b) * 256 + q * 16 + v] = y;
+      }
+    for (int i = 0; i < 64; ++i) N[i] = apply(M, M[i]);  // M <- M * M
+    M.swap(N);
+  }
+}
+
+}  // namespace mpc
+
+// ======================================================= C entry points ====
+extern "C" {
+
+int mpc_abi_version(void) { return MPC_ABI_VERSION; }
+
+size_t mpc_struct_size(int which) {
+  switch (which) {
+    case 0:
+      return sizeof(mpc_request_t);
+    case 1:
+      return sizeof(mpc_result_t);
+    case 2:
+      return sizeof(mpc_device_info_t);
+    case 3:
+      return sizeof(mpc_options_t);
+    case 4:
+      return sizeof(mpc_support_t);
+    case 5:
+      return sizeof(mpc_artifact_t);
+    case 6:
+      return sizeof(mpc_server_options_t);
+    case 7:
+      return sizeof(mpc_server_stats_t);
+    default:
+      return 0;
+  }
+}
+
+const char* mpc_status_string(int status) {
+  switch (status) {
+    case MPC_OK:
+      return "MPC_OK";
+    case MPC_E_INVALID_CONFIG:
+      return "MPC_E_INVALID_CONFIG";
+    case MPC_E_UNSUPPORTED:
+      return "MPC_E_UNSUPPORTED";
+    case MPC_E_NO_DEVICE:
+      return "MPC_E_NO_DEVICE";
+    case MPC_E_OOM_BUDGET:
+      return "MPC_E_OOM_BUDGET";
+    case MPC_E_TIMEOUT:
+      return "MPC_E_TIMEOUT";
+    case MPC_E_CUDA:
+      return "MPC_E_CUDA";
+    case MPC_E_BUSY:
+      return "MPC_E_BUSY";
+    case MPC_E_NOT_FOUND:
+      return "MPC_E_NOT_FOUND";
+    case MPC_E_CANCELLED:
+      return "MPC_E_CANCELLED";
+    default:
+      return "MPC_E_UNKNOWN";
+  }
+}
+
+int mpc_device_count(int* count) {
+  if (!count) return MPC_E_INVALID_CONFIG;
+  int n = 0;
+  cudaError_t err = cudaGetDeviceCount(&n);
+  if (err != cudaSuccess) {
+    *count = 0;
+    return MPC_E_NO_DEVICE;
+  }
+  *count = n;
+  return MPC_OK;
+}
+
+int mpc_device_info(int index, mpc_device_info_t* info) {
+  if (!info) return MPC_E_INVALID_CONFIG;
+  std::memset(info, 0, sizeof(*info));
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || index < 0 || index >= n) return MPC_E_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, index) != cudaSuccess) return MPC_E_NO_DEVICE;
+  info->index = index;
+  info->sm_count = prop.multiProcessorCount;
+  info->cc_major = prop.major;
+  info->cc_minor = prop.minor;
+  info->total_memory_bytes = prop.totalGlobalMem;
+  int clk = 0;
+  cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, index);
+  info->clock_khz = clk;
+  info->l2_bytes = prop.l2CacheSize;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  size_t free_b = 0, total_b = 0;
+  if (cudaSetDevice(index) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+    info->free_memory_bytes = free_b;
+  cudaSetDevice(cur);
+  std::snprintf(info->name, sizeof(info->name), "%s", prop.name);
+  return MPC_OK;
+}
+
+// Rust `Default` impls of the configs (cpu.rs:1311-1815).
+int mpc_request_defaults(mpc_request_t* r, int workload) {
+  if (!r) return MPC_E_INVALID_CONFIG;
+  std::memset(r, 0, sizeof(*r));
+  r->workload = workload;
+  r->model = MPC_MODEL_GBM;
+  r->method = MPC_METHOD_AUTO;
+  r->technique = MPC_TECHNIQUE_STANDARD;
+  r->sampling = MPC_SAMPLING_PSEUDORANDOM;
+  r->precision = MPC_PRECISION_FP32_PATH;
+  r->n_paths = 100000;
+  r->n_steps = 252;
+  r->seed = 42;
+  r->s0 = 100.0;
+  r->k = 100.0;
+  r->r = 0.03;
+  r->sigma = 0.2;
+  r->t = 1.0;
+  r->v0 = 0.04;
+  r->kappa = 1.5;
+  r->theta = 0.04;
+  r->vol_of_vol = 0.3;
+  r->rho = -0.6;
+  r->jump_intensity = 0.4;
+  r->jump_mean = -0.08;
+  r->jump_volatility = 0.25;
+  r->n_assets = 2;
+  r->spots[0] = 100.0;
+  r->spots[1] = 95.0;
+  r->sigmas[0] = 0.2;
+  r->sigmas[1] = 0.25;
+  r->weights[0] = 0.5;
+  r->weights[1] = 0.5;
+  r->corr[0] = 1.0;
+  r->corr[1] = 0.35;
+  r->corr[2] = 0.35;
+  r->corr[3] = 1.0;
+  r->basis_degree = 2;
+  r->base_steps = 16;
+  r->levels = 4;
+  r->refinement_factor = 2;
+  r->scramble_replicates = 1;
+  r->paths_per_level[0] = 50000;
+  r->paths_per_level[1] = 25000;
+  r->paths_per_level[2] = 12500;
+  r->paths_per_level[3] = 6250;
+  r->pilot_paths_per_level = 2048;
+  r->min_step_updates = 100000;
+  r->max_step_updates = 10000000;
+  switch (workload) {
+    case MPC_WORKLOAD_DOWN_AND_OUT_CALL:
+      r->barrier = 80.0;
+      break;
+    case MPC_WORKLOAD_UP_AND_OUT_CALL:
+      r->barrier = 120.0;
+      break;
+    case MPC_WORKLOAD_AMERICAN_PUT:
+      r->n_steps = 64;
+      break;
+    case MPC_WORKLOAD_BERMUDAN_PUT:
+      r->n_steps = 64;
+      r->n_exercise = 4;
+      r->exercise_steps[0] = 16;
+      r->exercise_steps[1] = 32;
+      r->exercise_steps[2] = 48;
+      r->exercise_steps[3] = 64;
+      break;
+    case MPC_WORKLOAD_BASKET_CALL:
+      r->method = MPC_METHOD_TERMINAL;
+      r->n_steps = 1;
+      break;
+    default:
+      break;
+  }
+  if (workload < 0 || workload > MPC_WORKLOAD_ASIAN_MLMC) return MPC_E_INVALID_CONFIG;
+  return MPC_OK;
+}
+
+int mpc_validate(const mpc_request_t* req, char* message, size_t message_len) {
+  if (!req) return MPC_E_INVALID_CONFIG;
+  std::string msg;
+  int st = validate(*req, &msg);
+  if (message && message_len) std::snprintf(message, message_len, "%s", msg.c_str());
+  return st;
+}
+
+int mpc_supports(const mpc_request_t* req, mpc_support_t* out) {
+  if (!req || !out) return MPC_E_INVALID_CONFIG;
+  std::memset(out, 0, sizeof(*out));
+  std::string msg;
+  int st = validate(*req, &msg);
+  out->supported = st == MPC_OK ? 1 : 0;
+  out->reason = st;
+  out->estimated_bytes = estimate_bytes(*req);
+  std::snprintf(out->message, sizeof(out->message), "%s",
+                st == MPC_OK ? "native CUDA execution on sm_100a" : msg.c_str());
+  return MPC_OK;
+}
+
+int mpc_estimate_bytes(const mpc_request_t* req, uint64_t* bytes) {
+  if (!req || !bytes) return MPC_E_INVALID_CONFIG;
+  *bytes = estimate_bytes(*req);
+  return MPC_OK;
+}
+
+int mpc_create(const mpc_options_t* options, mpc_context_t** out) {
+  if (!out) return MPC_E_INVALID_CONFIG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return MPC_E_NO_DEVICE;
+  mpc_context* ctx = new mpc_context();
+  ctx->device = options ? options->device : 0;
+  if (ctx->device < 0 || ctx->device >= n) {
+    delete ctx;
+    return MPC_E_NO_DEVICE;
+  }
+  ctx->budget = (options && options->hbm_budget_bytes) ? options->hbm_budget_bytes : (64ull << 30);
+  auto bail = [&](cudaError_t e, const char* what) {
+    std::fprintf(stderr, "montepath_cuda: %s failed: %s\n", what, cudaGetErrorString(e));
+    delete ctx;
+    return e == cudaErrorMemoryAllocation ? MPC_E_OOM_BUDGET : MPC_E_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaSetDevice(ctx->device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return bail(e, "cudaStreamCreate");
+  cudaEventCreate(&ctx->ev_start);
+  cudaEventCreate(&ctx->ev_stop);
+  std::vector<uint32_t> sob;
+  std::vector<uint64_t> jump;
+  build_tables(sob, jump);
+  if ((e = cudaMalloc(&ctx->d_sobol, sob.size() * 4)) != cudaSuccess) return bail(e, "cudaMalloc tables");
+  if ((e = cudaMalloc(&ctx->d_jump, jump.size() * 8)) != cudaSuccess) return bail(e, "cudaMalloc tables");
+  cudaMemcpy(ctx->d_sobol, sob.data(), sob.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(ctx->d_jump, jump.data(), jump.size() * 8, cudaMemcpyHostToDevice);
+  ctx->live_bytes = sob.size() * 4 + jump.size() * 8;
+  ctx->tabs.sobol = static_cast<const uint32_t*>(ctx->d_sobol);
+  ctx->tabs.jump = static_cast<const uint64_t*>(ctx->d_jump);
+  *out = ctx;
+  return MPC_OK;
+}
+
+int mpc_destroy(mpc_context_t* ctx) {
+  if (!ctx) return MPC_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  for (auto& kv : ctx->bufs)
+    if (kv.second.ptr) cudaFree(kv.second.ptr);
+  if (ctx->d_sobol) cudaFree(ctx->d_sobol);
+  if (ctx->d_jump) cudaFree(ctx->d_jump);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return MPC_OK;
+}
+
+const char* mpc_last_error_message(const mpc_context_t* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int mpc_prepare(mpc_context_t* ctx, const mpc_request_t* req, mpc_artifact_t* out) {
+  if (!ctx || !req || !out) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  std::memset(out, 0, sizeof(*out));
+  std::string msg;
+  if (req->workload == MPC_WORKLOAD_ASIAN_MLMC || is_lsm(req->workload)) {
+    int st = validate(*req, &msg);
+    if (st != MPC_OK) return fail(ctx, st, msg);
+    out->kernel_family = is_lsm(req->workload) ? 100 : FAM_MLMC_LEVEL;
+    out->block_size = 256;
+    out->paths_per_thread = 1;
+    out->bytes = estimate_bytes(*req);
+    std::snprintf(out->name, sizeof(out->name), "%s", is_lsm(req->workload) ? "lsm_cooperative" : "mlmc_levels");
+    return MPC_OK;
+  }
+  Prepared p;
+  int st = prepare(ctx, *req, &p, &msg);
+  if (st != MPC_OK) return fail(ctx, st, msg);
+  Shape s = choose_shape(ctx, p);
+  out->kernel_family = p.family;
+  out->block_size = s.block;
+  out->paths_per_thread = s.ppt;
+  out->tiles = uint32_t((p.q.n_units + s.block * s.ppt - 1) / (s.block * s.ppt));
+  out->bytes = estimate_bytes(*req);
+  std::snprintf(out->name, sizeof(out->name), "%s_family%d_sampler%d", p.plain ? "plain_fp64" : "fused_fp32",
+                p.family, p.sampler);
+  return MPC_OK;
+}
+
+int mpc_price(mpc_context_t* ctx, const mpc_request_t* req, mpc_result_t* out) {
+  if (!ctx || !req || !out) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  return price_one(ctx, req, out, nullptr, 0);
+}
+
+int mpc_price_paths(mpc_context_t* ctx, const mpc_request_t* req, double* host_payoffs, uint64_t capacity) {
+  if (!ctx || !req || !host_payoffs) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  if (req->workload == MPC_WORKLOAD_ASIAN_MLMC || is_lsm(req->workload))
+    return fail(ctx, MPC_E_UNSUPPORTED, "per-path payoffs are available for path-payoff workloads");
+  mpc_result_t tmp;
+  return price_one(ctx, req, &tmp, host_payoffs, capacity);
+}
+
+int mpc_price_batch(mpc_context_t* ctx, const mpc_request_t* reqs, size_t n, mpc_result_t* out) {
+  if (!ctx || (!reqs && n) || (!out && n)) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  std::vector<Prepared> preps(n);
+  std::vector<Prepared*> fused;
+  std::vector<mpc_result_t*> fused_out;
+  int first_error = MPC_OK;
+  double total_ms = 0.0;
+  uint64_t launches_before = kernel_launch_count();
+  for (size_t i = 0; i < n; ++i) {
+    std::memset(&out[i], 0, sizeof(out[i]));
+    std::string msg;
+    int st = validate(reqs[i], &msg);
+    if (st == MPC_OK && reqs[i].workload != MPC_WORKLOAD_ASIAN_MLMC && !is_lsm(reqs[i].workload)) {
+      st = prepare(ctx, reqs[i], &preps[i], &msg);
+      if (st == MPC_OK && !preps[i].plain) {
+        fused.push_back(&preps[i]);
+        fused_out.push_back(&out[i]);
+        continue;
+      }
+    }
+    if (st != MPC_OK) {
+      out[i].status = st;
+      if (first_error == MPC_OK) {
+        first_error = st;
+        ctx->last_error = msg;
+      }
+      continue;
+    }
+    // FP64-plain, LSM and MLMC requests run one launch sequence each
+    st = price_one(ctx, &reqs[i], &out[i], nullptr, 0);
+    total_ms += ctx->last_ms;
+    if (st != MPC_OK && first_error == MPC_OK) first_error = st;
+  }
+  if (!fused.empty()) {
+    int st = run_fused(ctx, fused, fused_out, nullptr, 0);
+    total_ms += ctx->last_ms;
+    for (mpc_result_t* o : fused_out) o->status = st;
+    if (st != MPC_OK && first_error == MPC_OK) first_error = st;
+  }
+  ctx->last_ms = total_ms;
+  ctx->last_launches = kernel_launch_count() - launches_before;
+  return first_error;
+}
+
+int mpc_generate_normals(mpc_context_t* ctx, int sampling, uint64_t seed, uint64_t n_points, uint32_t dimensions,
+                         int precision, void* host_out) {
+  if (!ctx || !host_out || n_points == 0 || dimensions == 0) return MPC_E_INVALID_CONFIG;
+  if (sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE)
+    return fail(ctx, MPC_E_UNSUPPORTED, "bridge ordering applies to paths, not raw normals");
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  Prepared p;
+  DevReq& q = p.q;
+  std::memset(&q, 0, sizeof(q));
+  p.sampler = sampler_of(sampling);
+  q.seed = seed;
+  q.seed32 = uint32_t(seed);
+  q.n_paths = n_points;
+  q.n_units = n_points;
+  q.n_chunks = 1;
+  q.normals_per_unit = dimensions;  // the reference generator is one stream over point-major normals
+  build_sampler_tables(&p, seed, n_points, dimensions);
+  std::vector<Prepared*> one{&p};
+  int st = upload_aux(ctx, one);
+  if (st != MPC_OK) return st;
+  const size_t elem = precision == MPC_PRECISION_FP32_PATH ? 4 : 8;
+  void* d_out = nullptr;
+  if ((st = scratch(ctx, "gen_out", n_points * dimensions * elem, &d_out))) return st;
+  cudaError_t e = launch_generate_normals(q, p.sampler, precision == MPC_PRECISION_FP32_PATH, d_out, n_points,
+                                          dimensions, ctx->tabs, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "generate normals");
+  MPC_CUDA(ctx, cudaMemcpyAsync(host_out, d_out, n_points * dimensions * elem, cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return MPC_OK;
+}
+
+int mpc_counter_hash_u32(mpc_context_t* ctx, uint32_t seed, uint32_t n_paths, uint32_t n_steps, uint32_t* host_out) {
+  if (!ctx || !host_out) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  size_t bytes = size_t(n_paths) * n_steps * 2 * 4;
+  void* d = nullptr;
+  int st = scratch(ctx, "gen_out", bytes, &d);
+  if (st != MPC_OK) return st;
+  cudaError_t e = launch_counter_hash(seed, n_paths, n_steps, static_cast<uint32_t*>(d), ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "counter hash");
+  MPC_CUDA(ctx, cudaMemcpyAsync(host_out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return MPC_OK;
+}
+
+int mpc_xorshift_u64(mpc_context_t* ctx, uint64_t seed, uint64_t offset, uint64_t count, uint64_t* host_out) {
+  if (!ctx || !host_out) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  void* d = nullptr;
+  int st = scratch(ctx, "gen_out", count * 8, &d);
+  if (st != MPC_OK) return st;
+  cudaError_t e = launch_xorshift(seed, offset, count, static_cast<uint64_t*>(d), ctx->tabs, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "xorshift stream");
+  MPC_CUDA(ctx, cudaMemcpyAsync(host_out, d, count * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return MPC_OK;
+}
+
+int mpc_european_call_stepwise_v1(const double* normals, double* payoffs, int32_t n_paths, int32_t n_steps,
+                                  double log_s0, double strike, double drift_dt, double vol_dt, double discount,
+                                  void* stream) {
+  if (n_paths < 0 || n_steps < 0 || (n_paths > 0 && (!normals || !payoffs))) return MPC_E_INVALID_CONFIG;
+  cudaError_t e = launch_european_call_stepwise_v1(normals, payoffs, n_paths, n_steps, log_s0, strike, drift_dt,
+                                                   vol_dt, discount, static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? MPC_OK : MPC_E_CUDA;
+}
+
+int mpc_flush_l2(mpc_context_t* ctx) {
+  if (!ctx) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  void* d = nullptr;
+  const size_t bytes = 256ull << 20;  // twice the 126 MB L2
+  int st = scratch(ctx, "flush", bytes, &d);
+  if (st != MPC_OK) return st;
+  cudaError_t e = launch_flush(d, bytes, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "flush");
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return MPC_OK;
+}
+
+int mpc_last_timing(const mpc_context_t* ctx, double* device_ms, uint64_t* kernel_launches) {
+  if (!ctx) return MPC_E_INVALID_CONFIG;
+  if (device_ms) *device_ms = ctx->last_ms;
+  if (kernel_launches) *kernel_launches = ctx->last_launches;
+  return MPC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,92 @@
+// mpc_runtime.h -- internal host runtime shared by mpc_runtime.cu and mpc_server.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/montepath_cuda.h"
+#include "mpc_launch.h"
+#include "mpc_types.h"
+
+namespace mpc {
+
+// A growable device allocation charged against the context's HBM budget.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+// Launch shape chosen for one request (autotuner output).
+struct Shape {
+  uint32_t block = 256;
+  uint32_t ppt = 1;  // units per thread per tile
+};
+
+// Host view of a request prepared for the device.
+struct Prepared {
+  DevReq q{};
+  int sampler = 0;
+  int family = 0;
+  bool plain = false;     // FP64 plain pipeline
+  bool lsm = false;
+  bool mlmc = false;
+  double cv_expectation = 0.0;
+  std::vector<uint32_t> halton_primes;
+  std::vector<double> halton_shifts;
+  std::vector<LhsDim> lhs;
+  uint64_t path_steps = 0;
+};
+
+struct Autotuner {
+  std::mutex mu;
+  std::map<uint64_t, Shape> cache;  // key: family | sampler | steps bucket | size bucket
+  uint64_t hits = 0, misses = 0;
+};
+
+}  // namespace mpc
+
+struct mpc_context {
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  mpc::DeviceTables tabs{};
+  void* d_sobol = nullptr;
+  void* d_jump = nullptr;
+  uint64_t budget = 0;
+  uint64_t live_bytes = 0;
+  uint64_t peak_bytes = 0;
+  std::string last_error;
+  std::recursive_mutex mu;
+  double last_ms = 0.0;
+  uint64_t last_launches = 0;
+  std::map<std::string, mpc::DevBuf> bufs;  // named scratch buffers
+  void* pinned = nullptr;                   // pinned staging for descriptors and results
+  size_t pinned_bytes = 0;
+  mpc::Autotuner tuner;
+  // graph cache of the last fused batch
+  cudaGraphExec_t graph_exec = nullptr;
+  uint64_t graph_key = 0;
+};
+
+namespace mpc {
+
+int fail(mpc_context* ctx, int status, const std::string& msg);
+int cuda_fail(mpc_context* ctx, cudaError_t err, const char* what);
+// Returns a device buffer of at least `bytes` for `name`, growing it under the budget.
+int scratch(mpc_context* ctx, const std::string& name, size_t bytes, void** out);
+int validate(const mpc_request_t& r, std::string* msg);
+int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* msg);
+uint64_t estimate_bytes(const mpc_request_t& r);
+Shape choose_shape(mpc_context* ctx, const Prepared& p);
+void summarize_moments(const Prepared& p, const double* m, mpc_result_t* out);
+// Fused FP32 requests: one persistent launch per (sampler, family) group on the context stream.
+int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_result_t*>& outs,
+              double* per_unit_host, uint64_t per_unit_cap);
+
+}  // namespace mpc

@@ -1,0 +1,82 @@
+// mpc_types.h -- host/device shared data layout of the B200 Monte Carlo backend.
+#pragma once
+
+#include <stdint.h>
+
+#define MPC_SOBOL_TABLE_DIMS 256
+// Moments per tile / request: count, sum p, sum p^2, sum c, sum c^2, sum p*c (+2 pad).
+#define MPC_MOMENTS 8
+
+namespace mpc {
+
+// Kernel families: the model-specific loop a tile runs.
+enum Family : int32_t {
+  FAM_GBM_STEP = 0,
+  FAM_GBM_TERMINAL = 1,
+  FAM_HESTON = 2,
+  FAM_MERTON_STEP = 3,
+  FAM_MERTON_TERMINAL = 4,
+  FAM_BASKET = 5,
+  FAM_MLMC_LEVEL = 6,
+  FAM_COUNT = 7
+};
+
+// Device samplers.
+enum Sampler : int32_t {
+  SMP_XORSHIFT = 0,  // replay of MonteCarloRng
+  SMP_HALTON = 1,
+  SMP_LHS = 2,
+  SMP_SOBOL = 3,
+  SMP_COUNTER = 5,
+};
+
+struct LhsDim {
+  uint64_t multiplier, offset, jitter_seed;
+};
+
+// Everything a tile needs to simulate units of one request.  Built on the
+// host (double precision constants); FP32 kernels round them once per tile.
+struct alignas(16) DevReq {
+  int32_t family, workload, technique, sampling;
+  uint32_t n_steps;        // model steps (fine steps for an MLMC level)
+  uint32_t n_assets;
+  uint64_t n_paths;        // simulated paths
+  uint64_t n_units;        // paths, or antithetic pairs
+  uint64_t normals_per_unit;
+  uint64_t seed;
+  uint32_t seed32;
+  uint32_t n_chunks;       // reference CPU chunk split (1 = one stream)
+  uint64_t chunk_base, chunk_rem;
+  // GBM / payoff
+  double s0, k, barrier, log_s0, log_barrier, discount, drift_dt, vol_dt, cv_expectation;
+  // Heston
+  double v0, kappa, theta, xi, rho, rho_perp, dt, sqrt_dt, rate;
+  // Merton
+  double jump_mean, jump_vol, lam_dt;
+  // Basket: lower Cholesky factor and per-asset step constants
+  double chol[64], b_drift[8], b_vol[8], spots[8], weights[8];
+  // MLMC level
+  uint32_t level, refinement;
+  uint64_t coarse_steps;
+  double f_drift, f_vol, c_drift, c_vol, inv_sqrt_m, inv_fine, inv_coarse;
+  // samplers
+  const uint32_t* halton_primes;
+  const double* halton_shifts;
+  const LhsDim* lhs;
+  // tiling and outputs
+  uint32_t tile_units;     // units per tile
+  uint32_t n_tiles;
+  double* partials;        // [n_tiles][MPC_MOMENTS]
+  double* moments;         // [MPC_MOMENTS] final, written by the last tile
+  uint32_t* tiles_done;    // completion counter for the last-tile finalize
+  double* per_unit;        // optional [n_units] payoffs (parity checks)
+  uint32_t cv;             // record control variate moments
+  uint32_t anti;           // antithetic pairs
+};
+
+struct Tile {
+  uint32_t req;
+  uint32_t tile;
+};
+
+}  // namespace mpc
