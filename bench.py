@@ -1,0 +1,366 @@
+"""Benchmark of the B200 Monte Carlo pricing backend.
+
+Workload (the configuration the headline metric is quoted on): Heston and
+Merton European calls, 1,048,576 paths x 256 steps each, scrambled Sobol
+samples (2 and 3 dimensions per step), FP32 path arithmetic with FP64
+accumulation -- one step prices both requests through ``mpc_price_batch``.
+Synthetic inputs: every sample is generated on the device from the seed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  ``value`` is path-steps/s over all ranks with the
+requests already resident (device time of each step from CUDA events on the
+library stream, summed over K steps, max over ranks); ``e2e`` is the same
+metric through the public C ABI with host request structs, wall-clock per
+call including the descriptor upload and the result read-back.  The plain
+FP64 one-request-per-launch path is timed beside it for the speed-up ratio.
+N > 1 runs independent replicas (one per GPU): Monte Carlo paths need no
+exchange, so there is no data-path collective.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_PATHS = 1_048_576
+N_STEPS = 256
+SEED = 42
+WORKLOAD = "heston_merton_european_sobol_1048576x256"
+
+HESTON = dict(model="heston", s0=100.0, k=100.0, r=0.03, t=1.0, kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7,
+              v0=0.04, n_paths=N_PATHS, n_steps=N_STEPS, seed=SEED, sampling="scrambled_sobol")
+MERTON = dict(model="merton", method="stepwise", s0=100.0, k=100.0, r=0.03, sigma=0.2, t=1.0, jump_intensity=0.5,
+              jump_mean=-0.1, jump_volatility=0.15, n_paths=N_PATHS, n_steps=N_STEPS, seed=SEED + 1,
+              sampling="scrambled_sobol")
+
+# Algorithmic work per path-step (fixed by convention; FMA = 2 flops, one MUFU op = 1 SFU op):
+# Sobol + Acklam normal 24 flops + 1 SFU; Heston step 16 flops + 1 SFU (sqrt v+);
+# Merton step 4 flops (+ the Sobol uniform of the Poisson dimension, no inverse CDF).
+FLOPS_PER_STEP = {"heston": 2 * 24 + 16, "merton": 24 + 4}
+SFU_PER_STEP = {"heston": 2 * 1 + 1, "merton": 1}
+
+
+def requests(precision: str):
+    from montepath_b200.requests import make_request
+
+    h = make_request("european_call", dict(HESTON, precision=precision))
+    m = make_request("european_call", dict(MERTON, precision=precision))
+    return [h, m]
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu), "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                        rows.append(parts)
+        finally:
+            try:
+                os.remove(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = sorted(float(r[1]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reduce_max(pg, value: float, local: int) -> float:
+    if pg is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def load_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+def load_traffic() -> dict:
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def cpu_baseline(seconds_target: float = 12.0) -> dict:
+    """The oracle (FP64 C++ restatement of the reference CPU path) on a
+    bounded sample of the same workload, all host threads."""
+
+    from montepath_b200.requests import make_request
+    from oracle import oracle as O
+
+    O.lib()  # compile/load the oracle before timing
+    threads = os.cpu_count() or 1
+    paths = 2048
+    while True:
+        total_steps = 0
+        t0 = time.perf_counter()
+        for cfg in (HESTON, MERTON):
+            req = make_request("european_call", dict(cfg, n_paths=paths, precision="fp64_plain"))
+            O.price_threaded(req, threads)
+            total_steps += paths * N_STEPS
+        dt = time.perf_counter() - t0
+        if dt * threads >= seconds_target or paths >= N_PATHS:
+            break
+        paths = min(N_PATHS, int(paths * max(2.0, seconds_target / max(dt * threads, 1e-3))))
+    return {
+        "value": total_steps / dt,
+        "unit": "path-steps/s",
+        "cores": threads,
+        "kind": "port",
+        "sample": f"Heston + Merton Sobol {paths} paths x {N_STEPS} steps each (of {N_PATHS}), FP64, {dt:.2f} s wall",
+    }
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    for _ in range(args.warmup):
+        cpu_baseline(seconds_target=2.0)
+    vals = []
+    t0 = time.perf_counter()
+    last = None
+    for _ in range(args.steps):
+        last = cpu_baseline(seconds_target=8.0)
+        vals.append(last["value"])
+    wall = time.perf_counter() - t0
+    value = sum(vals) / len(vals)
+    line = {
+        "impl": "reference",
+        "metric": "path-steps/s",
+        "value": value,
+        "unit": "path-steps/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * wall / max(args.steps, 1),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded scrambled Sobol samples)",
+        "config": {"workload": WORKLOAD, "paths": N_PATHS, "steps_per_path": N_STEPS, "requests": 2,
+                   "note": "CPU restatement of the reference path on a bounded sample of the workload"},
+        "cpu_baseline": dict(last, value=value),
+        "e2e": {"value": value, "unit": "path-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    rank, world, local, pg = dist_setup(args.gpus)
+    from montepath_b200.backend import CudaBackend
+
+    backend = CudaBackend(local)
+    fused = requests("fp32_path")
+    plain = requests("fp64_plain")
+    path_steps = sum(r.n_paths * r.n_steps for r in fused)
+
+    for _ in range(max(args.warmup, 3)):
+        backend.price_batch(fused)
+    # timed region: device time of each step (CUDA events on the library stream)
+    barrier(pg)
+    device_ms = 0.0
+    launches = 0
+    results = None
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            backend.flush_l2()  # between steps, outside the events
+            results = backend.price_batch(fused)
+            ms, n = backend.last_timing()
+            device_ms += ms
+            launches += n
+    barrier(pg)
+    clock_info = clocks.summary()
+    device_ms = reduce_max(pg, device_ms, local)
+    value = world * path_steps * args.steps / (device_ms * 1e-3)
+
+    # end to end through the public ABI: host request structs in, results out
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        backend.price_batch(fused)
+        e2e_s += time.perf_counter() - t0
+    h2d, d2h = backend.last_transfer()
+    e2e_s = reduce_max(pg, e2e_s, local)
+    e2e_value = world * path_steps * args.steps / e2e_s
+
+    # plain FP64 one-request-per-launch baseline (same requests, same seeds)
+    plain_ms = 0.0
+    plain_steps = max(1, min(2, args.steps))
+    backend.price_batch(plain)
+    plain_results = None
+    for _ in range(plain_steps):
+        plain_results = backend.price_batch(plain)
+        plain_ms += backend.last_timing()[0]
+    plain_ms = reduce_max(pg, plain_ms, local)
+    plain_value = world * path_steps * plain_steps / (plain_ms * 1e-3)
+
+    # roofline of the fused kernels (compute-bound: FP32 pipe and MUFU)
+    fp32_peak, sfu_peak = backend.measure_peaks()
+    per_rank_rate = path_steps / (device_ms / args.steps * 1e-3)
+    flops = sum(FLOPS_PER_STEP[k] for k in ("heston", "merton")) * (per_rank_rate / 2)
+    sfu = sum(SFU_PER_STEP[k] for k in ("heston", "merton")) * (per_rank_rate / 2)
+    fr_fp32 = flops / 1e12 / fp32_peak if fp32_peak else None
+    fr_sfu = sfu / 1e12 / sfu_peak if sfu_peak else None
+    traffic = load_traffic().get("fused_heston_merton_sobol", {}).get("bytes_per_step")
+    bound, achieved, peak, unit, frac = "fp32", flops / 1e12, fp32_peak, "TFLOP/s", fr_fp32
+    if fr_sfu is not None and fr_fp32 is not None and fr_sfu > fr_fp32:
+        bound, achieved, peak, unit, frac = "sfu", sfu / 1e12, sfu_peak, "Tops/s", fr_sfu
+
+    from oracle import oracle as O
+
+    heston_ref = O.heston_call(100, 100, 0.03, 0.04, 2.0, 0.04, 0.5, -0.7, 1.0)
+    merton_ref = O.merton_series(100, 100, 0.03, 0.2, 0.5, -0.1, 0.15, 1.0, exact=True)
+    line = None
+    if rank == 0:
+        line = {
+            "metric": "path-steps/s",
+            "value": value,
+            "unit": "path-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": device_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 path / f64 accumulation",
+            "data": "synthetic (seeded scrambled Sobol samples generated on the device)",
+            "config": {
+                "workload": WORKLOAD,
+                "paths": N_PATHS,
+                "steps_per_path": N_STEPS,
+                "requests_per_step": 2,
+                "precision": "fp32_path",
+                "parallelism": f"replicas x{world}",
+                "l2": "flushed between steps (256 MiB write); samples never touch HBM",
+            },
+            "e2e": {"value": e2e_value, "unit": "path-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clock_info,
+            "roofline": {
+                "bound": bound,
+                "achieved": achieved,
+                "peak": peak,
+                "unit": unit,
+                "frac": frac,
+                "traffic": traffic,
+                "fractions": {"fp32": fr_fp32, "sfu": fr_sfu},
+                "peak_source": "measured by mpc_measure_peaks on this GPU (FP32 FMA chains / MUFU ex2 chains)",
+                "hbm_peak_gbs": load_peaks().get("hbm_gbs"),
+            },
+            "plain_fp64": {"value": plain_value, "unit": "path-steps/s", "ms_per_step": plain_ms / plain_steps,
+                           "speedup_fused_vs_plain": value / plain_value},
+            "prices": {
+                "heston": {"price": results[0].price, "stderr": results[0].stderr,
+                           "fp64_plain": plain_results[0].price, "semi_analytic": heston_ref},
+                "merton": {"price": results[1].price, "stderr": results[1].stderr,
+                           "fp64_plain": plain_results[1].price, "series": merton_ref},
+            },
+        }
+        if not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    backend.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

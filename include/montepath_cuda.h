@@ -308,6 +308,11 @@ int mpc_flush_l2(mpc_context_t* ctx);
 /* Device time (ms) of the last mpc_price / mpc_price_batch and the number of
  * kernels it launched. */
 int mpc_last_timing(const mpc_context_t* ctx, double* device_ms, uint64_t* kernel_launches);
+/* Host<->device bytes the last mpc_price / mpc_price_batch copied (no reference counterpart: diagnostics). */
+int mpc_last_transfer(const mpc_context_t* ctx, uint64_t* h2d_bytes, uint64_t* d2h_bytes);
+/* Measured FP32 FMA (TFLOP/s) and MUFU (Tops/s) throughput of the device, the
+ * roofline denominators of the compute-bound fused kernels (no reference counterpart). */
+int mpc_measure_peaks(mpc_context_t* ctx, double* fp32_tflops, double* sfu_tops);
 
 /* ----- serving ------------------------------------------------------------ */
 int mpc_server_start(mpc_context_t* ctx, const mpc_server_options_t* options, mpc_server_t** out);

@@ -310,6 +310,8 @@ FUNCTIONS = [
     ),
     ("mpc_flush_l2", c_int, [c_void_p]),
     ("mpc_last_timing", c_int, [c_void_p, POINTER(c_double), POINTER(c_uint64)]),
+    ("mpc_last_transfer", c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64)]),
+    ("mpc_measure_peaks", c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
     ("mpc_server_start", c_int, [c_void_p, POINTER(ServerOptions), POINTER(c_void_p)]),
     ("mpc_submit", c_int, [c_void_p, POINTER(Request), POINTER(c_uint64)]),
     ("mpc_poll", c_int, [c_void_p, c_uint64, POINTER(Result)]),

@@ -115,6 +115,18 @@ class CudaBackend:
         self.lib.mpc_last_timing(self.handle, byref(ms), byref(launches))
         return ms.value, launches.value
 
+    def last_transfer(self) -> tuple[int, int]:
+        h2d = c_uint64()
+        d2h = c_uint64()
+        self.lib.mpc_last_transfer(self.handle, byref(h2d), byref(d2h))
+        return h2d.value, d2h.value
+
+    def measure_peaks(self) -> tuple[float, float]:
+        fp32 = c_double()
+        sfu = c_double()
+        self._check(self.lib.mpc_measure_peaks(self.handle, byref(fp32), byref(sfu)))
+        return fp32.value, sfu.value
+
     def server(self, hbm_budget_bytes: int = 0, max_slots: int = 0, wave_tiles: int = 0, plain: bool = False) -> "Server":
         return Server(self, hbm_budget_bytes, max_slots, wave_tiles, plain)
 

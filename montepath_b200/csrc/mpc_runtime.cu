@@ -589,8 +589,8 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
   if ((st = scratch(ctx, "moments", n * MPC_MOMENTS * sizeof(double), &d_mom))) return st;
   if ((st = scratch(ctx, "done", n * sizeof(uint32_t), &d_done))) return st;
   if ((st = scratch(ctx, "counter", 64 * sizeof(uint32_t), &d_counter))) return st;
-  if (per_unit_host) {
-    if ((st = scratch(ctx, "per_unit", per_unit_cap * sizeof(double), &d_unit))) return st;
+  if (per_unit_host) {  // the kernel writes every unit of request 0; the copy-out is clipped to the capacity
+    if ((st = scratch(ctx, "per_unit", reqs[0]->q.n_units * sizeof(double), &d_unit))) return st;
   }
   for (size_t i = 0; i < n; ++i) {
     DevReq& q = reqs[i]->q;
@@ -661,6 +661,8 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
   cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
   ctx->last_ms = ms;
   ctx->last_launches = kernel_launch_count() - launches_before;
+  ctx->last_h2d = desc_bytes + tile_bytes;
+  ctx->last_d2h = mom_bytes;
   for (size_t i = 0; i < n; ++i) {
     summarize_moments(*reqs[i], hm + i * MPC_MOMENTS, outs[i]);
     outs[i]->path_steps = reqs[i]->path_steps;
@@ -718,6 +720,8 @@ static int run_plain(mpc_context* ctx, Prepared* p, mpc_result_t* out, double* p
   cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
   ctx->last_ms = ms;
   ctx->last_launches = kernel_launch_count() - launches_before;
+  ctx->last_h2d = sizeof(DevReq);
+  ctx->last_d2h = MPC_MOMENTS * sizeof(double);
   summarize_moments(*p, hm, out);
   out->path_steps = p->path_steps;
   out->runtime_ms = ms;
@@ -818,6 +822,8 @@ static int run_lsm(mpc_context* ctx, const mpc_request_t& r, mpc_result_t* out, 
   cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
   ctx->last_ms = ms;
   ctx->last_launches = kernel_launch_count() - launches_before;
+  ctx->last_h2d = sched.size() * 4 + disc_pow.size() * 8;
+  ctx->last_d2h = 8 * 8 + 4;
   if (*herr != 0) return fail(ctx, MPC_E_TIMEOUT, "LSM grid barrier timed out");
   double price, se;
   summarize(hout[0], hout[1], hout[2], &price, &se);
@@ -1554,6 +1560,13 @@ int mpc_last_timing(const mpc_context_t* ctx, double* device_ms, uint64_t* kerne
   if (!ctx) return MPC_E_INVALID_CONFIG;
   if (device_ms) *device_ms = ctx->last_ms;
   if (kernel_launches) *kernel_launches = ctx->last_launches;
+  return MPC_OK;
+}
+
+int mpc_last_transfer(const mpc_context_t* ctx, uint64_t* h2d_bytes, uint64_t* d2h_bytes) {
+  if (!ctx) return MPC_E_INVALID_CONFIG;
+  if (h2d_bytes) *h2d_bytes = ctx->last_h2d;
+  if (d2h_bytes) *d2h_bytes = ctx->last_d2h;
   return MPC_OK;
 }
 

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <string>
@@ -65,6 +66,7 @@ struct mpc_context {
   std::recursive_mutex mu;
   double last_ms = 0.0;
   uint64_t last_launches = 0;
+  uint64_t last_h2d = 0, last_d2h = 0;
   std::map<std::string, mpc::DevBuf> bufs;  // named scratch buffers
   void* pinned = nullptr;                   // pinned staging for descriptors and results
   size_t pinned_bytes = 0;

@@ -1,0 +1,295 @@
+"""GPU parity: the CUDA backend through its C ABI against the CPU oracle.
+
+Tolerances (stated per test):
+  * integer streams (xorshift64*, counter hash, Sobol, Halton digits): bit-exact;
+  * FP64 samples: 1e-13 relative (CUDA vs glibc transcendentals, <= 1-2 ulp);
+  * FP64-plain prices / per-path payoffs: 1e-11 relative;
+  * FP32-path per-path payoffs fed the same samples: 2e-4 relative + 1e-4 absolute,
+    prices within 3 standard errors of the FP64 oracle (and far closer in practice);
+  * the Metal same-normals precedent (backend/metal.rs:1155-1164): price 1e-3, stderr 1e-4.
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from montepath_b200 import abi
+from montepath_b200.requests import make_request
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def req(workload, **kw):
+    return make_request(workload, kw)
+
+
+# --------------------------------------------------------------- generators --
+@pytest.mark.parametrize("seed,offset", [(42, 0), (1, 1), (0, 12345), (0xDEADBEEF, 999_999)])
+def test_xorshift_jump_ahead_bit_exact(backend, seed, offset):
+    count = 4096
+    ref = O.xorshift_u64(seed, offset + count)[offset:]
+    got = backend.xorshift(seed, offset, count)
+    assert np.array_equal(got, ref)
+
+
+def test_counter_hash_bit_exact(backend):
+    got = backend.counter_hash(42, 64, 33)
+    L = O.lib()
+    for path in (0, 1, 17, 63):
+        for step in (0, 5, 32):
+            for lane in (0, 1):
+                assert got[path, step, lane] == L.or_counter_hash(42, path, step, lane)
+
+
+def test_counter_hash_fp32_normals(backend):
+    got = backend.generate_normals(abi.SAMPLING_COUNTER_HASH, 42, 256, 32, fp32=True)
+    ref = O.stateless_normals_f32(42, 256, 32).reshape(256, 32)
+    # same u32 hashes and f32 uniforms; logf/cosf differ by a few ulp
+    assert np.max(np.abs(got - ref)) < 4e-6
+
+
+@pytest.mark.parametrize(
+    "sampling",
+    [abi.SAMPLING_PSEUDORANDOM, abi.SAMPLING_SCRAMBLED_SOBOL, abi.SAMPLING_RANDOMIZED_HALTON, abi.SAMPLING_LATIN_HYPERCUBE],
+)
+def test_fp64_samples_match_oracle(backend, sampling):
+    n, d = 2048, 37
+    got = backend.generate_normals(sampling, 7, n, d)
+    ref = O.generate_normals(sampling, 7, n, d)
+    assert np.allclose(got, ref, rtol=1e-13, atol=1e-13)
+
+
+def test_sobol_fp32_normals_same_uniforms(backend):
+    n, d = 70_000, 9  # crosses a 2^16-point block boundary
+    got = backend.generate_normals(abi.SAMPLING_SCRAMBLED_SOBOL, 5, n, d, fp32=True)
+    ref = O.generate_normals(abi.SAMPLING_SCRAMBLED_SOBOL, 5, n, d)
+    assert np.max(np.abs(got - ref)) < 2e-5
+
+
+# -------------------------------------------------------------- plain FP64 --
+def test_config1_plain_fp64_replays_reference_stream(backend):
+    r = req("european_call", method="stepwise", n_paths=20000, n_steps=64, seed=42, n_threads=1,
+            precision="fp64_plain")
+    got = backend.price(r)
+    ref = O.price(r)
+    assert abs(got.price - ref.price) <= 1e-11 * ref.price
+    assert abs(got.stderr - ref.stderr) <= 1e-9 * ref.stderr
+    assert abs(got.price - 9.413403383853016) < 3 * got.stderr
+
+
+@pytest.mark.parametrize("threads", [1, 4])
+@pytest.mark.parametrize("technique", ["standard", "antithetic", "control_variate"])
+def test_gbm_stepwise_paths_fp64(backend, technique, threads):
+    r = req("european_call", method="stepwise", n_paths=9001, n_steps=33, seed=9, n_threads=threads,
+            technique=technique, precision="fp64_plain")
+    if threads > 1:
+        r.n_paths = 9001 * 4 // 3
+    _, ref = O.price_paths(r)
+    got = backend.price_paths(r)
+    assert np.allclose(got, ref, rtol=1e-11, atol=1e-11)
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) <= 1e-10 * abs(b.price)
+
+
+@pytest.mark.parametrize("workload", ["arithmetic_asian_call", "down_and_out_call", "up_and_out_call", "lookback_call"])
+def test_path_dependent_fp64(backend, workload):
+    r = req(workload, n_paths=5000, n_steps=48, seed=21, n_threads=1, precision="fp64_plain",
+            barrier=(85.0 if workload == "down_and_out_call" else 125.0))
+    _, ref = O.price_paths(r)
+    got = backend.price_paths(r)
+    assert np.allclose(got, ref, rtol=1e-11, atol=1e-11)
+
+
+@pytest.mark.parametrize("sampling", ["scrambled_sobol", "randomized_halton", "latin_hypercube", "counter_hash"])
+def test_heston_and_merton_fp64_structured(backend, sampling):
+    for kw in (
+        dict(model="heston", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04),
+        dict(model="merton", method="stepwise", jump_intensity=0.5, jump_mean=-0.1, jump_volatility=0.15),
+    ):
+        r = req("european_call", n_paths=3000, n_steps=24, seed=42, sampling=sampling, precision="fp64_plain", **kw)
+        _, ref = O.price_paths(r)
+        got = backend.price_paths(r)
+        assert np.allclose(got, ref, rtol=1e-10, atol=1e-10), (sampling, kw["model"])
+
+
+def test_heston_pseudorandom_chunked_fp64(backend):
+    r = req("european_call", model="heston", n_paths=12000, n_steps=16, seed=3, n_threads=3, precision="fp64_plain",
+            technique="antithetic")
+    _, ref = O.price_paths(r)
+    assert np.allclose(backend.price_paths(r), ref, rtol=1e-11, atol=1e-11)
+
+
+def test_basket_reference_two_asset_fp64(backend):
+    r = req("basket_call", n_paths=6000, seed=8, precision="fp64_plain")
+    _, ref = O.price_paths(r)
+    assert np.allclose(backend.price_paths(r), ref, rtol=1e-11, atol=1e-11)
+
+
+# ------------------------------------------------------------- fused FP32 ---
+def test_metal_same_normals_precedent(backend):
+    # backend/metal.rs:1127-1164: 4,096 x 32, price within 1e-3, stderr within 1e-4
+    r = req("european_call", method="stepwise", n_paths=4096, n_steps=32, seed=42, sampling="counter_hash")
+    z = O.stateless_normals_f32(42, 4096, 32)
+    ref, _ = O.price_from_f32_normals(r, z)
+    got = backend.price(r)
+    assert abs(got.price - ref.price) <= 1e-3
+    assert abs(got.stderr - ref.stderr) <= 1e-4
+
+
+@pytest.mark.parametrize("workload", ["european_call", "arithmetic_asian_call", "down_and_out_call", "lookback_call"])
+def test_fused_counter_hash_same_normals(backend, workload):
+    r = req(workload, method="stepwise", n_paths=4096, n_steps=64, seed=11, sampling="counter_hash")
+    z = O.stateless_normals_f32(11, 4096, 64)
+    ref, ref_paths = O.price_from_f32_normals(r, z)
+    got_paths = backend.price_paths(r)
+    close = np.isclose(got_paths, ref_paths, rtol=2e-4, atol=1e-4)
+    # a barrier crossing within FP32 rounding of the level may flip a path
+    assert close.mean() > 0.999
+    got = backend.price(r)
+    assert abs(got.price - ref.price) <= 1e-3
+
+
+@pytest.mark.parametrize("sampling", ["pseudorandom", "scrambled_sobol", "randomized_halton", "counter_hash"])
+def test_fused_gbm_against_fp64_oracle(backend, sampling):
+    r = req("european_call", method="stepwise", n_paths=8192, n_steps=64, seed=5, sampling=sampling)
+    _, ref_paths = O.price_paths(r)
+    got_paths = backend.price_paths(r)
+    assert np.allclose(got_paths, ref_paths, rtol=2e-4, atol=1e-3)
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) < 0.05 * b.stderr
+
+
+def test_fused_heston_merton_sobol_small(backend):
+    for kw in (
+        dict(model="heston", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04),
+        dict(model="merton", method="stepwise", jump_intensity=0.5, jump_mean=-0.1, jump_volatility=0.15),
+    ):
+        r = req("european_call", n_paths=16384, n_steps=256, seed=42, sampling="scrambled_sobol", **kw)
+        _, ref_paths = O.price_paths(r)
+        got_paths = backend.price_paths(r)
+        assert np.isclose(got_paths, ref_paths, rtol=1e-3, atol=2e-3).mean() > 0.999
+        a, b = backend.price(r), O.price(r)
+        assert abs(a.price - b.price) < 0.1 * b.stderr, kw["model"]
+
+
+def test_fused_basket_five_assets(backend):
+    r = req("basket_call", method="stepwise", n_steps=20, n_paths=8000, seed=4, sampling="counter_hash",
+            spots=[100, 95, 105, 98, 102], sigmas=[0.2, 0.25, 0.3, 0.15, 0.22], weights=[0.2] * 5, corr=0.3, k=100)
+    _, ref_paths = O.price_paths(r)
+    got = backend.price_paths(r)
+    assert np.allclose(got, ref_paths, rtol=2e-4, atol=1e-3)
+
+
+# --------------------------------------------------------------------- LSM --
+def test_lsm_fp64_plain_matches_oracle(backend):
+    r = req("american_put", n_paths=8192, n_steps=50, seed=5, r=0.06, basis_degree=3, precision="fp64_plain")
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) <= 1e-9 * b.price
+    assert a.early_exercise_count == b.early_exercise_count
+    assert a.regression_steps == b.regression_steps
+
+
+@pytest.mark.parametrize("s0", [90.0, 100.0, 110.0])
+def test_lsm_fp32_within_se(backend, s0):
+    r = req("american_put", n_paths=32768, n_steps=50, seed=5, r=0.06, basis_degree=3, s0=s0)
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) < 0.5 * b.stderr + 1e-3
+    crr = O.crr_put(s0, 100, 0.06, 0.2, 1.0, 2048)
+    assert abs(a.price - crr) < 5 * a.stderr + 0.15
+
+
+def test_bermudan_fp64(backend):
+    r = req("bermudan_put", n_paths=4096, n_steps=64, seed=3, exercise_steps=[48, 16, 32, 16], precision="fp64_plain")
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) <= 1e-9 * b.price
+    assert a.warnings & abi.WARN_SCHEDULE_NORMALISED
+
+
+# -------------------------------------------------------------------- MLMC --
+def test_mlmc_fp64_plain_matches_oracle(backend):
+    r = make_request("arithmetic_asian_mlmc", {"paths_per_level": [4000, 2000, 1000, 500], "seed": 3,
+                                                "precision": "fp64_plain"})
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) <= 1e-10 * abs(b.price)
+    for level in range(4):
+        assert abs(a.level_variance[level] - b.level_variance[level]) <= 1e-9 * b.level_variance[level]
+
+
+def test_mlmc_tolerance_fp32(backend):
+    r = make_request("arithmetic_asian_mlmc", {"target_stderr": 0.02, "levels": 5, "seed": 9})
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) < 3 * math.hypot(a.stderr, b.stderr)
+    assert a.total_step_updates <= r.max_step_updates * 1.01 + 64
+
+
+# ------------------------------------------------------ batch and serving ---
+def test_batch_equals_individual(backend):
+    reqs = [
+        req("european_call", method="stepwise", n_paths=3000 + 1000 * i, n_steps=16 + 7 * i, seed=i,
+            sampling="counter_hash")
+        for i in range(6)
+    ] + [req("basket_call", method="stepwise", n_steps=12, n_paths=5000, seed=77, sampling="counter_hash",
+             spots=[100] * 5, sigmas=[0.2] * 5, weights=[0.2] * 5, corr=0.3)]
+    alone = [backend.price(r) for r in reqs]
+    batch = backend.price_batch(reqs)
+    for a, b in zip(alone, batch):
+        assert a.price == b.price and a.stderr == b.stderr
+
+
+def test_serving_alone_equals_mix(backend):
+    reqs = [req("european_call", method="stepwise", n_paths=20000 + 5000 * i, n_steps=64, seed=100 + i,
+                sampling="counter_hash") for i in range(8)]
+    reqs += [req("european_call", model="heston", n_paths=8000, n_steps=32, seed=5, sampling="scrambled_sobol")]
+    alone = [backend.price(r) for r in reqs]
+    with backend.server(max_slots=4) as srv:
+        tickets = [srv.submit(r) for r in reqs]
+        mixed = [srv.wait(t) for t in tickets]
+        stats = srv.stats()
+    for a, b in zip(alone, mixed):
+        assert abs(a.price - b.price) <= 1e-12 * abs(a.price)
+    assert stats.completed == len(reqs)
+    assert stats.p99_ms >= stats.p50_ms > 0
+
+
+# ------------------------------------------------------ errors and contract --
+def test_invalid_config_returns_code(backend):
+    from montepath_b200.backend import BackendError
+
+    r = req("european_call", n_paths=0)
+    with pytest.raises(BackendError) as err:
+        backend.price(r)
+    assert err.value.status == abi.E_INVALID_CONFIG
+    r = req("european_call", model="merton", sampling="pseudorandom")
+    with pytest.raises(BackendError) as err:
+        backend.price(r)
+    assert err.value.status == abi.E_UNSUPPORTED
+
+
+def test_budget_exceeded_returns_code():
+    from montepath_b200.backend import BackendError, CudaBackend
+
+    with CudaBackend(0, hbm_budget_bytes=64 << 20) as small:
+        r = req("european_call", model="heston", n_paths=1 << 20, n_steps=256, sampling="scrambled_sobol",
+                precision="fp64_plain")
+        with pytest.raises(BackendError) as err:
+            small.price(r)
+        assert err.value.status == abi.E_OOM_BUDGET
+
+
+def test_reference_v1_kernel_contract(backend):
+    torch = pytest.importorskip("torch")
+    n_paths, n_steps = 5000, 40
+    z = O.pseudorandom_normals(42, n_paths * n_steps)
+    normals = torch.tensor(z, dtype=torch.float64, device="cuda")
+    payoffs = torch.zeros(n_paths, dtype=torch.float64, device="cuda")
+    dt = 1.0 / n_steps
+    drift, vol, disc = (0.03 - 0.02) * dt, 0.2 * math.sqrt(dt), math.exp(-0.03)
+    lib = abi.load_library()
+    status = lib.mpc_european_call_stepwise_v1(normals.data_ptr(), payoffs.data_ptr(), n_paths, n_steps,
+                                               math.log(100.0), 100.0, drift, vol, disc, None)
+    torch.cuda.synchronize()
+    assert status == abi.OK
+    ref = np.maximum(np.exp(math.log(100.0) + np.cumsum(drift + vol * z.reshape(n_paths, n_steps), axis=1)[:, -1]) - 100.0, 0) * disc
+    assert np.allclose(payoffs.cpu().numpy(), ref, rtol=1e-12, atol=1e-12)
