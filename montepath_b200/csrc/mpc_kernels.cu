@@ -66,22 +66,43 @@ struct Source<SMP_COUNTER> {
   }
 };
 
+// Scrambled Sobol with the per-point work hoisted: the Owen-shuffled index
+// and its nibble offsets depend only on (point, dimension group of 256), so
+// they are recomputed when a path crosses into the next group; per
+// dimension only the 8 table lookups and the output scramble remain.  The
+// values equal sobol_point() bit for bit.
 template <>
 struct Source<SMP_SOBOL> {
   const uint32_t* table;
-  uint64_t point;
-  uint32_t seed;
+  uint32_t local, block_seed, group, seed_g, combine_g;
+  uint32_t off[8];
   template <bool FP64>
   __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
     table = c.sobol;
-    point = u;
-    seed = q.seed32;
+    local = (uint32_t)(u & 0xFFFFu);
+    block_seed = q.seed32 + (uint32_t)(u >> 16) * 0x9E3779B9u;
+    group = 0xFFFFFFFFu;
   }
-  __device__ __forceinline__ float n32(uint32_t d) { return icdf_f32(sobol_unit_f32(sobol_point(table, point, d, seed))); }
-  __device__ __forceinline__ double n64(uint32_t d) {
-    return icdf_f64(sobol_unit_f64(sobol_point(table, point, d, seed)));
+  __device__ __forceinline__ uint32_t sample(uint32_t d) {
+    const uint32_t g = d / MPC_SOBOL_TABLE_DIMS;
+    if (g != group) {
+      group = g;
+      seed_g = block_seed + g;
+      const uint32_t shuffled = nested_uniform_scramble(local, seed_g);
+#pragma unroll
+      for (int q = 0; q < 8; ++q) off[q] = q * 16 + ((shuffled >> (4 * q)) & 0xFu);
+      combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
+    }
+    const uint32_t dim = d & (MPC_SOBOL_TABLE_DIMS - 1);
+    const uint32_t* td = table + dim * 128;
+    uint32_t x = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) x ^= __ldg(td + off[q]);
+    return nested_uniform_scramble(x, seed_g ^ (dim + combine_g));  // hash_combine(seed_g, dim)
   }
-  __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sobol_point(table, point, d, seed)); }
+  __device__ __forceinline__ float n32(uint32_t d) { return normcdfinvf(sobol_unit_f32(sample(d))); }
+  __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(sobol_unit_f64(sample(d))); }
+  __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sample(d)); }
 };
 
 template <>
@@ -99,7 +120,7 @@ struct Source<SMP_HALTON> {
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
   __device__ __forceinline__ float n32(uint32_t d) {
     float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
-    return icdf_f32(u);
+    return normcdfinvf(u);
   }
 };
 
@@ -123,7 +144,7 @@ struct Source<SMP_LHS> {
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
   __device__ __forceinline__ float n32(uint32_t d) {
     float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
-    return icdf_f32(u);
+    return normcdfinvf(u);
   }
 };
 
@@ -166,10 +187,15 @@ __device__ __forceinline__ Real ex(Real x) {
   else
     return exp(x);
 }
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 template <class Real>
 __device__ __forceinline__ Real sq_root(Real x) {
   if constexpr (sizeof(Real) == 4)
-    return sqrtf(x);
+    return sqrt_approx(x);
   else
     return sqrt(x);
 }

@@ -1,0 +1,251 @@
+"""Mapping-ABI module for montepath's Python surface, backed by the CUDA library.
+
+montepath's pricing helpers call a native module by name with a config
+mapping and expect a mapping back (python/montepath/pricing.py:711-780):
+
+    price_european_call(native_module="montepath_b200.native", ...)
+
+Every function here has the name and the ``fn(mapping) -> dict`` shape of
+the reference's PyO3 bridge (crates/montepath-python/src/lib.rs:24-284,
+response shape ``pricing_response`` lib.rs:680-707): ``price``, ``stderr``,
+``values``, ``manifest`` (``backend: "nvidia_cuda"``) and ``warnings``.  The
+``*_cuda`` aliases mirror the naming of the Metal bridge
+(``price_european_call_metal``, production.py:80-90).  Pricing always runs on
+the GPU; a request the device path cannot run raises with its status code.
+"""
+
+from __future__ import annotations
+
+import threading
+from typing import Any, Mapping
+
+from . import abi
+from .backend import BackendError, CudaBackend
+from .requests import ConfigError, make_request, request_to_dict
+
+__version__ = "0.1.0"
+
+_lock = threading.Lock()
+_backend: CudaBackend | None = None
+
+
+def backend() -> CudaBackend:
+    """The process-wide device context (created on first use, device 0)."""
+
+    global _backend
+    with _lock:
+        if _backend is None:
+            _backend = CudaBackend(0)
+        return _backend
+
+
+def _manifest(workload: str, function: str, config: Mapping[str, Any], req: abi.Request) -> dict:
+    precision = "fp64_plain" if req.precision == abi.PRECISION_FP64_PLAIN else "fp32_path"
+    return {
+        "schema_version": "python-native-runtime.v1",
+        "workload": workload,
+        "backend": "nvidia_cuda",
+        "execution_mode": "native_cuda_sm100a",
+        "function": function,
+        "native_module": __name__,
+        "config": dict(config),
+        "request": request_to_dict(req),
+        "precision": precision,
+        "reproducibility": (
+            "deterministic for identical config, seed, library version and GPU: fixed tile order reductions; "
+            "pseudorandom sampling replays the reference MonteCarloRng stream"
+        ),
+        "performance_claim": "use bench.py artifacts for timing claims",
+    }
+
+
+def _warnings(req: abi.Request, res: abi.Result, config: Mapping[str, Any]) -> list[str]:
+    out = []
+    if req.precision == abi.PRECISION_FP32_PATH:
+        out.append("path arithmetic in FP32 with FP64 accumulation; compare against the FP64 oracle tolerance")
+    if config.get("n_threads", 0) == 0 and req.sampling == abi.SAMPLING_PSEUDORANDOM:
+        out.append("n_threads=0 runs one deterministic pseudorandom stream (the reference uses the host core count)")
+    if res.warnings & abi.WARN_BASIS_DEGREE_CLAMPED:
+        out.append("basis_degree was clamped to the supported range [1, 3].")
+    if res.warnings & abi.WARN_SCHEDULE_NORMALISED:
+        out.append("exercise_steps were sorted, deduplicated and maturity-appended before LSM execution.")
+    if res.warnings & abi.WARN_THREADS_IGNORED:
+        out.append("n_threads is accepted for API symmetry; the LSM regression runs as one GPU launch.")
+    return out
+
+
+def _values(res: abi.Result, req: abi.Request) -> dict:
+    values = {
+        "price": res.price,
+        "stderr": res.stderr,
+        "runtime_ms": res.runtime_ms,
+        "samples": res.n_samples,
+        "path_steps": res.path_steps,
+    }
+    if req.workload in (abi.WORKLOAD_AMERICAN_PUT, abi.WORKLOAD_BERMUDAN_PUT):
+        values.update(
+            early_exercise_count=res.early_exercise_count,
+            maturity_exercise_count=res.maturity_exercise_count,
+            regression_steps=res.regression_steps,
+            regression_basis=f"laguerre_lsm_degree_{res.basis_degree}",
+            paths=req.n_paths,
+            steps=req.n_steps,
+            seed=req.seed,
+        )
+    if req.workload == abi.WORKLOAD_ASIAN_MLMC:
+        levels = []
+        for level in range(res.n_levels):
+            fine = res.level_fine_steps[level]
+            levels.append(
+                {
+                    "level": level,
+                    "paths": res.level_paths[level],
+                    "fine_steps": fine,
+                    "coarse_steps": None if level == 0 else fine // max(req.refinement_factor, 1),
+                    "mean": res.level_mean[level],
+                    "variance": res.level_variance[level],
+                }
+            )
+        values.update(
+            total_paths=res.total_paths,
+            total_step_updates=res.total_step_updates,
+            levels=levels,
+            target_met=bool(res.target_met) if req.target_stderr > 0 else None,
+            estimated_stderr=res.estimated_stderr if req.target_stderr > 0 else None,
+        )
+    return values
+
+
+def _price(workload: str, function: str, config: Mapping[str, Any], extra: Mapping[str, Any] | None = None) -> dict:
+    cfg = dict(config or {})
+    params = dict(cfg)
+    params.update(extra or {})
+    try:
+        req = make_request(workload, params)
+    except ConfigError as exc:
+        raise ValueError(f"MC_CONFIG_INVALID: {exc}") from exc
+    res = abi.Result()
+    be = backend()
+    try:
+        res = be.price(req)
+    except BackendError as exc:
+        raise ValueError(f"MC_BACKEND_CUDA_{exc.code.replace('MPC_E_', '')}: {exc}") from exc
+    return {
+        "price": res.price,
+        "stderr": res.stderr,
+        "values": _values(res, req),
+        "manifest": _manifest(workload, function, cfg, req),
+        "warnings": _warnings(req, res, cfg),
+    }
+
+
+def price_european_call(config: Mapping[str, Any]) -> dict:
+    """european_call_price_mc_cpu (cpu.rs:3009): terminal unless ``method`` says stepwise."""
+
+    return _price("european_call", "price_european_call", config)
+
+
+def price_arithmetic_asian_call(config: Mapping[str, Any]) -> dict:
+    return _price("arithmetic_asian_call", "price_arithmetic_asian_call", config)
+
+
+def price_down_and_out_call(config: Mapping[str, Any]) -> dict:
+    return _price("down_and_out_call", "price_down_and_out_call", config)
+
+
+def price_up_and_out_call(config: Mapping[str, Any]) -> dict:
+    return _price("up_and_out_call", "price_up_and_out_call", config)
+
+
+def price_lookback_call(config: Mapping[str, Any]) -> dict:
+    return _price("lookback_call", "price_lookback_call", config)
+
+
+def price_basket_call(config: Mapping[str, Any]) -> dict:
+    return _price("basket_call", "price_basket_call", config)
+
+
+def price_american_put(config: Mapping[str, Any]) -> dict:
+    return _price("american_put", "price_american_put", config)
+
+
+def price_bermudan_put(config: Mapping[str, Any]) -> dict:
+    return _price("bermudan_put", "price_bermudan_put", config)
+
+
+def price_heston_european_call(config: Mapping[str, Any]) -> dict:
+    return _price("european_call", "price_heston_european_call", config, {"model": "heston", "method": "stepwise"})
+
+
+def price_merton_jump_diffusion_call(config: Mapping[str, Any]) -> dict:
+    """The reference Merton config has no sampling field (cpu.rs:1470-1482) and
+    draws a variable number of normals per path from one stream, which a
+    parallel device cannot replay; pseudorandom requests use the stateless
+    counter-hash generator instead."""
+
+    cfg = dict(config or {})
+    extra = {"model": "merton"}
+    if cfg.get("sampling", "pseudorandom") in (None, "pseudorandom"):
+        extra["sampling"] = "counter_hash"
+    out = _price("european_call", "price_merton_jump_diffusion_call", cfg, extra)
+    if "sampling" in extra:
+        out["warnings"].append("pseudorandom Merton runs on the counter-hash generator (statistically equivalent)")
+    return out
+
+
+def arithmetic_asian_mlmc(config: Mapping[str, Any]) -> dict:
+    out = _price("arithmetic_asian_mlmc", "arithmetic_asian_mlmc", config)
+    # workload_response shape (lib.rs:709-727): values + manifest + stderr
+    return out
+
+
+def price_european_call_parameter_sweep(config: Mapping[str, Any]) -> dict:
+    """price_european_call_parameter_sweep_cpu (cpu.rs:3028-3096) as one batched launch."""
+
+    cfg = dict(config or {})
+    base = dict(cfg.get("base_config") or {})
+    for key in ("n_paths", "n_steps", "seed"):
+        if cfg.get(key) is not None:
+            base[key] = cfg[key]
+    stride = int(cfg.get("seed_stride", 10_000))
+    method = cfg.get("method", "terminal_distribution")
+    scenarios = cfg.get("scenarios") or [{"scenario_id": "base"}]
+    reqs, rows_cfg = [], []
+    for index, sc in enumerate(scenarios):
+        sc = dict(sc)
+        scenario_cfg = dict(base)
+        for key in ("spot", "strike", "rate", "volatility", "maturity", "n_paths", "n_steps", "sampling", "technique"):
+            if sc.get(key) is not None:
+                scenario_cfg[key] = sc[key]
+        seed = sc.get("seed")
+        scenario_cfg["seed"] = int(seed) if seed is not None else (int(base.get("seed", 42)) + stride * index) % (1 << 64)
+        scenario_cfg["method"] = sc.get("method") or method
+        reqs.append(make_request("european_call", scenario_cfg))
+        rows_cfg.append((sc.get("scenario_id", f"scenario_{index}"), scenario_cfg))
+    try:
+        results = backend().price_batch(reqs)
+    except BackendError as exc:
+        raise ValueError(f"MC_BACKEND_CUDA_{exc.code.replace('MPC_E_', '')}: {exc}") from exc
+    rows = []
+    for index, ((sid, sc), req, res) in enumerate(zip(rows_cfg, reqs, results)):
+        rows.append({"scenario_index": index, "scenario_id": sid, "config": sc, "price": res.price, "stderr": res.stderr})
+    return {
+        "values": {"schema_version": "european-call-sweep.v1", "scenario_count": len(rows), "rows": rows,
+                   "total_paths": sum(r.n_paths for r in reqs)},
+        "manifest": _manifest("european_call_parameter_sweep", "price_european_call_parameter_sweep", cfg, reqs[0]),
+        "warnings": [],
+    }
+
+
+# Aliases in the naming of the Metal bridge.
+price_european_call_cuda = price_european_call
+price_arithmetic_asian_call_cuda = price_arithmetic_asian_call
+price_down_and_out_call_cuda = price_down_and_out_call
+price_up_and_out_call_cuda = price_up_and_out_call
+price_lookback_call_cuda = price_lookback_call
+price_basket_call_cuda = price_basket_call
+price_american_put_cuda = price_american_put
+price_bermudan_put_cuda = price_bermudan_put
+price_heston_european_call_cuda = price_heston_european_call
+price_merton_jump_diffusion_call_cuda = price_merton_jump_diffusion_call
+arithmetic_asian_mlmc_cuda = arithmetic_asian_mlmc

@@ -58,14 +58,18 @@ def test_fp64_samples_match_oracle(backend, sampling):
     n, d = 2048, 37
     got = backend.generate_normals(sampling, 7, n, d)
     ref = O.generate_normals(sampling, 7, n, d)
-    assert np.allclose(got, ref, rtol=1e-13, atol=1e-13)
+    err = np.abs(got - ref) / np.maximum(1.0, np.abs(ref))
+    worst = np.unravel_index(np.argmax(err), err.shape)
+    assert err.max() < 1e-13, (float(err.max()), worst, float(got[worst]), float(ref[worst]))
 
 
 def test_sobol_fp32_normals_same_uniforms(backend):
     n, d = 70_000, 9  # crosses a 2^16-point block boundary
     got = backend.generate_normals(abi.SAMPLING_SCRAMBLED_SOBOL, 5, n, d, fp32=True)
     ref = O.generate_normals(abi.SAMPLING_SCRAMBLED_SOBOL, 5, n, d)
-    assert np.max(np.abs(got - ref)) < 2e-5
+    # same 23-bit uniforms; FP32 inverse CDF vs the FP64 Acklam rational
+    err = np.abs(got - ref) / np.maximum(1.0, np.abs(ref))
+    assert err.max() < 2e-6, float(err.max())
 
 
 # -------------------------------------------------------------- plain FP64 --
@@ -111,7 +115,9 @@ def test_heston_and_merton_fp64_structured(backend, sampling):
         r = req("european_call", n_paths=3000, n_steps=24, seed=42, sampling=sampling, precision="fp64_plain", **kw)
         _, ref = O.price_paths(r)
         got = backend.price_paths(r)
-        assert np.allclose(got, ref, rtol=1e-10, atol=1e-10), (sampling, kw["model"])
+        # counter-hash normals are FP32 values computed by two libms (a few ulp apart)
+        tol = 2e-5 if sampling == "counter_hash" else 1e-10
+        assert np.allclose(got, ref, rtol=tol, atol=tol), (sampling, kw["model"], float(np.max(np.abs(got - ref))))
 
 
 def test_heston_pseudorandom_chunked_fp64(backend):
