@@ -238,21 +238,27 @@ __device__ __forceinline__ double icdf_f64(double p) {
                c3 = -2.549732539343734, c4 = 4.374664141464968, c5 = 2.938163982698783;
   const double d0 = 7.784695709041462e-3, d1 = 3.224671290700398e-1, d2 = 2.445134137142996,
                d3 = 3.754408661907416;
+  // Every product and sum is rounded separately (no FMA contraction), as the
+  // CPU reference evaluates it, so both give the same bits up to log().
   p = fmin(fmax(p, 2.2250738585072014e-308), 1.0 - 2.220446049250313e-16);
+  auto mad = [](double acc, double x, double c) { return __dadd_rn(__dmul_rn(acc, x), c); };
   if (p < 0.02425) {
-    double q = sqrt(-2.0 * log(p));
-    return (((((c0 * q + c1) * q + c2) * q + c3) * q + c4) * q + c5) /
-           ((((d0 * q + d1) * q + d2) * q + d3) * q + 1.0);
+    double q = sqrt(__dmul_rn(-2.0, log(p)));
+    double num = mad(mad(mad(mad(mad(c0, q, c1), q, c2), q, c3), q, c4), q, c5);
+    double den = mad(mad(mad(mad(d0, q, d1), q, d2), q, d3), q, 1.0);
+    return num / den;
   }
   if (p <= 1.0 - 0.02425) {
-    double q = p - 0.5;
-    double r = q * q;
-    return (((((a0 * r + a1) * r + a2) * r + a3) * r + a4) * r + a5) * q /
-           (((((b0 * r + b1) * r + b2) * r + b3) * r + b4) * r + 1.0);
+    double q = __dadd_rn(p, -0.5);
+    double r = __dmul_rn(q, q);
+    double num = __dmul_rn(mad(mad(mad(mad(mad(a0, r, a1), r, a2), r, a3), r, a4), r, a5), q);
+    double den = mad(mad(mad(mad(mad(b0, r, b1), r, b2), r, b3), r, b4), r, 1.0);
+    return num / den;
   }
-  double q = sqrt(-2.0 * log(1.0 - p));
-  return -(((((c0 * q + c1) * q + c2) * q + c3) * q + c4) * q + c5) /
-         ((((d0 * q + d1) * q + d2) * q + d3) * q + 1.0);
+  double q = sqrt(__dmul_rn(-2.0, log(__dadd_rn(1.0, -p))));
+  double num = mad(mad(mad(mad(mad(c0, q, c1), q, c2), q, c3), q, c4), q, c5);
+  double den = mad(mad(mad(mad(d0, q, d1), q, d2), q, d3), q, 1.0);
+  return -num / den;
 }
 
 // --------------------------------------------------------------- Halton ---
