@@ -131,14 +131,20 @@ def dist_setup(n_gpus: int):
     return rank, world, local, pg
 
 
-def reduce_max(pg, value: float, local: int) -> float:
+def reduce_max(pg, value: float, device: str) -> float:
+    """Max over ranks (device time of the slowest replica)."""
     if pg is None:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(world: int, path_steps_per_rank: int, steps: int, max_ms: float) -> float:
+    """Whole-job path-steps/s: every replica prices the same work (weak scaling)."""
+    return world * path_steps_per_rank * steps / (max_ms * 1e-3)
 
 
 def barrier(pg):
@@ -253,8 +259,9 @@ def run_ours(args) -> None:
             launches += n
     barrier(pg)
     clock_info = clocks.summary()
-    device_ms = reduce_max(pg, device_ms, local)
-    value = world * path_steps * args.steps / (device_ms * 1e-3)
+    dev = f"cuda:{local}"
+    device_ms = reduce_max(pg, device_ms, dev)
+    value = aggregate(world, path_steps, args.steps, device_ms)
 
     # end to end through the public ABI: host request structs in, results out
     e2e_s = 0.0
@@ -263,8 +270,8 @@ def run_ours(args) -> None:
         backend.price_batch(fused)
         e2e_s += time.perf_counter() - t0
     h2d, d2h = backend.last_transfer()
-    e2e_s = reduce_max(pg, e2e_s, local)
-    e2e_value = world * path_steps * args.steps / e2e_s
+    e2e_s = reduce_max(pg, e2e_s, dev)
+    e2e_value = aggregate(world, path_steps, args.steps, e2e_s * 1e3)
 
     # plain FP64 one-request-per-launch baseline (same requests, same seeds)
     plain_ms = 0.0
@@ -274,8 +281,8 @@ def run_ours(args) -> None:
     for _ in range(plain_steps):
         plain_results = backend.price_batch(plain)
         plain_ms += backend.last_timing()[0]
-    plain_ms = reduce_max(pg, plain_ms, local)
-    plain_value = world * path_steps * plain_steps / (plain_ms * 1e-3)
+    plain_ms = reduce_max(pg, plain_ms, dev)
+    plain_value = aggregate(world, path_steps, plain_steps, plain_ms)
 
     # roofline of the fused kernels (compute-bound: FP32 pipe and MUFU)
     fp32_peak, sfu_peak = backend.measure_peaks()

@@ -42,12 +42,19 @@ enum Workload : int32_t {
 struct SrcCtx {
   const uint32_t* sobol;
   const uint64_t* jump;
+  uint32_t* win;  // shared-memory window of Sobol tables (fused kernel), null elsewhere
 };
+
+// Dimensions of the Sobol tables staged in shared memory at a time (32 KB).
+constexpr uint32_t kSobolWindow = 64;
 
 // ------------------------------------------------------------- sources ----
 // A Source yields the samples of one unit (path or antithetic pair) by
 // dimension index.  n32/n64: standard normal in FP32 / FP64; u64: the raw
-// uniform (Merton's Poisson dimension).
+// uniform (Merton's Poisson dimension).  Models announce each step's
+// dimensions with at_step(first, count) before sampling them; every thread
+// of a block makes the same at_step calls, which lets the Sobol source stage
+// its tables block-synchronously.
 template <int S>
 struct Source;
 
@@ -59,6 +66,7 @@ struct Source<SMP_COUNTER> {
     seed = q.seed32;
     unit = (uint32_t)u;
   }
+  __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
   __device__ __forceinline__ float n32(uint32_t d) { return counter_normal_f32(seed, unit, d); }
   __device__ __forceinline__ double n64(uint32_t d) { return (double)counter_normal_f32(seed, unit, d); }
   __device__ __forceinline__ double u64(uint32_t d) {
@@ -74,14 +82,31 @@ struct Source<SMP_COUNTER> {
 template <>
 struct Source<SMP_SOBOL> {
   const uint32_t* table;
+  uint32_t* win;        // shared-memory window, or null to read the global table
+  uint32_t win_first;   // first dimension held in the window
   uint32_t local, block_seed, group, seed_g, combine_g;
   uint32_t off[8];
   template <bool FP64>
   __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
     table = c.sobol;
+    win = c.win;
+    win_first = 0xFFFFFFFFu;
     local = (uint32_t)(u & 0xFFFFu);
     block_seed = q.seed32 + (uint32_t)(u >> 16) * 0x9E3779B9u;
     group = 0xFFFFFFFFu;
+  }
+  // Block-synchronous: stages the tables of dimensions [d0, d0 + kSobolWindow)
+  // when this step's dimensions are not all in the window.
+  __device__ __forceinline__ void at_step(uint32_t d0, uint32_t count) {
+    if (!win) return;
+    if (win_first != 0xFFFFFFFFu && d0 >= win_first && d0 + count <= win_first + kSobolWindow) return;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kSobolWindow * 128; i += blockDim.x) {
+      const uint32_t dim = (d0 + (i >> 7)) & (MPC_SOBOL_TABLE_DIMS - 1);
+      win[i] = __ldg(table + dim * 128 + (i & 127));
+    }
+    __syncthreads();
+    win_first = d0;
   }
   __device__ __forceinline__ uint32_t sample(uint32_t d) {
     const uint32_t g = d / MPC_SOBOL_TABLE_DIMS;
@@ -94,10 +119,16 @@ struct Source<SMP_SOBOL> {
       combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
     }
     const uint32_t dim = d & (MPC_SOBOL_TABLE_DIMS - 1);
-    const uint32_t* td = table + dim * 128;
     uint32_t x = 0;
+    if (win) {
+      const uint32_t* td = win + (d - win_first) * 128;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) x ^= __ldg(td + off[q]);
+      for (int q = 0; q < 8; ++q) x ^= td[off[q]];
+    } else {
+      const uint32_t* td = table + dim * 128;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) x ^= __ldg(td + off[q]);
+    }
     return nested_uniform_scramble(x, seed_g ^ (dim + combine_g));  // hash_combine(seed_g, dim)
   }
   __device__ __forceinline__ float n32(uint32_t d) { return normcdfinvf(sobol_unit_f32(sample(d))); }
@@ -116,6 +147,7 @@ struct Source<SMP_HALTON> {
     primes = q.halton_primes;
     shifts = q.halton_shifts;
   }
+  __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
   __device__ __forceinline__ double u64(uint32_t d) { return halton_shifted(index, __ldg(primes + d), __ldg(shifts + d)); }
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
   __device__ __forceinline__ float n32(uint32_t d) {
@@ -134,6 +166,7 @@ struct Source<SMP_LHS> {
     n_paths = q.n_paths;
     dims = q.lhs;
   }
+  __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
   __device__ __forceinline__ double u64(uint32_t d) {
     LhsDim ld;
     ld.multiplier = __ldg(&dims[d].multiplier);
@@ -157,6 +190,7 @@ struct Source<SMP_XORSHIFT> {
     chunk_of(q, u, &seed, &local);
     st.seek(c.jump, seed, local * q.normals_per_unit, !FP64);
   }
+  __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
   // Sequential stream: dimensions must be requested in increasing order.
   __device__ __forceinline__ float n32(uint32_t) { return st.normal_f32(); }
   __device__ __forceinline__ double n64(uint32_t) { return st.normal_f64(); }
@@ -167,6 +201,7 @@ struct Source<SMP_XORSHIFT> {
 struct BufSource {
   const double* buf;
   uint64_t n_units, unit;
+  __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
   __device__ __forceinline__ double n64(uint32_t d) { return buf[(uint64_t)d * n_units + unit]; }
   __device__ __forceinline__ double u64(uint32_t d) { return buf[(uint64_t)d * n_units + unit]; }
   __device__ __forceinline__ float n32(uint32_t d) { return (float)n64(d); }
@@ -228,6 +263,7 @@ __device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double&
   bool ko0 = (W == W_DAO && q.s0 <= q.barrier) || (W == W_UAO && q.s0 >= q.barrier), ko1 = ko0;
   const uint32_t n = q.n_steps;
   for (uint32_t s = 0; s < n; ++s) {
+    src.at_step(s, 1);
     const Real z = normal<Real>(src, s);
     ls0 += drift + vol * z;
     if (anti) ls1 += drift - vol * z;
@@ -283,6 +319,7 @@ __device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double&
 // GBM terminal European (european_call_payoff_from_shock, cpu.rs:7773-7783).
 template <class Real, class Src>
 __device__ __forceinline__ void unit_gbm_terminal(const DevReq& q, Src& src, double& pay, double& ctl) {
+  src.at_step(0, 1);
   const Real z = normal<Real>(src, 0);
   const Real s0 = (Real)q.s0, drift = (Real)q.drift_dt, vol = (Real)q.vol_dt, kk = (Real)q.k,
              disc = (Real)q.discount;
@@ -307,6 +344,7 @@ __device__ __forceinline__ void unit_heston(const DevReq& q, Src& src, double& p
   Real ls0 = (Real)q.log_s0, ls1 = ls0, v0 = (Real)q.v0, v1 = v0;
   const uint32_t n = q.n_steps;
   for (uint32_t s = 0; s < n; ++s) {
+    src.at_step(2 * s, 2);
     const Real zv = normal<Real>(src, 2 * s);
     const Real zi = normal<Real>(src, 2 * s + 1);
     {
@@ -348,6 +386,7 @@ __device__ __forceinline__ void unit_merton(const DevReq& q, Src& src, double& p
   Real ls = (Real)q.log_s0;
   const uint32_t n = STEP ? q.n_steps : 1;
   for (uint32_t s = 0; s < n; ++s) {
+    src.at_step(3 * s, 3);
     const Real z = normal<Real>(src, 3 * s);
     const uint32_t jumps = poisson_inverse(src.u64(3 * s + 1), lam);
     ls += drift + vol * z;
@@ -373,6 +412,7 @@ __device__ __forceinline__ void unit_basket(const DevReq& q, Src& src, double& p
   uint32_t dim = 0;
   for (uint32_t s = 0; s < n; ++s) {
     Real z[8];
+    src.at_step(dim, d);
 #pragma unroll
     for (int a = 0; a < 8; ++a)
       if (a < (int)d) z[a] = normal<Real>(src, dim++);
@@ -417,6 +457,7 @@ __device__ __forceinline__ void unit_mlmc(const DevReq& q, Src& src, double& pay
     const Real drift = (Real)q.f_drift, vol = (Real)q.f_vol;
     Real ls = (Real)q.log_s0, acc = 0;
     for (uint32_t s = 0; s < q.n_steps; ++s) {
+      src.at_step(s, 1);
       ls += drift + vol * normal<Real>(src, s);
       acc += ex<Real>(ls);
     }
@@ -434,6 +475,7 @@ __device__ __forceinline__ void unit_mlmc(const DevReq& q, Src& src, double& pay
   uint32_t j = 0;
   for (uint64_t c = 0; c < q.coarse_steps; ++c) {
     Real zsum = 0;
+    src.at_step(j, M);
     for (uint32_t m = 0; m < M; ++m) {
       const Real z = normal<Real>(src, j++);
       zsum += z;
@@ -593,6 +635,8 @@ template <int FAM, int SMP>
 __global__ void __launch_bounds__(kFusedBlock) fused_kernel(const DevReq* __restrict__ reqs,
                                                             const Tile* __restrict__ tiles, uint32_t n_tiles,
                                                             uint32_t* __restrict__ counter, SrcCtx ctx) {
+  extern __shared__ uint32_t sobol_window[];
+  ctx.win = SMP == SMP_SOBOL ? sobol_window : nullptr;
   __shared__ DevReq sq;
   __shared__ double red[kWarps][5];
   __shared__ uint32_t s_tile;
@@ -614,12 +658,20 @@ __global__ void __launch_bounds__(kFusedBlock) fused_kernel(const DevReq* __rest
     double v[5] = {0, 0, 0, 0, 0};
     const bool cv = sq.cv != 0;
     double* per_unit = sq.per_unit;
-    for (uint64_t u = first + threadIdx.x; u < last; u += blockDim.x) {
+    // Every thread runs the same number of units so that block-synchronous
+    // sources stay in lockstep; a thread past the tile end repeats the first
+    // unit and discards it.
+    const uint32_t iters = (uint32_t)((last - first + blockDim.x - 1) / blockDim.x);
+    for (uint32_t it = 0; it < iters; ++it) {
+      uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
+      const bool valid = u < last;
+      if (!valid) u = first;
       double p, c;
       if constexpr (FAM >= 0)
         fused_unit<FAM, SMP>(sq, ctx, u, p, c);
       else
         fused_unit_any<SMP>(sq, ctx, u, p, c);
+      if (!valid) continue;
       v[0] += p;
       v[1] += p * p;
       if (cv) {
@@ -646,10 +698,15 @@ __global__ void __launch_bounds__(kFusedBlock) fused_kernel(const DevReq* __rest
   }
 }
 
+template <int SMP>
+constexpr size_t fused_dynamic_smem() {
+  return SMP == SMP_SOBOL ? kSobolWindow * 128 * sizeof(uint32_t) : 0;
+}
+
 template <int FAM, int SMP>
 static cudaError_t launch_fused_t(const DevReq* reqs, const Tile* tiles, uint32_t n_tiles, uint32_t* counter,
                                   const SrcCtx& ctx, int grid, int block, cudaStream_t stream) {
-  fused_kernel<FAM, SMP><<<grid, block, 0, stream>>>(reqs, tiles, n_tiles, counter, ctx);
+  fused_kernel<FAM, SMP><<<grid, block, fused_dynamic_smem<SMP>(), stream>>>(reqs, tiles, n_tiles, counter, ctx);
   count_launch();
   return cudaGetLastError();
 }
@@ -684,7 +741,7 @@ static cudaError_t launch_fused_s(int family, const DevReq* reqs, const Tile* ti
 cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_tiles, uint32_t* d_tile_counter,
                          int family, int sampler, const DeviceTables& tabs, int grid, int block,
                          cudaStream_t stream) {
-  SrcCtx ctx{tabs.sobol, tabs.jump};
+  SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
   if (block != kFusedBlock) return cudaErrorInvalidValue;
   switch (sampler) {
     case SMP_XORSHIFT:
@@ -705,7 +762,7 @@ cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_t
 template <int FAM, int SMP>
 static int occ_t(int block) {
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fused_kernel<FAM, SMP>, block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fused_kernel<FAM, SMP>, block, fused_dynamic_smem<SMP>());
   return n;
 }
 template <int SMP>
@@ -764,7 +821,7 @@ __global__ void __launch_bounds__(256) plain_generate_kernel(DevReq q, double* _
 
 cudaError_t launch_plain_generate(const DevReq& q, double* d_buf, int sampler, const DeviceTables& tabs,
                                   cudaStream_t stream) {
-  SrcCtx ctx{tabs.sobol, tabs.jump};
+  SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1220,7 +1277,7 @@ static cudaError_t launch_lsm_t(const LsmArgs& a, const SrcCtx& ctx, int* grid_u
 }
 
 cudaError_t launch_lsm(const LsmArgs& a, const DeviceTables& tabs, int* grid_used, cudaStream_t stream) {
-  SrcCtx ctx{tabs.sobol, tabs.jump};
+  SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
   if (a.n_steps > 511) return cudaErrorInvalidValue;
   if (a.fp64) {
     if (a.sampler == SMP_COUNTER) return launch_lsm_t<double, SMP_COUNTER>(a, ctx, grid_used, stream);
@@ -1251,7 +1308,7 @@ __global__ void __launch_bounds__(256) generate_kernel(DevReq q, int fp32, void*
 
 cudaError_t launch_generate_normals(const DevReq& q, int sampler, int fp32, void* d_out, uint64_t n_points,
                                     uint32_t dims, const DeviceTables& tabs, cudaStream_t stream) {
-  SrcCtx ctx{tabs.sobol, tabs.jump};
+  SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
   uint64_t want = (n_points + 255) / 256;
   int grid = (int)(want < 4096 ? want : 4096);
   if (grid < 1) grid = 1;

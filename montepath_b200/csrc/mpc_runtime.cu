@@ -160,6 +160,7 @@ int validate(const mpc_request_t& r, std::string* msg) {
     if (r.base_steps == 0) return invalid(msg, "base_steps must be > 0");
     if (r.levels == 0 || r.levels > MPC_MAX_LEVELS) return invalid(msg, "levels must be in 1..=16");
     if (r.refinement_factor < 2) return invalid(msg, "refinement_factor must be >= 2");
+    if (r.refinement_factor > 64) return unsupported(msg, "refinement_factor above 64 is not supported");
     if (r.scramble_replicates == 0) return invalid(msg, "scramble_replicates must be > 0");
     uint64_t fine = r.base_steps;
     for (uint32_t l = 1; l < r.levels; ++l) {
