@@ -72,6 +72,7 @@ struct Source<SMP_COUNTER> {
   __device__ __forceinline__ double u64(uint32_t d) {
     return (double)counter_open01(hash_u32(counter_mix(seed, unit, d, 0u)));
   }
+  __device__ __forceinline__ float u32(uint32_t d) { return counter_open01(hash_u32(counter_mix(seed, unit, d, 0u))); }
 };
 
 // Scrambled Sobol with the per-point work hoisted: the Owen-shuffled index
@@ -131,7 +132,8 @@ struct Source<SMP_SOBOL> {
     }
     return nested_uniform_scramble(x, seed_g ^ (dim + combine_g));  // hash_combine(seed_g, dim)
   }
-  __device__ __forceinline__ float n32(uint32_t d) { return normcdfinvf(sobol_unit_f32(sample(d))); }
+  __device__ __forceinline__ float n32(uint32_t d) { return icdf_fast(sobol_unit_f32(sample(d))); }
+  __device__ __forceinline__ float u32(uint32_t d) { return sobol_unit_f32(sample(d)); }
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(sobol_unit_f64(sample(d))); }
   __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sample(d)); }
 };
@@ -152,8 +154,9 @@ struct Source<SMP_HALTON> {
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
   __device__ __forceinline__ float n32(uint32_t d) {
     float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
-    return normcdfinvf(u);
+    return icdf_fast(u);
   }
+  __device__ __forceinline__ float u32(uint32_t d) { return (float)u64(d); }
 };
 
 template <>
@@ -177,8 +180,9 @@ struct Source<SMP_LHS> {
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
   __device__ __forceinline__ float n32(uint32_t d) {
     float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
-    return normcdfinvf(u);
+    return icdf_fast(u);
   }
+  __device__ __forceinline__ float u32(uint32_t d) { return (float)u64(d); }
 };
 
 template <>
@@ -195,6 +199,7 @@ struct Source<SMP_XORSHIFT> {
   __device__ __forceinline__ float n32(uint32_t) { return st.normal_f32(); }
   __device__ __forceinline__ double n64(uint32_t) { return st.normal_f64(); }
   __device__ __forceinline__ double u64(uint32_t) { return st.next_open01(); }
+  __device__ __forceinline__ float u32(uint32_t) { return (float)st.next_open01(); }
 };
 
 // Reads materialised samples [dim][unit] (FP64 plain path).
@@ -205,6 +210,7 @@ struct BufSource {
   __device__ __forceinline__ double n64(uint32_t d) { return buf[(uint64_t)d * n_units + unit]; }
   __device__ __forceinline__ double u64(uint32_t d) { return buf[(uint64_t)d * n_units + unit]; }
   __device__ __forceinline__ float n32(uint32_t d) { return (float)n64(d); }
+  __device__ __forceinline__ float u32(uint32_t d) { return (float)u64(d); }
 };
 
 template <class Real, class Src>
@@ -235,10 +241,11 @@ __device__ __forceinline__ Real sq_root(Real x) {
     return sqrt(x);
 }
 
-// sample_poisson by inversion with the uniform supplied (cpu.rs:932-953).
-__device__ __forceinline__ uint32_t poisson_inverse(double u, double mean) {
-  if (mean == 0.0) return 0;
-  double prob = exp(-mean), cum = prob;
+// sample_poisson by inversion with the uniform supplied (cpu.rs:932-953),
+// entered only when u > exp(-mean) (at least one jump); p0 = exp(-mean) is
+// precomputed on the host.
+__device__ __noinline__ uint32_t poisson_tail(double u, double mean, double p0) {
+  double prob = p0, cum = p0;
   uint32_t k = 0;
   while (u > cum && k < 4095u) {
     ++k;
@@ -382,13 +389,19 @@ __device__ __forceinline__ void unit_heston(const DevReq& q, Src& src, double& p
 template <class Real, bool STEP, class Src>
 __device__ __forceinline__ void unit_merton(const DevReq& q, Src& src, double& pay, double& ctl) {
   const Real drift = (Real)q.drift_dt, vol = (Real)q.vol_dt, jm = (Real)q.jump_mean, jv = (Real)q.jump_vol;
-  const double lam = q.lam_dt;
   Real ls = (Real)q.log_s0;
   const uint32_t n = STEP ? q.n_steps : 1;
   for (uint32_t s = 0; s < n; ++s) {
     src.at_step(3 * s, 3);
     const Real z = normal<Real>(src, 3 * s);
-    const uint32_t jumps = poisson_inverse(src.u64(3 * s + 1), lam);
+    uint32_t jumps;
+    if constexpr (sizeof(Real) == 4) {
+      const float u = src.u32(3 * s + 1);
+      jumps = u <= q.lam_p0_f ? 0u : poisson_tail((double)u, q.lam_dt, q.lam_p0);
+    } else {
+      const double u = src.u64(3 * s + 1);
+      jumps = u <= q.lam_p0 ? 0u : poisson_tail(u, q.lam_dt, q.lam_p0);
+    }
     ls += drift + vol * z;
     if (jumps > 0) {
       const Real zj = normal<Real>(src, 3 * s + 2);

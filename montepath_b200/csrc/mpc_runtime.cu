@@ -433,6 +433,9 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
     q.drift_dt = (r.r - kj - 0.5 * r.sigma * r.sigma) * dt;
     q.vol_dt = r.sigma * std::sqrt(dt);
     q.lam_dt = r.jump_intensity * dt;
+    q.lam_p0 = std::exp(-q.lam_dt);
+    q.lam_p0_f = float(q.lam_p0);
+    if (double(q.lam_p0_f) > q.lam_p0) q.lam_p0_f = std::nextafter(q.lam_p0_f, 0.0f);
     q.jump_mean = r.jump_mean;
     q.jump_vol = r.jump_volatility;
     q.normals_per_unit = 3ull * q.n_steps;

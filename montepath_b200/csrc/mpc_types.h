@@ -53,6 +53,9 @@ struct alignas(16) DevReq {
   double v0, kappa, theta, xi, rho, rho_perp, dt, sqrt_dt, rate;
   // Merton
   double jump_mean, jump_vol, lam_dt;
+  double lam_p0;   // exp(-lam_dt): no jump while u <= lam_p0
+  float lam_p0_f;  // largest float <= lam_p0 (exact FP32 test of the same event)
+  uint32_t _pad_m;
   // Basket: lower Cholesky factor and per-asset step constants
   double chol[64], b_drift[8], b_vol[8], spots[8], weights[8];
   // MLMC level
