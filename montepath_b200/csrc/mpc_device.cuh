@@ -227,8 +227,8 @@ __device__ __forceinline__ double sobol_unit_f64(uint32_t x) {
 
 // ------------------------------------------------------- Acklam inverse ---
 // inverse_standard_normal (cpu.rs:6012-6061): the reference rational in FP64.
-// The FP32 path uses icdf_fast below: the rational's 1.15e-9 relative error
-// is far below what FP32 resolves, so only the exact inverse matters there.
+// The FP32 path calls CUDA's normcdfinvf: the rational's 1.15e-9 relative
+// error is far below what FP32 resolves, so only the exact inverse matters there.
 __device__ __forceinline__ double icdf_f64(double p) {
   const double a0 = -3.969683028665376e1, a1 = 2.209460984245205e2, a2 = -2.759285104469687e2,
                a3 = 1.38357751867269e2, a4 = -3.066479806614716e1, a5 = 2.506628277459239;
@@ -259,45 +259,6 @@ __device__ __forceinline__ double icdf_f64(double p) {
   double num = mad(mad(mad(mad(mad(c0, q, c1), q, c2), q, c3), q, c4), q, c5);
   double den = mad(mad(mad(mad(d0, q, d1), q, d2), q, d3), q, 1.0);
   return -num / den;
-}
-
-// FP32 inverse normal CDF of the fused path: z = x * g(w) with x = 2u - 1
-// and w = -ln(4u(1-u)); g is a degree-9 polynomial in w for w < 5 (u in
-// (0.0017, 0.9983), one branch for nearly every lane of a warp) and in
-// sqrt(w) beyond.  Coefficients: Chebyshev least-squares fits against the
-// exact inverse (gen_icdf_coeffs.py), max relative error 3.1e-7 in FP32.
-__device__ __forceinline__ float icdf_fast(float u) {
-  const float x = 2.0f * u - 1.0f;
-  const float w = -__logf(4.0f * u * (1.0f - u));
-  float g;
-  if (w < 5.0f) {
-    const float t = w - 2.5f;
-    g = -1.235998749e-08f;
-    g = fmaf(g, t, 3.293115710e-08f);
-    g = fmaf(g, t, 6.582156229e-07f);
-    g = fmaf(g, t, -4.897925260e-06f);
-    g = fmaf(g, t, -7.014136516e-06f);
-    g = fmaf(g, t, 3.087891681e-04f);
-    g = fmaf(g, t, -1.771653801e-03f);
-    g = fmaf(g, t, -5.907721253e-03f);
-    g = fmaf(g, t, 3.488020423e-01f);
-    g = fmaf(g, t, 2.123313479e+00f);
-  } else {
-    float sw;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(sw) : "f"(w));
-    const float t = sw - 3.51594975f;
-    g = 3.604991201e-05f;
-    g = fmaf(g, t, 1.593232879e-05f);
-    g = fmaf(g, t, -3.732004057e-04f);
-    g = fmaf(g, t, 7.160452489e-04f);
-    g = fmaf(g, t, -8.584798099e-04f);
-    g = fmaf(g, t, 1.387827629e-03f);
-    g = fmaf(g, t, -2.834495800e-03f);
-    g = fmaf(g, t, 4.514224367e-03f);
-    g = fmaf(g, t, 1.424781295e+00f);
-    g = fmaf(g, t, 4.739812304e+00f);
-  }
-  return x * g;
 }
 
 // --------------------------------------------------------------- Halton ---

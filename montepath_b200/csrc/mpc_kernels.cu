@@ -132,7 +132,7 @@ struct Source<SMP_SOBOL> {
     }
     return nested_uniform_scramble(x, seed_g ^ (dim + combine_g));  // hash_combine(seed_g, dim)
   }
-  __device__ __forceinline__ float n32(uint32_t d) { return icdf_fast(sobol_unit_f32(sample(d))); }
+  __device__ __forceinline__ float n32(uint32_t d) { return normcdfinvf(sobol_unit_f32(sample(d))); }
   __device__ __forceinline__ float u32(uint32_t d) { return sobol_unit_f32(sample(d)); }
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(sobol_unit_f64(sample(d))); }
   __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sample(d)); }
@@ -154,7 +154,7 @@ struct Source<SMP_HALTON> {
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
   __device__ __forceinline__ float n32(uint32_t d) {
     float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
-    return icdf_fast(u);
+    return normcdfinvf(u);
   }
   __device__ __forceinline__ float u32(uint32_t d) { return (float)u64(d); }
 };
@@ -180,7 +180,7 @@ struct Source<SMP_LHS> {
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
   __device__ __forceinline__ float n32(uint32_t d) {
     float u = fminf(fmaxf((float)u64(d), 5.9604645e-08f), 0.99999994f);
-    return icdf_fast(u);
+    return normcdfinvf(u);
   }
   __device__ __forceinline__ float u32(uint32_t d) { return (float)u64(d); }
 };
@@ -244,7 +244,7 @@ __device__ __forceinline__ Real sq_root(Real x) {
 // sample_poisson by inversion with the uniform supplied (cpu.rs:932-953),
 // entered only when u > exp(-mean) (at least one jump); p0 = exp(-mean) is
 // precomputed on the host.
-__device__ __noinline__ uint32_t poisson_tail(double u, double mean, double p0) {
+__device__ __forceinline__ uint32_t poisson_tail(double u, double mean, double p0) {
   double prob = p0, cum = p0;
   uint32_t k = 0;
   while (u > cum && k < 4095u) {
@@ -645,7 +645,7 @@ __device__ void finalize_request(DevReq& q, double (*red)[5]) {
 // --------------------------------------------------------- fused kernel ---
 // FAM >= 0: every request in the list has that family; FAM < 0: switch per tile.
 template <int FAM, int SMP>
-__global__ void __launch_bounds__(kFusedBlock) fused_kernel(const DevReq* __restrict__ reqs,
+__global__ void __launch_bounds__(kFusedBlock, (FAM < 0 ? 2 : 4)) fused_kernel(const DevReq* __restrict__ reqs,
                                                             const Tile* __restrict__ tiles, uint32_t n_tiles,
                                                             uint32_t* __restrict__ counter, SrcCtx ctx) {
   extern __shared__ uint32_t sobol_window[];
