@@ -314,6 +314,28 @@ int mpc_last_transfer(const mpc_context_t* ctx, uint64_t* h2d_bytes, uint64_t* d
  * roofline denominators of the compute-bound fused kernels (no reference counterpart). */
 int mpc_measure_peaks(mpc_context_t* ctx, double* fp32_tflops, double* sfu_tops);
 
+/* Prices one FP32-path request like mpc_price, but allocates nothing: no
+ * context, no cudaMalloc/cudaFree, no pinned host buffers.  It is meant for
+ * callers that cannot let a library allocate device memory -- a service whose
+ * own allocator reserves the GPU's memory at start-up, or a latency-critical
+ * path where cudaMalloc/cudaFree (which can synchronise the device) are
+ * forbidden.  It has no counterpart in the reference.
+ *  - Runs on the current device and `stream` (a cudaStream_t, NULL = legacy
+ *    default stream) and returns after the result is on the host.
+ *  - Device buffers are file-scope static arrays of fixed size (about 0.6 MB
+ *    per GPU, held until the process exits): at most 16,777,216 paths (or
+ *    antithetic pairs) per request; larger requests return MPC_E_OOM_BUDGET.
+ *  - Samplers: pseudorandom, counter_hash, scrambled_sobol; path-payoff
+ *    workloads only (not LSM, MLMC or FP64-plain requests: MPC_E_UNSUPPORTED).
+ *  - The first call on a device resolves the arrays' device addresses and
+ *    uploads the lookup tables (set-up); make that first call before any
+ *    stream capture.
+ *  - All calls share the same arrays: calls that overlap on the GPU (other
+ *    streams, other host threads) race and must be serialised by the caller.
+ *  - error_message (optional) receives the reason for a non-zero status. */
+int mpc_price_fused_noalloc(const mpc_request_t* req, mpc_result_t* out, void* stream, char* error_message,
+                            size_t error_message_len);
+
 /* ----- serving ------------------------------------------------------------ */
 int mpc_server_start(mpc_context_t* ctx, const mpc_server_options_t* options, mpc_server_t** out);
 int mpc_submit(mpc_server_t* server, const mpc_request_t* req, uint64_t* ticket);

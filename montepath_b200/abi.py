@@ -312,6 +312,7 @@ FUNCTIONS = [
     ("mpc_last_timing", c_int, [c_void_p, POINTER(c_double), POINTER(c_uint64)]),
     ("mpc_last_transfer", c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64)]),
     ("mpc_measure_peaks", c_int, [c_void_p, POINTER(c_double), POINTER(c_double)]),
+    ("mpc_price_fused_noalloc", c_int, [POINTER(Request), POINTER(Result), c_void_p, c_char_p, c_size_t]),
     ("mpc_server_start", c_int, [c_void_p, POINTER(ServerOptions), POINTER(c_void_p)]),
     ("mpc_submit", c_int, [c_void_p, POINTER(Request), POINTER(c_uint64)]),
     ("mpc_poll", c_int, [c_void_p, c_uint64, POINTER(Result)]),

@@ -1093,7 +1093,7 @@ static int price_one(mpc_context* ctx, const mpc_request_t* req, mpc_result_t* o
 }
 
 // ----------------------------------------------------------- device setup ---
-static void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {
+void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {
   sob.assign(size_t(MPC_SOBOL_TABLE_DIMS) * 8 * 16, 0u);
   for (int d = 0; d < MPC_SOBOL_TABLE_DIMS; ++d)
     for (int q = 0; q < 8; ++q)

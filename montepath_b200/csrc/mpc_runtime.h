@@ -87,6 +87,9 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
 uint64_t estimate_bytes(const mpc_request_t& r);
 Shape choose_shape(mpc_context* ctx, const Prepared& p);
 void summarize_moments(const Prepared& p, const double* m, mpc_result_t* out);
+// Host copies of the device lookup tables: Sobol nibble tables [256][8][16]
+// and xorshift64* jump-ahead nibble tables [64][16][16].
+void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump);
 // Fused FP32 requests: one persistent launch per (sampler, family) group on the context stream.
 int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_result_t*>& outs,
               double* per_unit_host, uint64_t per_unit_cap);
