@@ -241,6 +241,9 @@ def run_ours(args) -> None:
     backend = CudaBackend(local)
     fused = requests("fp32_path")
     plain = requests("fp64_plain")
+    if args.paths:
+        for r in fused + plain:
+            r.n_paths = args.paths
     path_steps = sum(r.n_paths * r.n_steps for r in fused)
 
     for _ in range(max(args.warmup, 3)):
@@ -274,15 +277,16 @@ def run_ours(args) -> None:
     e2e_value = aggregate(world, path_steps, args.steps, e2e_s * 1e3)
 
     # plain FP64 one-request-per-launch baseline (same requests, same seeds)
-    plain_ms = 0.0
-    plain_steps = max(1, min(2, args.steps))
-    backend.price_batch(plain)
-    plain_results = None
-    for _ in range(plain_steps):
-        plain_results = backend.price_batch(plain)
-        plain_ms += backend.last_timing()[0]
-    plain_ms = reduce_max(pg, plain_ms, dev)
-    plain_value = aggregate(world, path_steps, plain_steps, plain_ms)
+    plain_value = plain_ms = plain_results = None
+    if not args.no_plain:
+        plain_ms = 0.0
+        plain_steps = max(1, min(2, args.steps))
+        backend.price_batch(plain)
+        for _ in range(plain_steps):
+            plain_results = backend.price_batch(plain)
+            plain_ms += backend.last_timing()[0]
+        plain_ms = reduce_max(pg, plain_ms, dev) / plain_steps
+        plain_value = aggregate(world, path_steps, 1, plain_ms)
 
     # roofline of the fused kernels (compute-bound: FP32 pipe and MUFU)
     fp32_peak, sfu_peak = backend.measure_peaks()
@@ -300,7 +304,6 @@ def run_ours(args) -> None:
 
     heston_ref = O.heston_call(100, 100, 0.03, 0.04, 2.0, 0.04, 0.5, -0.7, 1.0)
     merton_ref = O.merton_series(100, 100, 0.03, 0.2, 0.5, -0.1, 0.15, 1.0, exact=True)
-    line = None
     if rank == 0:
         line = {
             "metric": "path-steps/s",
@@ -317,7 +320,7 @@ def run_ours(args) -> None:
             "data": "synthetic (seeded scrambled Sobol samples generated on the device)",
             "config": {
                 "workload": WORKLOAD,
-                "paths": N_PATHS,
+                "paths": fused[0].n_paths,
                 "steps_per_path": N_STEPS,
                 "requests_per_step": 2,
                 "precision": "fp32_path",
@@ -338,21 +341,129 @@ def run_ours(args) -> None:
                 "peak_source": "measured by mpc_measure_peaks on this GPU (FP32 FMA chains / MUFU ex2 chains)",
                 "hbm_peak_gbs": load_peaks().get("hbm_gbs"),
             },
-            "plain_fp64": {"value": plain_value, "unit": "path-steps/s", "ms_per_step": plain_ms / plain_steps,
-                           "speedup_fused_vs_plain": value / plain_value},
             "prices": {
-                "heston": {"price": results[0].price, "stderr": results[0].stderr,
-                           "fp64_plain": plain_results[0].price, "semi_analytic": heston_ref},
-                "merton": {"price": results[1].price, "stderr": results[1].stderr,
-                           "fp64_plain": plain_results[1].price, "series": merton_ref},
+                "heston": {"price": results[0].price, "stderr": results[0].stderr, "semi_analytic": heston_ref},
+                "merton": {"price": results[1].price, "stderr": results[1].stderr, "series": merton_ref},
             },
         }
+        if plain_value is not None:
+            line["plain_fp64"] = {"value": plain_value, "unit": "path-steps/s", "ms_per_step": plain_ms,
+                                  "speedup_fused_vs_plain": value / plain_value}
+            line["prices"]["heston"]["fp64_plain"] = plain_results[0].price
+            line["prices"]["merton"]["fp64_plain"] = plain_results[1].price
+        legs = [x for x in args.legs.split(",") if x and x != "none"]
+        if "all" in legs:
+            legs = ["config1", "config3", "config4", "config5"]
+        if legs:
+            line["configs"] = {}
+            for leg in legs:
+                line["configs"][leg] = LEGS[leg](backend)
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     backend.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def _timed(backend, fn):
+    res = fn()
+    return res, backend.last_timing()[0]
+
+
+def leg_config1(backend) -> dict:
+    """Plain method, small: GBM European 20,000 x 64, seed 42, pseudorandom (the
+    reference's MonteCarloRng stream replayed), FP64 one request per launch."""
+
+    from montepath_b200.requests import make_request
+    from oracle import oracle as O
+
+    cfg = dict(method="stepwise", n_paths=20000, n_steps=64, seed=42, n_threads=1)
+    r64 = make_request("european_call", dict(cfg, precision="fp64_plain"))
+    r32 = make_request("european_call", dict(cfg, precision="fp32_path"))
+    for _ in range(3):
+        backend.price(r64)
+        backend.price(r32)
+    a, t64 = _timed(backend, lambda: backend.price(r64))
+    b, t32 = _timed(backend, lambda: backend.price(r32))
+    t0 = time.perf_counter()
+    c = O.price(r64)
+    t_cpu = time.perf_counter() - t0
+    bs = 9.413403383853016
+    ps = 20000 * 64
+    return {
+        "fp64_plain": {"price": a.price, "stderr": a.stderr, "ms": t64, "path_steps_per_sec": ps / (t64 * 1e-3),
+                       "err_vs_black_scholes_se": (a.price - bs) / a.stderr, "abs_diff_vs_oracle": abs(a.price - c.price)},
+        "fp32_path": {"price": b.price, "stderr": b.stderr, "ms": t32, "path_steps_per_sec": ps / (t32 * 1e-3)},
+        "cpu_oracle_1_thread": {"price": c.price, "seconds": t_cpu, "path_steps_per_sec": ps / t_cpu},
+    }
+
+
+def leg_config3(backend) -> dict:
+    """American put by Longstaff-Schwartz, 524,288 paths x 50 dates, S0 in {90, 100, 110}."""
+
+    from montepath_b200.requests import make_request
+    from oracle import oracle as O
+
+    out = {}
+    for s0 in (90.0, 100.0, 110.0):
+        row = {"crr_2048": O.crr_put(s0, 100.0, 0.06, 0.2, 1.0, 2048)}
+        for precision in ("fp32_path", "fp64_plain"):
+            r = make_request("american_put", dict(s0=s0, k=100.0, r=0.06, sigma=0.2, t=1.0, n_paths=524288,
+                                                  n_steps=50, basis_degree=3, seed=42, precision=precision))
+            backend.price(r)
+            res, ms = _timed(backend, lambda: backend.price(r))
+            row[precision] = {"price": res.price, "stderr": res.stderr, "ms": ms,
+                              "path_steps_per_sec": 524288 * 50 / (ms * 1e-3),
+                              "early_exercise": res.early_exercise_count, "regressions": res.regression_steps}
+        out[f"s0_{int(s0)}"] = row
+    return out
+
+
+def leg_config4(backend) -> dict:
+    """4,096-contract heterogeneous book in one batched launch vs plain FP64
+    per-request launches (timed on every 64th contract, extrapolated)."""
+
+    from montepath_b200 import workloads
+    from montepath_b200.requests import copy_request
+
+    book = workloads.book(42)
+    total = workloads.book_path_steps(book)
+    backend.price_batch(book)
+    res, ms = _timed(backend, lambda: backend.price_batch(book))
+    _, launches = backend.last_timing()
+    sample = book[::64]
+    plain_ms = 0.0
+    for r in sample:
+        p = copy_request(r)
+        p.precision = 0
+        backend.price(p)
+        plain_ms += backend.last_timing()[0]
+    sample_steps = workloads.book_path_steps(sample)
+    plain_rate = sample_steps / (plain_ms * 1e-3)
+    return {
+        "contracts": len(book),
+        "path_steps": total,
+        "batched_fp32": {"ms": ms, "path_steps_per_sec": total / (ms * 1e-3), "kernel_launches": launches},
+        "plain_fp64_sampled": {"contracts_timed": len(sample), "ms_sample": plain_ms, "path_steps_per_sec": plain_rate,
+                               "estimated_ms_full_book": total / plain_rate * 1e3},
+        "speedup_batched_vs_plain": (total / (ms * 1e-3)) / plain_rate,
+        "price_checksum": sum(x.price for x in res),
+    }
+
+
+def leg_config5(backend) -> dict:
+    """Poisson serving stream at 2,000 requests/s: continuous batching on a
+    2 s slice of arrivals, plain FIFO FP64 on a 0.25 s slice."""
+
+    from montepath_b200 import serving, workloads
+
+    fused = serving.replay(backend, workloads.serving_stream(42, duration_s=2.0))
+    plain = serving.replay(backend, workloads.serving_stream(42, duration_s=0.25, precision="fp64_plain"), plain=True)
+    return {"continuous_batching": fused, "plain_fifo": plain}
+
+
+LEGS = {"config1": leg_config1, "config3": leg_config3, "config4": leg_config4, "config5": leg_config5}
 
 
 def main() -> None:
@@ -362,6 +473,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain comparison of the headline")
+    ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling cases)")
+    ap.add_argument("--legs", default="all", help="comma list of config1,config3,config4,config5, all or none")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -1,0 +1,79 @@
+"""Open-loop load generator for the serving loop: submits a timed request
+stream to an ``mpc_server`` at its arrival times and reports latency
+percentiles and throughput from the server's own timestamps."""
+
+from __future__ import annotations
+
+import threading
+import time
+from typing import Sequence
+
+from . import abi
+from .backend import CudaBackend
+
+
+def replay(backend: CudaBackend, stream: Sequence[tuple[float, str, abi.Request]], plain: bool = False,
+           hbm_budget_bytes: int = 64 << 30, max_slots: int = 256, drain_timeout_s: float = 600.0) -> dict:
+    """Runs the stream (arrival seconds, kind, request) through a fresh server.
+
+    Arrivals are open-loop: submissions follow the schedule whether or not
+    earlier requests have finished.  Returns a summary with per-kind latency
+    percentiles, throughput in path-steps/s and the server statistics.
+    """
+
+    tickets: list[tuple[int, str, abi.Request]] = []
+    lock = threading.Lock()
+    with backend.server(hbm_budget_bytes=hbm_budget_bytes, max_slots=max_slots, plain=plain) as srv:
+        t0 = time.perf_counter()
+        lag = 0.0
+        for arrival, kind, req in stream:
+            delay = arrival - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            else:
+                lag = max(lag, -delay)
+            ticket = srv.submit(req)
+            with lock:
+                tickets.append((ticket, kind, req))
+        submitted_at = time.perf_counter() - t0
+        results = []
+        for ticket, kind, req in tickets:
+            res = srv.wait(ticket, timeout_ms=int(drain_timeout_s * 1000))
+            results.append((kind, req, res))
+        wall = time.perf_counter() - t0
+        stats = srv.stats()
+    lat_all = sorted(r.t_complete_ms - r.t_enqueue_ms for _, _, r in results)
+
+    def pct(values, q):
+        if not values:
+            return None
+        pos = q * (len(values) - 1)
+        lo = int(pos)
+        hi = min(lo + 1, len(values) - 1)
+        return values[lo] + (values[hi] - values[lo]) * (pos - lo)
+
+    per_kind = {}
+    for kind in sorted({k for k, _, _ in results}):
+        lat = sorted(r.t_complete_ms - r.t_enqueue_ms for k, _, r in results if k == kind)
+        per_kind[kind] = {"count": len(lat), "p50_ms": pct(lat, 0.5), "p99_ms": pct(lat, 0.99)}
+    path_steps = sum(r.path_steps for _, _, r in results)
+    span_s = (max(r.t_complete_ms for _, _, r in results) - min(r.t_enqueue_ms for _, _, r in results)) / 1e3
+    return {
+        "mode": "plain_fifo_fp64" if plain else "continuous_batching_fp32",
+        "requests": len(results),
+        "offered_seconds": stream[-1][0] if stream else 0.0,
+        "submit_lag_max_ms": lag * 1e3,
+        "submitted_s": submitted_at,
+        "wall_s": wall,
+        "p50_ms": pct(lat_all, 0.5),
+        "p99_ms": pct(lat_all, 0.99),
+        "max_ms": lat_all[-1] if lat_all else None,
+        "per_kind": per_kind,
+        "path_steps": path_steps,
+        "path_steps_per_sec": path_steps / span_s if span_s > 0 else None,
+        "busy_ms": stats.busy_ms,
+        "waves": stats.waves,
+        "peak_bytes": stats.peak_bytes,
+        "mlmc_target_met": sum(1 for k, _, r in results if k == "asian_mlmc" and r.target_met),
+        "mlmc_requests": sum(1 for k, _, _ in results if k == "asian_mlmc"),
+    }
