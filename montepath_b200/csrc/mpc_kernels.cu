@@ -643,9 +643,16 @@ __device__ void finalize_request(DevReq& q, double (*red)[5]) {
 }
 
 // --------------------------------------------------------- fused kernel ---
+// Resident blocks per SM the register allocation must allow: the
+// family-switching instance is the widest; the GBM and terminal families
+// with the counter-hash generator are long serial chains that want more warps.
+constexpr int fused_min_blocks(int fam, int smp) {
+  return fam < 0 ? 2 : ((fam == FAM_GBM_STEP || fam == FAM_GBM_TERMINAL) && smp == SMP_COUNTER ? 6 : 4);
+}
+
 // FAM >= 0: every request in the list has that family; FAM < 0: switch per tile.
 template <int FAM, int SMP>
-__global__ void __launch_bounds__(kFusedBlock, (FAM < 0 ? 2 : 4)) fused_kernel(const DevReq* __restrict__ reqs,
+__global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused_kernel(const DevReq* __restrict__ reqs,
                                                             const Tile* __restrict__ tiles, uint32_t n_tiles,
                                                             uint32_t* __restrict__ counter, SrcCtx ctx) {
   extern __shared__ uint32_t sobol_window[];

@@ -603,16 +603,15 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
     q.tiles_done = static_cast<uint32_t*>(d_done) + i;
     q.per_unit = (per_unit_host && i == 0) ? static_cast<double*>(d_unit) : nullptr;
   }
-  // Launch groups.  A kernel instance is compiled per (family, sampler); a
-  // small batch launches one specialised kernel per pair (lower register
-  // pressure), a large heterogeneous book one persistent kernel per sampler
-  // that switches on each tile's family.  Within a group tiles are ordered
-  // by per-tile cost, longest first.
+  // Launch groups: one persistent launch of the specialised kernel instance
+  // per (sampler, family) pair present in the batch (a heterogeneous book of
+  // GBM payoffs and baskets is two launches); within a group tiles are
+  // ordered by per-tile cost, longest first.
   struct Group {
     int sampler, family;
     std::vector<size_t> members;
   };
-  const bool split_families = n <= 16;
+  const bool split_families = true;
   std::vector<Group> gl;
   for (size_t i = 0; i < n; ++i) {
     Group* g = nullptr;
