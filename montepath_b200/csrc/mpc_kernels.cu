@@ -1011,17 +1011,17 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Grid barrier for a cooperative launch.  The wait is bounded: after
-// timeout_ns the block records the failure in *error and every block leaves
-// the kernel at the next check.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* error, uint64_t timeout_ns) {
+// Barrier over the `nblocks` blocks of one job of a cooperative launch.  The
+// wait is bounded: after timeout_ns the block records the failure in *error
+// and every block of the job leaves the kernel at the next check.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* error, uint64_t timeout_ns, uint32_t nblocks) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* gen = bar + 1;
     const unsigned g = *gen;
     __threadfence();
-    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+    if (atomicAdd(bar, 1u) == nblocks - 1) {
       atomicExch(bar, 0u);
       __threadfence();
       atomicAdd(bar + 1, 1u);
@@ -1090,23 +1090,33 @@ __device__ bool solve4(double a[4][4], double rhs[4], int dim) {
   return true;
 }
 
-constexpr int kLsmBlock = 256;
-constexpr int kLsmMaxP = 8;
+constexpr int kLsmBlock = (int)kLsmThreads;
+constexpr int kLsmMaxP = (int)kLsmPathsPerThreadMax;
 constexpr int kLsmMom = 15;  // 10 unique A^T A, 4 A^T b, ITM count
 
 template <class Real, int SMP>
-__global__ void __launch_bounds__(kLsmBlock) lsm_kernel(LsmArgs a, SrcCtx ctx) {
+__global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restrict__ jobs, uint32_t n_jobs, SrcCtx ctx) {
   __shared__ double red[kWarps][5];
   __shared__ double s_mom[16];
   __shared__ double s_beta[4];
   __shared__ int s_ok;
+  __shared__ uint32_t s_job;
   __shared__ Real s_disc[512];
+  if (threadIdx.x == 0) {
+    uint32_t j = 0;
+    while (j + 1 < n_jobs && blockIdx.x >= jobs[j + 1].block_first) ++j;
+    s_job = j;
+  }
+  __syncthreads();
+  const LsmArgs a = jobs[s_job];
+  const uint32_t nb = a.n_blocks;             // blocks of this job
+  const uint32_t lb = blockIdx.x - a.block_first;  // block index within the job
   const uint64_t n = a.n_paths;
   const uint32_t steps = a.n_steps;
   for (uint32_t j = threadIdx.x; j <= steps && j < 512; j += blockDim.x) s_disc[j] = (Real)a.disc_pow[j];
   __syncthreads();
-  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
-  const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint64_t nthreads = (uint64_t)nb * blockDim.x;
+  const uint64_t gtid = (uint64_t)lb * blockDim.x + threadIdx.x;
   Real* paths = reinterpret_cast<Real*>(a.paths);
   const Real k = (Real)a.k, drift = (Real)a.drift, vol = (Real)a.vol, inv_k = (Real)(1.0 / fmax(a.k, 2.2250738585072014e-308));
   const int coeffs = (int)a.degree + 1;
@@ -1163,7 +1173,7 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(LsmArgs a, SrcCtx ctx) {
       m[14] += 1.0;
     }
     // block reduction of the 15 moments in three rounds of five
-    double* part = a.partials + ((size_t)buf * gridDim.x + blockIdx.x) * 16;
+    double* part = a.partials + ((size_t)buf * nb + lb) * 16;
     for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
       double v[5] = {m[r0], m[r0 + 1], m[r0 + 2], m[r0 + 3], m[r0 + 4]};
       block_reduce5(v, red);
@@ -1171,14 +1181,14 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(LsmArgs a, SrcCtx ctx) {
         for (int i = 0; i < 5; ++i) part[r0 + i] = v[i];
       __syncthreads();
     }
-    if (!grid_barrier(a.barrier, a.error, a.timeout_ns)) return;
+    if (!grid_barrier(a.barrier, a.error, a.timeout_ns, nb)) return;
     // every block sums the block partials in the same fixed order (identical result everywhere)
     {
       double acc[kLsmMom];
 #pragma unroll
       for (int i = 0; i < kLsmMom; ++i) acc[i] = 0.0;
-      const double* base = a.partials + (size_t)buf * gridDim.x * 16;
-      for (uint32_t blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
+      const double* base = a.partials + (size_t)buf * nb * 16;
+      for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x)
 #pragma unroll
         for (int i = 0; i < kLsmMom; ++i) acc[i] += __ldcg(base + (size_t)blk * 16 + i);
       for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
@@ -1247,16 +1257,16 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(LsmArgs a, SrcCtx ctx) {
   }
   block_reduce5(v, red);
   if (threadIdx.x == 0) {
-    double* fp = a.final_partials + (size_t)blockIdx.x * 4;
+    double* fp = a.final_partials + (size_t)lb * 4;
     for (int i = 0; i < 4; ++i) fp[i] = v[i];
     __threadfence();
-    s_ok = atomicAdd(a.done, 1u) == gridDim.x - 1;
+    s_ok = atomicAdd(a.done, 1u) == nb - 1;
   }
   __syncthreads();
   if (s_ok) {
     __threadfence();
     double acc[5] = {0, 0, 0, 0, 0};
-    for (uint32_t blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
+    for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x)
       for (int i = 0; i < 4; ++i) acc[i] += __ldcg(a.final_partials + (size_t)blk * 4 + i);
     block_reduce5(acc, red);
     if (threadIdx.x != 0) return;
@@ -1271,40 +1281,42 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(LsmArgs a, SrcCtx ctx) {
 }
 
 template <class Real, int SMP>
-static cudaError_t launch_lsm_t(const LsmArgs& a, const SrcCtx& ctx, int* grid_used, cudaStream_t stream) {
+static uint32_t lsm_capacity_t() {
   int dev = 0, sms = 148, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lsm_kernel<Real, SMP>, kLsmBlock, 0);
-  if (per_sm < 1) return cudaErrorLaunchOutOfResources;
-  uint64_t need = (a.n_paths + (uint64_t)kLsmBlock * kLsmMaxP - 1) / ((uint64_t)kLsmBlock * kLsmMaxP);
-  uint64_t cap = (uint64_t)sms * (uint64_t)per_sm;
-  if (need > cap) return cudaErrorInvalidValue;  // more paths than co-resident threads x kLsmMaxP
-  // about two blocks per SM keeps the per-date barrier and partial sums cheap
-  uint64_t grid = (uint64_t)sms * 2 < cap ? (uint64_t)sms * 2 : cap;
-  uint64_t useful = (a.n_paths + kLsmBlock - 1) / kLsmBlock;
-  if (grid > useful) grid = useful;
-  if (grid < need) grid = need;
-  if (grid < 1) grid = 1;
-  *grid_used = (int)grid;
-  LsmArgs args = a;
+  return per_sm > 0 ? (uint32_t)(sms * per_sm) : 0u;
+}
+
+uint32_t lsm_capacity(int fp64, int sampler) {
+  if (fp64) return sampler == SMP_COUNTER ? lsm_capacity_t<double, SMP_COUNTER>() : lsm_capacity_t<double, SMP_XORSHIFT>();
+  return sampler == SMP_COUNTER ? lsm_capacity_t<float, SMP_COUNTER>() : lsm_capacity_t<float, SMP_XORSHIFT>();
+}
+
+template <class Real, int SMP>
+static cudaError_t launch_lsm_t(const LsmArgs* jobs, uint32_t n_jobs, uint32_t total_blocks, const SrcCtx& ctx,
+                                cudaStream_t stream) {
+  if (total_blocks == 0 || total_blocks > lsm_capacity_t<Real, SMP>()) return cudaErrorInvalidValue;
+  const LsmArgs* j = jobs;
+  uint32_t nj = n_jobs;
   SrcCtx c = ctx;
-  void* params[] = {&args, &c};
-  cudaError_t err = cudaLaunchCooperativeKernel((const void*)lsm_kernel<Real, SMP>, dim3((unsigned)grid),
+  void* params[] = {&j, &nj, &c};
+  cudaError_t err = cudaLaunchCooperativeKernel((const void*)lsm_kernel<Real, SMP>, dim3(total_blocks),
                                                 dim3(kLsmBlock), params, 0, stream);
   count_launch();
   return err;
 }
 
-cudaError_t launch_lsm(const LsmArgs& a, const DeviceTables& tabs, int* grid_used, cudaStream_t stream) {
+cudaError_t launch_lsm_batch(const LsmArgs* d_jobs, uint32_t n_jobs, uint32_t total_blocks, int fp64, int sampler,
+                             const DeviceTables& tabs, cudaStream_t stream) {
   SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
-  if (a.n_steps > 511) return cudaErrorInvalidValue;
-  if (a.fp64) {
-    if (a.sampler == SMP_COUNTER) return launch_lsm_t<double, SMP_COUNTER>(a, ctx, grid_used, stream);
-    return launch_lsm_t<double, SMP_XORSHIFT>(a, ctx, grid_used, stream);
+  if (fp64) {
+    if (sampler == SMP_COUNTER) return launch_lsm_t<double, SMP_COUNTER>(d_jobs, n_jobs, total_blocks, ctx, stream);
+    return launch_lsm_t<double, SMP_XORSHIFT>(d_jobs, n_jobs, total_blocks, ctx, stream);
   }
-  if (a.sampler == SMP_COUNTER) return launch_lsm_t<float, SMP_COUNTER>(a, ctx, grid_used, stream);
-  return launch_lsm_t<float, SMP_XORSHIFT>(a, ctx, grid_used, stream);
+  if (sampler == SMP_COUNTER) return launch_lsm_t<float, SMP_COUNTER>(d_jobs, n_jobs, total_blocks, ctx, stream);
+  return launch_lsm_t<float, SMP_XORSHIFT>(d_jobs, n_jobs, total_blocks, ctx, stream);
 }
 
 // ------------------------------------------------------------ generators ---

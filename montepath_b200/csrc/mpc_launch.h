@@ -51,8 +51,18 @@ struct LsmArgs {
   unsigned* done;            // last-block counter
   int* error;                // barrier timeout flag
   uint64_t timeout_ns;
+  uint32_t block_first;      // this job's blocks in the batched launch
+  uint32_t n_blocks;
 };
-cudaError_t launch_lsm(const LsmArgs& a, const DeviceTables& tabs, int* grid_used, cudaStream_t stream);
+// Several LSM requests in one cooperative launch: job j owns blocks
+// [block_first, block_first + n_blocks) and synchronises only them.  All jobs
+// of a launch share precision (fp64) and sampler.
+cudaError_t launch_lsm_batch(const LsmArgs* d_jobs, uint32_t n_jobs, uint32_t total_blocks, int fp64, int sampler,
+                             const DeviceTables& tabs, cudaStream_t stream);
+// Co-resident LSM blocks on the device for (fp64, sampler); 0 if the kernel cannot launch.
+uint32_t lsm_capacity(int fp64, int sampler);
+constexpr uint32_t kLsmPathsPerThreadMax = 8;
+constexpr uint32_t kLsmThreads = 256;
 
 // Device generators for the ABI's sampler entry points.
 cudaError_t launch_generate_normals(const DevReq& q, int sampler, int fp32, void* d_out, uint64_t n_points,

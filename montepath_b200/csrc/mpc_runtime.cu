@@ -753,114 +753,217 @@ static double powi(double a, int b) {  // f64::powi as compiler-rt __powidf2
   return recip ? 1.0 / r : r;
 }
 
-static int run_lsm(mpc_context* ctx, const mpc_request_t& r, mpc_result_t* out, double* per_unit_host) {
-  (void)per_unit_host;
-  const uint32_t degree = std::min<uint32_t>(std::max<uint32_t>(r.basis_degree, 1), 3);
+// Exercise schedule: every step (American, cpu.rs:3950) or the normalised
+// Bermudan dates (normalize_bermudan_exercise_schedule, cpu.rs:5155-5183).
+static std::vector<uint32_t> lsm_schedule(const mpc_request_t& r, bool* normalised) {
   std::vector<uint32_t> sched;
-  bool normalised = false;
+  *normalised = false;
   if (r.workload == MPC_WORKLOAD_AMERICAN_PUT) {
     for (uint32_t s = 1; s <= r.n_steps; ++s) sched.push_back(s);
-  } else {  // normalize_bermudan_exercise_schedule (cpu.rs:5155-5183)
-    std::vector<uint32_t> in(r.exercise_steps, r.exercise_steps + r.n_exercise);
-    sched = in;
-    std::sort(sched.begin(), sched.end());
-    sched.erase(std::unique(sched.begin(), sched.end()), sched.end());
-    if (sched != in) normalised = true;
-    if (std::find(sched.begin(), sched.end(), r.n_steps) == sched.end()) {
-      sched.push_back(r.n_steps);
-      normalised = true;
+    return sched;
+  }
+  std::vector<uint32_t> in(r.exercise_steps, r.exercise_steps + r.n_exercise);
+  sched = in;
+  std::sort(sched.begin(), sched.end());
+  sched.erase(std::unique(sched.begin(), sched.end()), sched.end());
+  if (sched != in) *normalised = true;
+  if (std::find(sched.begin(), sched.end(), r.n_steps) == sched.end()) {
+    sched.push_back(r.n_steps);
+    *normalised = true;
+  }
+  return sched;
+}
+
+// Longstaff-Schwartz for a batch of requests (price_put_lsm_cpu,
+// cpu.rs:3813-3945): requests are packed into cooperative launches, each
+// request owning enough co-resident blocks for <= 8 paths per thread.
+int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& reqs,
+                  const std::vector<mpc_result_t*>& outs) {
+  struct Job {
+    size_t index;
+    std::vector<uint32_t> sched;
+    std::vector<double> disc_pow;
+    bool normalised;
+    uint32_t degree, blocks;
+    int fp64, sampler;
+    LsmArgs args;
+  };
+  std::vector<Job> jobs(reqs.size());
+  for (size_t i = 0; i < reqs.size(); ++i) {
+    const mpc_request_t& r = *reqs[i];
+    Job& j = jobs[i];
+    j.index = i;
+    j.sched = lsm_schedule(r, &j.normalised);
+    j.degree = std::min<uint32_t>(std::max<uint32_t>(r.basis_degree, 1), 3);
+    j.fp64 = r.precision == MPC_PRECISION_FP64_PLAIN;
+    j.sampler = sampler_of(r.sampling);
+    const double dt = r.t / double(r.n_steps);
+    const double disc_step = std::exp(-r.r * dt);
+    j.disc_pow.resize(r.n_steps + 1);
+    for (uint32_t k = 0; k <= r.n_steps; ++k) j.disc_pow[k] = powi(disc_step, int(k));
+    const uint32_t cap = lsm_capacity(j.fp64, j.sampler);
+    const uint64_t per_block_max = uint64_t(kLsmThreads) * kLsmPathsPerThreadMax;
+    const uint64_t need = (r.n_paths + per_block_max - 1) / per_block_max;
+    if (cap == 0 || need > cap)
+      return fail(ctx, MPC_E_UNSUPPORTED, "LSM path count exceeds the co-resident capacity of the device");
+    // about four paths per thread, at most one full device
+    uint64_t want = (r.n_paths + 4 * kLsmThreads - 1) / (4 * kLsmThreads);
+    j.blocks = uint32_t(std::max<uint64_t>(need, std::min<uint64_t>(want, cap)));
+    LsmArgs& a = j.args;
+    std::memset(&a, 0, sizeof(a));
+    a.n_paths = r.n_paths;
+    a.n_steps = r.n_steps;
+    a.n_sched = uint32_t(j.sched.size());
+    a.degree = j.degree;
+    a.sampler = uint32_t(j.sampler);
+    a.seed = r.seed;
+    a.seed32 = uint32_t(r.seed);
+    a.fp64 = j.fp64;
+    a.s0 = r.s0;
+    a.k = r.k;
+    a.drift = (r.r - 0.5 * r.sigma * r.sigma) * dt;
+    a.vol = r.sigma * std::sqrt(dt);
+    a.disc_step = disc_step;
+    a.timeout_ns = 2000000000ull;
+  }
+  // launches: jobs of the same (fp64, sampler), packed under the capacity
+  std::vector<bool> done(jobs.size(), false);
+  double total_ms = 0.0;
+  uint64_t launches_before = kernel_launch_count(), h2d = 0, d2h = 0;
+  for (size_t first = 0; first < jobs.size(); ++first) {
+    if (done[first]) continue;
+    const int fp64 = jobs[first].fp64, sampler = jobs[first].sampler;
+    const uint32_t cap = lsm_capacity(fp64, sampler);
+    std::vector<size_t> group;
+    uint32_t blocks = 0;
+    for (size_t i = first; i < jobs.size(); ++i) {
+      if (done[i] || jobs[i].fp64 != fp64 || jobs[i].sampler != sampler) continue;
+      if (blocks + jobs[i].blocks > cap) continue;
+      group.push_back(i);
+      blocks += jobs[i].blocks;
+      done[i] = true;
+    }
+    // device arena layout per job: paths | sched | disc | partials | final | out | counters
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+    std::vector<size_t> offs;
+    size_t bytes = align(group.size() * sizeof(LsmArgs));
+    for (size_t i : group) {
+      const Job& j = jobs[i];
+      offs.push_back(bytes);
+      const size_t elem = j.fp64 ? 8 : 4;
+      bytes += align(j.args.n_paths * j.args.n_steps * elem) + align(j.sched.size() * 4) +
+               align(j.disc_pow.size() * 8) + align(2ull * j.blocks * 16 * 8) + align(j.blocks * 4ull * 8) +
+               align(8 * 8) + align(64);
+    }
+    void* arena = nullptr;
+    int st = scratch(ctx, "lsm_arena", bytes, &arena);
+    if (st != MPC_OK) return st;
+    size_t host_bytes = bytes - 0;
+    std::vector<uint8_t> host(align(group.size() * sizeof(LsmArgs)));
+    uint8_t* base = static_cast<uint8_t*>(arena);
+    uint32_t block_first = 0;
+    for (size_t g = 0; g < group.size(); ++g) {
+      Job& j = jobs[group[g]];
+      const size_t elem = j.fp64 ? 8 : 4;
+      size_t o = offs[g];
+      LsmArgs& a = j.args;
+      a.paths = base + o;
+      o += align(a.n_paths * a.n_steps * elem);
+      a.sched = reinterpret_cast<const uint32_t*>(base + o);
+      MPC_CUDA(ctx, cudaMemcpyAsync(base + o, j.sched.data(), j.sched.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+      h2d += j.sched.size() * 4;
+      o += align(j.sched.size() * 4);
+      a.disc_pow = reinterpret_cast<const double*>(base + o);
+      MPC_CUDA(ctx, cudaMemcpyAsync(base + o, j.disc_pow.data(), j.disc_pow.size() * 8, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+      h2d += j.disc_pow.size() * 8;
+      o += align(j.disc_pow.size() * 8);
+      a.partials = reinterpret_cast<double*>(base + o);
+      o += align(2ull * j.blocks * 16 * 8);
+      a.final_partials = reinterpret_cast<double*>(base + o);
+      o += align(j.blocks * 4ull * 8);
+      a.out = reinterpret_cast<double*>(base + o);
+      o += align(8 * 8);
+      a.barrier = reinterpret_cast<unsigned*>(base + o);
+      a.done = a.barrier + 4;
+      a.error = reinterpret_cast<int*>(a.barrier + 8);
+      MPC_CUDA(ctx, cudaMemsetAsync(a.barrier, 0, 64, ctx->stream));
+      a.block_first = block_first;
+      a.n_blocks = j.blocks;
+      block_first += j.blocks;
+      std::memcpy(host.data() + g * sizeof(LsmArgs), &a, sizeof(LsmArgs));
+    }
+    (void)host_bytes;
+    MPC_CUDA(ctx, cudaMemcpyAsync(base, host.data(), group.size() * sizeof(LsmArgs), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    h2d += group.size() * sizeof(LsmArgs);
+    MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+    cudaError_t e = launch_lsm_batch(reinterpret_cast<const LsmArgs*>(base), uint32_t(group.size()), block_first,
+                                     fp64, sampler, ctx->tabs, ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "LSM cooperative launch");
+    void* pin = nullptr;
+    if ((st = pinned_staging(ctx, group.size() * 80 + 64, &pin))) return st;
+    double* hout = static_cast<double*>(pin);
+    int* herr = reinterpret_cast<int*>(hout + group.size() * 8);
+    for (size_t g = 0; g < group.size(); ++g) {
+      const LsmArgs& a = jobs[group[g]].args;
+      MPC_CUDA(ctx, cudaMemcpyAsync(hout + g * 8, a.out, 8 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+      MPC_CUDA(ctx, cudaMemcpyAsync(herr + g, a.error, 4, cudaMemcpyDeviceToHost, ctx->stream));
+      d2h += 8 * 8 + 4;
+    }
+    MPC_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+    MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+    total_ms += ms;
+    for (size_t g = 0; g < group.size(); ++g) {
+      const Job& j = jobs[group[g]];
+      const mpc_request_t& r = *reqs[j.index];
+      mpc_result_t* out = outs[j.index];
+      const double* h = hout + g * 8;
+      if (herr[g] != 0) {
+        out->status = MPC_E_TIMEOUT;
+        return fail(ctx, MPC_E_TIMEOUT, "LSM block barrier timed out");
+      }
+      double price, se;
+      summarize(h[0], h[1], h[2], &price, &se);
+      uint32_t warnings = 0;
+      if (r.workload == MPC_WORKLOAD_AMERICAN_PUT) {  // intrinsic floor (cpu.rs:3919-3925)
+        double intrinsic = std::max(r.k - r.s0, 0.0);
+        if (intrinsic > price) {
+          price = intrinsic;
+          se = 0.0;
+          warnings |= MPC_WARN_INTRINSIC_FLOOR;
+        }
+      }
+      if (r.basis_degree != j.degree) warnings |= MPC_WARN_BASIS_DEGREE_CLAMPED;
+      if (j.normalised) warnings |= MPC_WARN_SCHEDULE_NORMALISED;
+      if (r.n_threads > 1) warnings |= MPC_WARN_THREADS_IGNORED;
+      out->price = price;
+      out->stderr = se;
+      out->n_samples = r.n_paths;
+      out->path_steps = r.n_paths * r.n_steps;
+      out->moments[0] = h[0];
+      out->moments[1] = h[1];
+      out->moments[2] = h[2];
+      out->early_exercise_count = uint64_t(h[3]);
+      out->maturity_exercise_count = uint64_t(h[4]);
+      out->regression_steps = uint32_t(h[5]);
+      out->basis_degree = j.degree;
+      out->warnings |= warnings;
+      out->runtime_ms = ms;
+      out->status = MPC_OK;
     }
   }
-  const bool fp64 = r.precision == MPC_PRECISION_FP64_PLAIN;
-  const double dt = r.t / double(r.n_steps);
-  std::vector<double> disc_pow(r.n_steps + 1);
-  const double disc_step = std::exp(-r.r * dt);
-  for (uint32_t j = 0; j <= r.n_steps; ++j) disc_pow[j] = powi(disc_step, int(j));
-  void *d_paths, *d_sched, *d_disc, *d_part, *d_fpart, *d_out, *d_bar;
-  int st;
-  const size_t elem = fp64 ? 8 : 4;
-  if ((st = scratch(ctx, "lsm_paths", r.n_paths * r.n_steps * elem, &d_paths))) return st;
-  if ((st = scratch(ctx, "lsm_sched", sched.size() * 4, &d_sched))) return st;
-  if ((st = scratch(ctx, "lsm_disc", disc_pow.size() * 8, &d_disc))) return st;
-  if ((st = scratch(ctx, "lsm_part", 2 * 16384 * 16 * 8, &d_part))) return st;
-  if ((st = scratch(ctx, "lsm_fpart", 16384 * 4 * 8, &d_fpart))) return st;
-  if ((st = scratch(ctx, "lsm_out", 8 * 8, &d_out))) return st;
-  if ((st = scratch(ctx, "lsm_bar", 64, &d_bar))) return st;
-  LsmArgs a{};
-  a.n_paths = r.n_paths;
-  a.n_steps = r.n_steps;
-  a.n_sched = uint32_t(sched.size());
-  a.degree = degree;
-  a.sampler = uint32_t(sampler_of(r.sampling));
-  a.seed = r.seed;
-  a.seed32 = uint32_t(r.seed);
-  a.fp64 = fp64 ? 1 : 0;
-  a.s0 = r.s0;
-  a.k = r.k;
-  a.drift = (r.r - 0.5 * r.sigma * r.sigma) * dt;
-  a.vol = r.sigma * std::sqrt(dt);
-  a.disc_step = disc_step;
-  a.sched = static_cast<uint32_t*>(d_sched);
-  a.disc_pow = static_cast<double*>(d_disc);
-  a.paths = d_paths;
-  a.partials = static_cast<double*>(d_part);
-  a.final_partials = static_cast<double*>(d_fpart);
-  a.out = static_cast<double*>(d_out);
-  a.barrier = static_cast<unsigned*>(d_bar);
-  a.done = static_cast<unsigned*>(d_bar) + 4;
-  a.error = reinterpret_cast<int*>(static_cast<unsigned*>(d_bar) + 8);
-  a.timeout_ns = 2000000000ull;
-  void* pin = nullptr;
-  if ((st = pinned_staging(ctx, 256, &pin))) return st;
-  double* hout = static_cast<double*>(pin);
-  int* herr = reinterpret_cast<int*>(hout + 8);
-  uint64_t launches_before = kernel_launch_count();
-  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-  MPC_CUDA(ctx, cudaMemcpyAsync(d_sched, sched.data(), sched.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-  MPC_CUDA(ctx, cudaMemcpyAsync(d_disc, disc_pow.data(), disc_pow.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-  MPC_CUDA(ctx, cudaMemsetAsync(d_bar, 0, 64, ctx->stream));
-  int grid = 0;
-  cudaError_t e = launch_lsm(a, ctx->tabs, &grid, ctx->stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "LSM cooperative launch");
-  MPC_CUDA(ctx, cudaMemcpyAsync(hout, d_out, 8 * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  MPC_CUDA(ctx, cudaMemcpyAsync(herr, a.error, 4, cudaMemcpyDeviceToHost, ctx->stream));
-  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
-  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  float ms = 0.0f;
-  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
-  ctx->last_ms = ms;
+  ctx->last_ms = total_ms;
   ctx->last_launches = kernel_launch_count() - launches_before;
-  ctx->last_h2d = sched.size() * 4 + disc_pow.size() * 8;
-  ctx->last_d2h = 8 * 8 + 4;
-  if (*herr != 0) return fail(ctx, MPC_E_TIMEOUT, "LSM grid barrier timed out");
-  double price, se;
-  summarize(hout[0], hout[1], hout[2], &price, &se);
-  uint32_t warnings = 0;
-  if (r.workload == MPC_WORKLOAD_AMERICAN_PUT) {  // intrinsic floor (cpu.rs:3919-3925)
-    double intrinsic = std::max(r.k - r.s0, 0.0);
-    if (intrinsic > price) {
-      price = intrinsic;
-      se = 0.0;
-      warnings |= MPC_WARN_INTRINSIC_FLOOR;
-    }
-  }
-  if (r.basis_degree != degree) warnings |= MPC_WARN_BASIS_DEGREE_CLAMPED;
-  if (normalised) warnings |= MPC_WARN_SCHEDULE_NORMALISED;
-  if (r.n_threads > 1) warnings |= MPC_WARN_THREADS_IGNORED;
-  out->price = price;
-  out->stderr = se;
-  out->n_samples = r.n_paths;
-  out->path_steps = r.n_paths * r.n_steps;
-  out->moments[0] = hout[0];
-  out->moments[1] = hout[1];
-  out->moments[2] = hout[2];
-  out->early_exercise_count = uint64_t(hout[3]);
-  out->maturity_exercise_count = uint64_t(hout[4]);
-  out->regression_steps = uint32_t(hout[5]);
-  out->basis_degree = degree;
-  out->warnings |= warnings;
-  out->runtime_ms = ms;
+  ctx->last_h2d = h2d;
+  ctx->last_d2h = d2h;
   return MPC_OK;
+}
+
+static int run_lsm(mpc_context* ctx, const mpc_request_t& r, mpc_result_t* out) {
+  return run_lsm_batch(ctx, {&r}, {out});
 }
 
 // ------------------------------------------------------------------ MLMC ---
@@ -911,152 +1014,207 @@ static void level_request(const mpc_request_t& r, uint64_t seed, uint32_t level,
   build_sampler_tables(p, level_seed, paths, fine);
 }
 
-// Runs all levels of one replicate; returns per-level (mean, variance) and cost.
-static int run_levels(mpc_context* ctx, const mpc_request_t& r, uint64_t seed, const std::vector<uint64_t>& paths,
-                      std::vector<double>* mean, std::vector<double>* var, double* device_ms) {
-  const uint32_t L = r.levels;
-  std::vector<Prepared> preps(L);
-  std::vector<mpc_result_t> res(L);
-  mean->assign(L, 0.0);
-  var->assign(L, 0.0);
-  for (uint32_t l = 0; l < L; ++l) level_request(r, seed, l, paths[l], &preps[l]);
-  if (r.precision == MPC_PRECISION_FP64_PLAIN) {
-    for (uint32_t l = 0; l < L; ++l) {
-      std::memset(&res[l], 0, sizeof(res[l]));
-      int st = run_plain(ctx, &preps[l], &res[l], nullptr, 0);
+// Prices a list of level requests (any mix of MLMC requests, replicates and
+// levels): FP32 entries in one fused batch, FP64-plain entries one launch
+// sequence each.  Returns per entry (mean, population variance).
+static int run_level_list(mpc_context* ctx, std::vector<Prepared>& preps, std::vector<double>* mean,
+                          std::vector<double>* var, double* device_ms) {
+  std::vector<mpc_result_t> res(preps.size());
+  std::vector<Prepared*> fused;
+  std::vector<mpc_result_t*> fused_out;
+  for (size_t i = 0; i < preps.size(); ++i) {
+    std::memset(&res[i], 0, sizeof(res[i]));
+    if (preps[i].plain) {
+      int st = run_plain(ctx, &preps[i], &res[i], nullptr, 0);
       if (st != MPC_OK) return st;
       *device_ms += ctx->last_ms;
+    } else {
+      fused.push_back(&preps[i]);
+      fused_out.push_back(&res[i]);
     }
-  } else {
-    std::vector<Prepared*> pp;
-    std::vector<mpc_result_t*> oo;
-    for (uint32_t l = 0; l < L; ++l) {
-      std::memset(&res[l], 0, sizeof(res[l]));
-      pp.push_back(&preps[l]);
-      oo.push_back(&res[l]);
-    }
-    int st = run_fused(ctx, pp, oo, nullptr, 0);
+  }
+  if (!fused.empty()) {
+    int st = run_fused(ctx, fused, fused_out, nullptr, 0);
     if (st != MPC_OK) return st;
     *device_ms += ctx->last_ms;
   }
-  for (uint32_t l = 0; l < L; ++l) {
-    double nn = res[l].moments[0];
-    double m = res[l].moments[1] / nn;
-    (*mean)[l] = m;
-    (*var)[l] = (res[l].moments[2] / nn) - m * m;
+  mean->assign(preps.size(), 0.0);
+  var->assign(preps.size(), 0.0);
+  for (size_t i = 0; i < preps.size(); ++i) {
+    double nn = res[i].moments[0];
+    double m = res[i].moments[1] / nn;
+    (*mean)[i] = m;
+    (*var)[i] = (res[i].moments[2] / nn) - m * m;
   }
   return MPC_OK;
 }
 
 // arithmetic_asian_call_price_mlmc_{single,replicated}_cpu (cpu.rs:3612-3751)
 // with solve_arithmetic_asian_mlmc_tolerance_cpu (cpu.rs:3352-3423) when
-// target_stderr > 0.  Level variances and the allocation are FP64 on the host.
-static int run_mlmc(mpc_context* ctx, const mpc_request_t& r_in, mpc_result_t* out) {
-  mpc_request_t r = r_in;
-  const uint32_t L = r.levels;
-  const bool pseudo = r.sampling == MPC_SAMPLING_PSEUDORANDOM || r.sampling == MPC_SAMPLING_COUNTER_HASH;
-  const uint64_t reps = pseudo ? 1 : std::max<uint32_t>(r.scramble_replicates, 1);
+// target_stderr > 0, for a batch of requests: every pilot level of every
+// request runs in one fused launch, then every level of every replicate.
+// Level variances and the allocation are FP64 on the host.
+int run_mlmc_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& reqs,
+                   const std::vector<mpc_result_t*>& outs) {
+  struct Job {
+    mpc_request_t r;
+    uint64_t reps;
+  };
+  std::vector<Job> jobs;
+  for (const mpc_request_t* rq : reqs) {
+    Job j;
+    j.r = *rq;
+    const bool pseudo = j.r.sampling == MPC_SAMPLING_PSEUDORANDOM || j.r.sampling == MPC_SAMPLING_COUNTER_HASH;
+    j.reps = pseudo ? 1 : std::max<uint32_t>(j.r.scramble_replicates, 1);
+    jobs.push_back(j);
+  }
   double device_ms = 0.0;
   uint64_t launches_before = kernel_launch_count();
-  auto cost = [&](uint32_t l) { return fine_steps(r, l) + (l == 0 ? 0 : fine_steps(r, l) / r.refinement_factor); };
-  if (r.target_stderr > 0.0) {
-    std::vector<uint64_t> pilot(L, r.pilot_paths_per_level);
+  auto cost = [](const mpc_request_t& r, uint32_t l) {
+    return fine_steps(r, l) + (l == 0 ? 0 : fine_steps(r, l) / r.refinement_factor);
+  };
+  // pilot phase for the tolerance solver
+  std::vector<Prepared> pilot;
+  std::vector<size_t> pilot_first(jobs.size(), 0);
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    pilot_first[i] = pilot.size();
+    if (jobs[i].r.target_stderr <= 0.0) continue;
+    for (uint32_t l = 0; l < jobs[i].r.levels; ++l) {
+      pilot.emplace_back();
+      level_request(jobs[i].r, jobs[i].r.seed, l, jobs[i].r.pilot_paths_per_level, &pilot.back());
+    }
+  }
+  if (!pilot.empty()) {
     std::vector<double> pm, pv;
-    int st = run_levels(ctx, r, r.seed, pilot, &pm, &pv, &device_ms);
+    int st = run_level_list(ctx, pilot, &pm, &pv, &device_ms);
     if (st != MPC_OK) return st;
-    for (uint32_t l = 0; l < L; ++l) pv[l] = std::max(pv[l], 1.0e-18);
-    auto allocate = [&](double target_variance, bool by_budget, uint64_t budget, std::vector<uint64_t>& paths) {
-      double denom = 0.0;
-      for (uint32_t l = 0; l < L; ++l) denom += std::sqrt(pv[l] * double(cost(l)));
-      uint64_t total = 0;
-      for (uint32_t l = 0; l < L; ++l) {
-        double w = std::sqrt(pv[l] / double(cost(l)));
-        double raw = by_budget ? std::ceil(double(budget) * w / denom) : std::ceil(denom * w / target_variance);
-        paths[l] = std::max<uint64_t>(uint64_t(raw), 2);
-        total += paths[l] * cost(l);
+    for (size_t i = 0; i < jobs.size(); ++i) {
+      mpc_request_t& r = jobs[i].r;
+      if (r.target_stderr <= 0.0) continue;
+      const uint32_t L = r.levels;
+      const uint64_t reps = jobs[i].reps;
+      std::vector<double> var(L);
+      for (uint32_t l = 0; l < L; ++l) var[l] = std::max(pv[pilot_first[i] + l], 1.0e-18);
+      auto allocate = [&](double target_variance, bool by_budget, uint64_t budget, std::vector<uint64_t>& paths) {
+        double denom = 0.0;
+        for (uint32_t l = 0; l < L; ++l) denom += std::sqrt(var[l] * double(cost(r, l)));
+        uint64_t total = 0;
+        for (uint32_t l = 0; l < L; ++l) {
+          double w = std::sqrt(var[l] / double(cost(r, l)));
+          double raw = by_budget ? std::ceil(double(budget) * w / denom) : std::ceil(denom * w / target_variance);
+          paths[l] = std::max<uint64_t>(uint64_t(raw), 2);
+          total += paths[l] * cost(r, l);
+        }
+        return total;
+      };
+      auto est_se = [&](const std::vector<uint64_t>& paths) {
+        double v = 0.0;
+        for (uint32_t l = 0; l < L; ++l) v += var[l] / double(paths[l]);
+        return std::sqrt(v / double(reps));
+      };
+      std::vector<uint64_t> paths(L);
+      uint64_t updates = allocate(r.target_stderr * r.target_stderr * double(reps), false, 0, paths) * reps;
+      double est = est_se(paths);
+      if (updates < r.min_step_updates) {
+        uint64_t per = std::max<uint64_t>((r.min_step_updates + reps - 1) / reps, 1);
+        updates = allocate(0, true, per, paths) * reps;
+        est = est_se(paths);
       }
-      return total;
-    };
-    auto est_se = [&](const std::vector<uint64_t>& paths) {
-      double v = 0.0;
-      for (uint32_t l = 0; l < L; ++l) v += pv[l] / double(paths[l]);
-      return std::sqrt(v / double(reps));
-    };
-    std::vector<uint64_t> paths(L);
-    uint64_t updates = allocate(r.target_stderr * r.target_stderr * double(reps), false, 0, paths) * reps;
-    double est = est_se(paths);
-    if (updates < r.min_step_updates) {
-      uint64_t per = std::max<uint64_t>((r.min_step_updates + reps - 1) / reps, 1);
-      updates = allocate(0, true, per, paths) * reps;
-      est = est_se(paths);
+      bool hit = false;
+      if (updates > r.max_step_updates) {
+        hit = true;
+        uint64_t per = std::max<uint64_t>(r.max_step_updates / reps, 1);
+        updates = allocate(0, true, per, paths) * reps;
+        est = est_se(paths);
+      }
+      for (uint32_t l = 0; l < L; ++l) r.paths_per_level[l] = paths[l];
+      outs[i]->estimated_stderr = est;
+      outs[i]->target_met = (est <= r.target_stderr && updates <= r.max_step_updates) ? 1 : 0;
+      outs[i]->max_step_updates_hit = hit ? 1 : 0;
     }
-    bool hit = false;
-    if (updates > r.max_step_updates) {
-      hit = true;
-      uint64_t per = std::max<uint64_t>(r.max_step_updates / reps, 1);
-      updates = allocate(0, true, per, paths) * reps;
-      est = est_se(paths);
+  }
+  // main phase: every level of every replicate of every request
+  std::vector<Prepared> mains;
+  std::vector<size_t> main_first(jobs.size(), 0);
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    const mpc_request_t& r = jobs[i].r;
+    main_first[i] = mains.size();
+    for (uint64_t rep = 0; rep < jobs[i].reps; ++rep) {
+      uint64_t seed = jobs[i].reps > 1 ? derive_chunk_seed(r.seed, rep) : r.seed;
+      for (uint32_t l = 0; l < r.levels; ++l) {
+        mains.emplace_back();
+        level_request(r, seed, l, r.paths_per_level[l], &mains.back());
+      }
     }
-    for (uint32_t l = 0; l < L; ++l) r.paths_per_level[l] = paths[l];
-    out->estimated_stderr = est;
-    out->target_met = (est <= r.target_stderr && updates <= r.max_step_updates) ? 1 : 0;
-    out->max_step_updates_hit = hit ? 1 : 0;
   }
-  std::vector<uint64_t> paths(r.paths_per_level, r.paths_per_level + L);
-  std::vector<double> rep_price(reps);
-  std::vector<std::vector<double>> lmean(reps), lvar(reps);
-  double single_se = 0.0;
-  uint64_t total_paths = 0, total_updates = 0;
-  for (uint64_t rep = 0; rep < reps; ++rep) {
-    uint64_t seed = reps > 1 ? derive_chunk_seed(r.seed, rep) : r.seed;
-    int st = run_levels(ctx, r, seed, paths, &lmean[rep], &lvar[rep], &device_ms);
-    if (st != MPC_OK) return st;
-    double price = 0.0, varc = 0.0;
-    for (uint32_t l = 0; l < L; ++l) {
-      lvar[rep][l] = std::max(lvar[rep][l], 0.0);
-      price += lmean[rep][l];
-      varc += lvar[rep][l] / double(paths[l]);
-      total_paths += paths[l];
-      total_updates += paths[l] * cost(l);
+  std::vector<double> mm, mv;
+  int st = run_level_list(ctx, mains, &mm, &mv, &device_ms);
+  if (st != MPC_OK) return st;
+  for (size_t i = 0; i < jobs.size(); ++i) {
+    const mpc_request_t& r = jobs[i].r;
+    mpc_result_t* out = outs[i];
+    const uint32_t L = r.levels;
+    const uint64_t reps = jobs[i].reps;
+    std::vector<double> rep_price(reps);
+    double single_se = 0.0;
+    uint64_t total_paths = 0, total_updates = 0;
+    for (uint64_t rep = 0; rep < reps; ++rep) {
+      double price = 0.0, varc = 0.0;
+      for (uint32_t l = 0; l < L; ++l) {
+        const size_t e = main_first[i] + rep * L + l;
+        mv[e] = std::max(mv[e], 0.0);
+        price += mm[e];
+        varc += mv[e] / double(r.paths_per_level[l]);
+        total_paths += r.paths_per_level[l];
+        total_updates += r.paths_per_level[l] * cost(r, l);
+      }
+      rep_price[rep] = price;
+      single_se = std::sqrt(varc);
     }
-    rep_price[rep] = price;
-    single_se = std::sqrt(varc);
-  }
-  double price = 0.0;
-  for (double p : rep_price) price += p;
-  price /= double(reps);
-  double se = single_se;
-  if (reps > 1) {
-    double sv = 0.0;
-    for (double p : rep_price) sv += (p - price) * (p - price);
-    sv /= double(reps - 1);
-    se = std::sqrt(sv / double(reps));
-  }
-  out->price = price;
-  out->stderr = se;
-  out->n_levels = L;
-  out->total_paths = total_paths;
-  out->total_step_updates = total_updates;
-  out->path_steps = total_updates;
-  for (uint32_t l = 0; l < L; ++l) {
-    double mean = 0.0;
-    for (uint64_t rep = 0; rep < reps; ++rep) mean += lmean[rep][l];
-    mean /= double(reps);
-    double var = lvar[0][l];
+    double price = 0.0;
+    for (double p : rep_price) price += p;
+    price /= double(reps);
+    double se = single_se;
     if (reps > 1) {
-      var = 0.0;
-      for (uint64_t rep = 0; rep < reps; ++rep) var += (lmean[rep][l] - mean) * (lmean[rep][l] - mean);
-      var /= double(reps - 1);
+      double sv = 0.0;
+      for (double p : rep_price) sv += (p - price) * (p - price);
+      sv /= double(reps - 1);
+      se = std::sqrt(sv / double(reps));
     }
-    out->level_mean[l] = mean;
-    out->level_variance[l] = var;
-    out->level_paths[l] = paths[l] * reps;
-    out->level_fine_steps[l] = fine_steps(r, l);
+    out->price = price;
+    out->stderr = se;
+    out->n_levels = L;
+    out->total_paths = total_paths;
+    out->total_step_updates = total_updates;
+    out->path_steps = total_updates;
+    for (uint32_t l = 0; l < L; ++l) {
+      double mean = 0.0;
+      for (uint64_t rep = 0; rep < reps; ++rep) mean += mm[main_first[i] + rep * L + l];
+      mean /= double(reps);
+      double var = mv[main_first[i] + l];
+      if (reps > 1) {
+        var = 0.0;
+        for (uint64_t rep = 0; rep < reps; ++rep) {
+          double d = mm[main_first[i] + rep * L + l] - mean;
+          var += d * d;
+        }
+        var /= double(reps - 1);
+      }
+      out->level_mean[l] = mean;
+      out->level_variance[l] = var;
+      out->level_paths[l] = r.paths_per_level[l] * reps;
+      out->level_fine_steps[l] = fine_steps(r, l);
+    }
+    out->runtime_ms = device_ms;
+    out->status = MPC_OK;
   }
-  out->runtime_ms = device_ms;
   ctx->last_ms = device_ms;
   ctx->last_launches = kernel_launch_count() - launches_before;
   return MPC_OK;
+}
+
+static int run_mlmc(mpc_context* ctx, const mpc_request_t& r, mpc_result_t* out) {
+  return run_mlmc_batch(ctx, {&r}, {out});
 }
 
 static int price_one(mpc_context* ctx, const mpc_request_t* req, mpc_result_t* out, double* per_unit,
@@ -1071,7 +1229,7 @@ static int price_one(mpc_context* ctx, const mpc_request_t* req, mpc_result_t* o
   if (req->workload == MPC_WORKLOAD_ASIAN_MLMC) {
     st = run_mlmc(ctx, *req, out);
   } else if (is_lsm(req->workload)) {
-    st = run_lsm(ctx, *req, out, per_unit);
+    st = run_lsm(ctx, *req, out);
   } else {
     Prepared p;
     st = prepare(ctx, *req, &p, &msg);
@@ -1441,6 +1599,8 @@ int mpc_price_batch(mpc_context_t* ctx, const mpc_request_t* reqs, size_t n, mpc
   std::vector<Prepared> preps(n);
   std::vector<Prepared*> fused;
   std::vector<mpc_result_t*> fused_out;
+  std::vector<const mpc_request_t*> lsm, mlmc;
+  std::vector<mpc_result_t*> lsm_out, mlmc_out;
   int first_error = MPC_OK;
   double total_ms = 0.0;
   uint64_t launches_before = kernel_launch_count();
@@ -1464,10 +1624,36 @@ int mpc_price_batch(mpc_context_t* ctx, const mpc_request_t* reqs, size_t n, mpc
       }
       continue;
     }
-    // FP64-plain, LSM and MLMC requests run one launch sequence each
+    if (is_lsm(reqs[i].workload)) {
+      lsm.push_back(&reqs[i]);
+      lsm_out.push_back(&out[i]);
+      continue;
+    }
+    if (reqs[i].workload == MPC_WORKLOAD_ASIAN_MLMC) {
+      mlmc.push_back(&reqs[i]);
+      mlmc_out.push_back(&out[i]);
+      continue;
+    }
+    // FP64-plain requests run one launch sequence each
     st = price_one(ctx, &reqs[i], &out[i], nullptr, 0);
     total_ms += ctx->last_ms;
     if (st != MPC_OK && first_error == MPC_OK) first_error = st;
+  }
+  if (!lsm.empty()) {  // packed into shared cooperative launches
+    int st = run_lsm_batch(ctx, lsm, lsm_out);
+    total_ms += ctx->last_ms;
+    if (st != MPC_OK) {
+      for (mpc_result_t* o : lsm_out) o->status = st;
+      if (first_error == MPC_OK) first_error = st;
+    }
+  }
+  if (!mlmc.empty()) {  // all pilot levels in one launch, all main levels in another
+    int st = run_mlmc_batch(ctx, mlmc, mlmc_out);
+    total_ms += ctx->last_ms;
+    if (st != MPC_OK) {
+      for (mpc_result_t* o : mlmc_out) o->status = st;
+      if (first_error == MPC_OK) first_error = st;
+    }
   }
   if (!fused.empty()) {
     int st = run_fused(ctx, fused, fused_out, nullptr, 0);

@@ -87,6 +87,11 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
 uint64_t estimate_bytes(const mpc_request_t& r);
 Shape choose_shape(mpc_context* ctx, const Prepared& p);
 void summarize_moments(const Prepared& p, const double* m, mpc_result_t* out);
+// Longstaff-Schwartz and MLMC requests of a batch, packed into shared launches.
+int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& reqs,
+                  const std::vector<mpc_result_t*>& outs);
+int run_mlmc_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& reqs,
+                   const std::vector<mpc_result_t*>& outs);
 // Host copies of the device lookup tables: Sobol nibble tables [256][8][16]
 // and xorshift64* jump-ahead nibble tables [64][16][16].
 void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump);

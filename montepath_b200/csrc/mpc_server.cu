@@ -9,7 +9,9 @@
 // arrive meanwhile join the next wave.  A request's tile partials stay
 // resident in its slot across waves and the block that completes its last
 // tile writes its moments, so a result is the same alone and in any mix.
-// LSM and MLMC requests run as their own launches between waves.
+// LSM and MLMC requests admitted between waves run batched: every LSM
+// request in shared cooperative launches, every MLMC request in one pilot
+// and one main launch.
 //
 // Plain mode (mode 1): one request per launch sequence, FP64, strictly FIFO
 // -- the baseline continuous batching is compared against.
@@ -48,6 +50,7 @@ struct Ticket {
   uint64_t bytes = 0;
   uint32_t next_tile = 0;
   uint32_t tiles_finished = 0;
+  bool uploaded = false;
   double t_enqueue = 0, t_admit = 0, t_complete = 0;
 };
 
@@ -61,6 +64,7 @@ struct mpc_server {
   std::deque<uint64_t> queue;
   std::map<uint64_t, Ticket> tickets;
   std::vector<int64_t> slot_owner;  // ticket id per slot or -1
+  std::vector<uint8_t> dirty;       // slot descriptor changed since the last upload
   uint64_t next_id = 1;
   bool stop = false;
   std::thread worker;
@@ -162,33 +166,62 @@ void admit(mpc_server* s) {
   }
 }
 
+// LSM and MLMC requests admitted so far run together: all LSM requests in
+// shared cooperative launches, all MLMC requests as one pilot launch and one
+// main launch.  Returns the number of requests completed.
+int run_batched_families(mpc_server* s, std::unique_lock<std::mutex>& lk) {
+  std::vector<uint64_t> lsm_ids, mlmc_ids;
+  for (size_t i = 0; i < s->slot_owner.size(); ++i) {
+    if (s->slot_owner[i] < 0) continue;
+    const Ticket& t = s->tickets[uint64_t(s->slot_owner[i])];
+    if (fused_eligible(t)) continue;
+    if (t.req.workload == MPC_WORKLOAD_ASIAN_MLMC)
+      mlmc_ids.push_back(t.id);
+    else if (t.req.workload == MPC_WORKLOAD_AMERICAN_PUT || t.req.workload == MPC_WORKLOAD_BERMUDAN_PUT)
+      lsm_ids.push_back(t.id);
+    else
+      mlmc_ids.push_back(t.id);  // structured-table samplers: priced whole through mpc_price_batch
+  }
+  if (lsm_ids.empty() && mlmc_ids.empty()) return 0;
+  std::vector<mpc_request_t> lsm_req, other_req;
+  for (uint64_t id : lsm_ids) lsm_req.push_back(s->tickets[id].req);
+  for (uint64_t id : mlmc_ids) other_req.push_back(s->tickets[id].req);
+  lk.unlock();
+  std::vector<mpc_result_t> lsm_res(lsm_req.size()), other_res(other_req.size());
+  int st_lsm = MPC_OK, st_other = MPC_OK;
+  {
+    std::lock_guard<std::recursive_mutex> g(s->ctx->mu);
+    cudaSetDevice(s->ctx->device);
+    if (!lsm_req.empty()) {
+      st_lsm = mpc_price_batch(s->ctx, lsm_req.data(), lsm_req.size(), lsm_res.data());
+      s->busy_ms += s->ctx->last_ms;
+    }
+    if (!other_req.empty()) {
+      st_other = mpc_price_batch(s->ctx, other_req.data(), other_req.size(), other_res.data());
+      s->busy_ms += s->ctx->last_ms;
+    }
+  }
+  lk.lock();
+  for (size_t i = 0; i < lsm_ids.size(); ++i) {
+    Ticket& t = s->tickets[lsm_ids[i]];
+    t.res = lsm_res[i];
+    complete(s, t, lsm_res[i].status != MPC_OK ? lsm_res[i].status : st_lsm);
+  }
+  for (size_t i = 0; i < mlmc_ids.size(); ++i) {
+    Ticket& t = s->tickets[mlmc_ids[i]];
+    t.res = other_res[i];
+    complete(s, t, other_res[i].status != MPC_OK ? other_res[i].status : st_other);
+  }
+  s->stats.waves++;
+  return int(lsm_ids.size() + mlmc_ids.size());
+}
+
 // Runs one wave: up to wave_tiles tiles from live fused requests, oldest first.
 int run_wave(mpc_server* s, std::unique_lock<std::mutex>& lk) {
   std::vector<uint64_t> live;
   for (size_t i = 0; i < s->slot_owner.size(); ++i)
     if (s->slot_owner[i] >= 0) live.push_back(uint64_t(s->slot_owner[i]));
   std::sort(live.begin(), live.end());
-  // non-fused requests: run whole, one at a time
-  for (uint64_t id : live) {
-    Ticket& t = s->tickets[id];
-    if (fused_eligible(t)) continue;
-    mpc_request_t req = t.req;
-    lk.unlock();
-    mpc_result_t res;
-    int st;
-    {
-      std::lock_guard<std::recursive_mutex> g(s->ctx->mu);
-      cudaSetDevice(s->ctx->device);
-      st = mpc_price(s->ctx, &req, &res);
-      s->busy_ms += s->ctx->last_ms;
-    }
-    lk.lock();
-    Ticket& t2 = s->tickets[id];
-    t2.res = res;
-    complete(s, t2, st);
-    s->stats.waves++;
-    return 1;
-  }
   // fused wave
   std::vector<Tile> tiles;
   std::vector<uint64_t> finishing;
@@ -235,7 +268,11 @@ int run_wave(mpc_server* s, std::unique_lock<std::mutex>& lk) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s->stream);
-    cudaMemcpyAsync(s->d_slots, s->h_slots, s->slot_owner.size() * sizeof(DevReq), cudaMemcpyHostToDevice, s->stream);
+    for (size_t i = 0; i < s->dirty.size(); ++i)
+      if (s->dirty[i]) {
+        cudaMemcpyAsync(s->d_slots + i, s->h_slots + i, sizeof(DevReq), cudaMemcpyHostToDevice, s->stream);
+        s->dirty[i] = 0;
+      }
     cudaMemcpyAsync(s->d_tiles, s->h_tiles, off * sizeof(Tile), cudaMemcpyHostToDevice, s->stream);
     cudaMemsetAsync(s->d_counter, 0, 64 * sizeof(uint32_t), s->stream);
     size_t first = 0, g_idx = 0;
@@ -312,7 +349,9 @@ void serve(mpc_server* s) {
     for (size_t i = 0; i < s->slot_owner.size(); ++i) {
       if (s->slot_owner[i] < 0) continue;
       Ticket& t = s->tickets[uint64_t(s->slot_owner[i])];
-      if (!fused_eligible(t) || t.next_tile != 0) continue;
+      if (!fused_eligible(t) || t.next_tile != 0 || t.uploaded) continue;
+      t.uploaded = true;
+      s->dirty[i] = 1;
       DevReq q = t.prep.q;
       q.partials = s->d_partials + i * size_t(s->max_tiles_per_slot) * MPC_MOMENTS;
       q.moments = s->d_moments + i * MPC_MOMENTS;
@@ -320,7 +359,9 @@ void serve(mpc_server* s) {
       q.per_unit = nullptr;
       s->h_slots[i] = q;
     }
-    int ran = run_wave(s, lk);
+    int ran = run_batched_families(s, lk);
+    if (ran) s->cv_done.notify_all();
+    ran += run_wave(s, lk);
     s->cv_done.notify_all();
     if (!ran) s->cv_work.wait_for(lk, std::chrono::milliseconds(20));
   }
@@ -339,6 +380,7 @@ int mpc_server_start(mpc_context_t* ctx, const mpc_server_options_t* options, mp
   if (s->opt.max_slots == 0) s->opt.max_slots = 256;
   s->opt.max_slots = std::min<uint32_t>(s->opt.max_slots, 1024);
   s->slot_owner.assign(s->opt.max_slots, -1);
+  s->dirty.assign(s->opt.max_slots, 0);
   s->t0 = Clock::now();
   cudaSetDevice(ctx->device);
   const size_t slots = s->opt.max_slots;
