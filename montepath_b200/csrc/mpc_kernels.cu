@@ -1030,7 +1030,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* error, uint64_t
       while (*gen == g) {
         if (*((volatile int*)error) != 0) break;
         if (global_ns() - start > timeout_ns) {
-          atomicExch(error, 1);
+          atomicCAS(error, 0, kLsmErrTimeout);
           break;
         }
         __nanosleep(64);
@@ -1094,6 +1094,16 @@ constexpr int kLsmBlock = (int)kLsmThreads;
 constexpr int kLsmMaxP = (int)kLsmPathsPerThreadMax;
 constexpr int kLsmMom = 15;  // 10 unique A^T A, 4 A^T b, ITM count
 
+// Records the first failed self-check of an LSM job (code and index).
+__device__ __noinline__ void lsm_report(const LsmArgs& a, int code, uint64_t index) {
+  if (atomicCAS(a.error, 0, code) == 0) *a.diag = (unsigned long long)index;
+}
+__device__ __forceinline__ bool lsm_ok(const LsmArgs& a, uint64_t index, uint64_t len, int code) {
+  if (index < len) return true;
+  lsm_report(a, code, index);
+  return false;
+}
+
 template <class Real, int SMP>
 __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restrict__ jobs, uint32_t n_jobs, SrcCtx ctx) {
   __shared__ double red[kWarps][5];
@@ -1113,7 +1123,17 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
   const uint32_t lb = blockIdx.x - a.block_first;  // block index within the job
   const uint64_t n = a.n_paths;
   const uint32_t steps = a.n_steps;
-  for (uint32_t j = threadIdx.x; j <= steps && j < 512; j += blockDim.x) s_disc[j] = (Real)a.disc_pow[j];
+  // launch-shape invariants: this block belongs to the job, the job's blocks
+  // cover every path with <= kLsmMaxP paths per thread, the dates fit s_disc
+  if (blockIdx.x < a.block_first || lb >= nb) {
+    if (threadIdx.x == 0) lsm_report(a, kLsmErrJob, blockIdx.x);
+    return;
+  }
+  if ((uint64_t)nb * blockDim.x * kLsmMaxP < n || steps >= 512 || a.n_sched == 0 || a.n_sched > steps) {
+    if (threadIdx.x == 0) lsm_report(a, kLsmErrCoverage, n);
+    return;
+  }
+  for (uint32_t j = threadIdx.x; j <= steps; j += blockDim.x) s_disc[j] = (Real)a.disc_pow[j];
   __syncthreads();
   const uint64_t nthreads = (uint64_t)nb * blockDim.x;
   const uint64_t gtid = (uint64_t)lb * blockDim.x + threadIdx.x;
@@ -1139,13 +1159,17 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
     for (uint32_t st = 1; st <= steps; ++st) {
       const Real z = normal<Real>(src, st - 1);
       s *= ex<Real>(drift + vol * z);  // multiplicative update as cpu.rs:3829-3830
-      paths[(uint64_t)(st - 1) * n + path] = s;
+      const uint64_t idx = (uint64_t)(st - 1) * n + path;
+      if (lsm_ok(a, idx, a.paths_len, kLsmErrPaths)) paths[idx] = s;
     }
     cash[j] = k - s > (Real)0 ? k - s : (Real)0;
   }
   uint32_t regressions = 0;
   for (int si = (int)a.n_sched - 2; si >= 0; --si) {
     const uint32_t step = a.sched[si];
+    if (step == 0 || step > steps) {
+      if (threadIdx.x == 0) lsm_report(a, kLsmErrSched, step);
+    }
     const int buf = si & 1;
     double m[kLsmMom];
 #pragma unroll
@@ -1155,11 +1179,17 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
     for (int j = 0; j < kLsmMaxP; ++j) {
       const uint64_t path = gtid + (uint64_t)j * nthreads;
       sv[j] = (Real)0;
-      if (path >= n) continue;
-      const Real s = paths[(uint64_t)(step - 1) * n + path];
+      if (path >= n || step == 0 || step > steps) continue;
+      const uint64_t at = (uint64_t)(step - 1) * n + path;
+      if (!lsm_ok(a, at, a.paths_len, kLsmErrPaths)) continue;
+      const Real s = paths[at];
       sv[j] = s;
       const Real imm = k - s;
       if (!(imm > (Real)0)) continue;
+      if (exd[j] < step || exd[j] > steps) {
+        lsm_report(a, kLsmErrDisc, exd[j]);
+        continue;
+      }
       const Real cont = cash[j] * s_disc[exd[j] - step];
       Real b[4];
       laguerre4<Real>(s * inv_k, b);
@@ -1173,11 +1203,12 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
       m[14] += 1.0;
     }
     // block reduction of the 15 moments in three rounds of five
-    double* part = a.partials + ((size_t)buf * nb + lb) * 16;
+    const uint64_t part_at = ((uint64_t)buf * nb + lb) * 16;
+    double* part = a.partials + part_at;
     for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
       double v[5] = {m[r0], m[r0 + 1], m[r0 + 2], m[r0 + 3], m[r0 + 4]};
       block_reduce5(v, red);
-      if (threadIdx.x == 0)
+      if (threadIdx.x == 0 && lsm_ok(a, part_at + r0 + 4, a.partials_len, kLsmErrPartials))
         for (int i = 0; i < 5; ++i) part[r0 + i] = v[i];
       __syncthreads();
     }
@@ -1187,10 +1218,13 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
       double acc[kLsmMom];
 #pragma unroll
       for (int i = 0; i < kLsmMom; ++i) acc[i] = 0.0;
-      const double* base = a.partials + (size_t)buf * nb * 16;
-      for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x)
+      const uint64_t base_at = (uint64_t)buf * nb * 16;
+      const double* base = a.partials + base_at;
+      for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
+        if (!lsm_ok(a, base_at + (uint64_t)blk * 16 + kLsmMom - 1, a.partials_len, kLsmErrPartials)) break;
 #pragma unroll
         for (int i = 0; i < kLsmMom; ++i) acc[i] += __ldcg(base + (size_t)blk * 16 + i);
+      }
       for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
         double v[5] = {acc[r0], acc[r0 + 1], acc[r0 + 2], acc[r0 + 3], acc[r0 + 4]};
         block_reduce5(v, red);
@@ -1247,6 +1281,10 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
   for (int j = 0; j < kLsmMaxP; ++j) {
     const uint64_t path = gtid + (uint64_t)j * nthreads;
     if (path >= n) continue;
+    if (exd[j] > steps) {
+      lsm_report(a, kLsmErrDisc, exd[j]);
+      continue;
+    }
     const double d = (double)cash[j] * a.disc_pow[exd[j]];
     v[0] += d;
     v[1] += d * d;
@@ -1258,7 +1296,8 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
   block_reduce5(v, red);
   if (threadIdx.x == 0) {
     double* fp = a.final_partials + (size_t)lb * 4;
-    for (int i = 0; i < 4; ++i) fp[i] = v[i];
+    if (lsm_ok(a, (uint64_t)lb * 4 + 3, a.final_len, kLsmErrFinal))
+      for (int i = 0; i < 4; ++i) fp[i] = v[i];
     __threadfence();
     s_ok = atomicAdd(a.done, 1u) == nb - 1;
   }
@@ -1266,8 +1305,10 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
   if (s_ok) {
     __threadfence();
     double acc[5] = {0, 0, 0, 0, 0};
-    for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x)
+    for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
+      if (!lsm_ok(a, (uint64_t)blk * 4 + 3, a.final_len, kLsmErrFinal)) break;
       for (int i = 0; i < 4; ++i) acc[i] += __ldcg(a.final_partials + (size_t)blk * 4 + i);
+    }
     block_reduce5(acc, red);
     if (threadIdx.x != 0) return;
     a.out[0] = (double)n;

@@ -49,10 +49,28 @@ struct LsmArgs {
   double* out;               // [8]: n, sum, sumsq, early, maturity, regressions
   unsigned* barrier;         // [2]: count, generation
   unsigned* done;            // last-block counter
-  int* error;                // barrier timeout flag
+  int* error;                // first failure: kLsmErr* code (0 = none)
+  unsigned long long* diag;  // offending index of a failed self-check
   uint64_t timeout_ns;
   uint32_t block_first;      // this job's blocks in the batched launch
   uint32_t n_blocks;
+  uint64_t paths_len;        // elements allocated for `paths`
+  uint32_t partials_len;     // elements allocated for `partials`
+  uint32_t final_len;        // elements allocated for `final_partials`
+};
+// Failure codes written to LsmArgs::error.  Every indexed global or shared
+// access of the kernel is checked against its allocation; a failed check
+// records its code and index, skips the access and makes every block of the
+// job leave at the next barrier.
+enum : int {
+  kLsmErrTimeout = 1,
+  kLsmErrPaths = 2,
+  kLsmErrPartials = 3,
+  kLsmErrFinal = 4,
+  kLsmErrSched = 5,
+  kLsmErrDisc = 6,
+  kLsmErrJob = 7,
+  kLsmErrCoverage = 8,
 };
 // Several LSM requests in one cooperative launch: job j owns blocks
 // [block_first, block_first + n_blocks) and synchronises only them.  All jobs

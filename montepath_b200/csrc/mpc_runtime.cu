@@ -70,7 +70,15 @@ int scratch(mpc_context* ctx, const std::string& name, size_t bytes, void** out)
   void* p = nullptr;
   cudaError_t err = cudaMalloc(&p, grow);
   if (err != cudaSuccess) return cuda_fail(ctx, err, ("cudaMalloc " + name).c_str());
-  cudaMemset(p, 0, grow);
+  // Zero-fill on the context stream and wait for it: the context stream is
+  // non-blocking, so a fill on the legacy stream would not be ordered before
+  // the caller's copies into the new buffer and could overwrite them.
+  err = cudaMemsetAsync(p, 0, grow, ctx->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(ctx->stream);
+  if (err != cudaSuccess) {
+    cudaFree(p);
+    return cuda_fail(ctx, err, ("zero-fill " + name).c_str());
+  }
   b.ptr = p;
   b.bytes = grow;
   ctx->live_bytes += grow;
@@ -806,9 +814,10 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     const uint64_t need = (r.n_paths + per_block_max - 1) / per_block_max;
     if (cap == 0 || need > cap)
       return fail(ctx, MPC_E_UNSUPPORTED, "LSM path count exceeds the co-resident capacity of the device");
-    // about four paths per thread, at most one full device
+    // about four paths per thread, at most two blocks per SM for one job
     uint64_t want = (r.n_paths + 4 * kLsmThreads - 1) / (4 * kLsmThreads);
-    j.blocks = uint32_t(std::max<uint64_t>(need, std::min<uint64_t>(want, cap)));
+    want = std::min<uint64_t>(want, std::min<uint64_t>(cap, 2ull * uint64_t(ctx->sm_count)));
+    j.blocks = uint32_t(std::max<uint64_t>(need, want));
     LsmArgs& a = j.args;
     std::memset(&a, 0, sizeof(a));
     a.n_paths = r.n_paths;
@@ -884,10 +893,16 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       o += align(j.blocks * 4ull * 8);
       a.out = reinterpret_cast<double*>(base + o);
       o += align(8 * 8);
+      // counters (64 bytes, zeroed per launch): barrier count and generation
+      // at 0, block-done counter at 16, error code at 32, failed index at 40
       a.barrier = reinterpret_cast<unsigned*>(base + o);
       a.done = a.barrier + 4;
       a.error = reinterpret_cast<int*>(a.barrier + 8);
+      a.diag = reinterpret_cast<unsigned long long*>(a.barrier + 10);
       MPC_CUDA(ctx, cudaMemsetAsync(a.barrier, 0, 64, ctx->stream));
+      a.paths_len = a.n_paths * a.n_steps;
+      a.partials_len = 2u * j.blocks * 16u;
+      a.final_len = j.blocks * 4u;
       a.block_first = block_first;
       a.n_blocks = j.blocks;
       block_first += j.blocks;
@@ -901,15 +916,17 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     cudaError_t e = launch_lsm_batch(reinterpret_cast<const LsmArgs*>(base), uint32_t(group.size()), block_first,
                                      fp64, sampler, ctx->tabs, ctx->stream);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "LSM cooperative launch");
+    // pinned results: per job 8 doubles of output, then per job 16 bytes of
+    // {error code, pad, failed index} copied from the counters at byte 32
     void* pin = nullptr;
-    if ((st = pinned_staging(ctx, group.size() * 80 + 64, &pin))) return st;
+    if ((st = pinned_staging(ctx, group.size() * 80, &pin))) return st;
     double* hout = static_cast<double*>(pin);
-    int* herr = reinterpret_cast<int*>(hout + group.size() * 8);
+    uint8_t* hdiag = reinterpret_cast<uint8_t*>(hout + group.size() * 8);
     for (size_t g = 0; g < group.size(); ++g) {
       const LsmArgs& a = jobs[group[g]].args;
       MPC_CUDA(ctx, cudaMemcpyAsync(hout + g * 8, a.out, 8 * 8, cudaMemcpyDeviceToHost, ctx->stream));
-      MPC_CUDA(ctx, cudaMemcpyAsync(herr + g, a.error, 4, cudaMemcpyDeviceToHost, ctx->stream));
-      d2h += 8 * 8 + 4;
+      MPC_CUDA(ctx, cudaMemcpyAsync(hdiag + g * 16, a.error, 16, cudaMemcpyDeviceToHost, ctx->stream));
+      d2h += 8 * 8 + 16;
     }
     MPC_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
     MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -921,9 +938,21 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       const mpc_request_t& r = *reqs[j.index];
       mpc_result_t* out = outs[j.index];
       const double* h = hout + g * 8;
-      if (herr[g] != 0) {
+      int code = 0;
+      unsigned long long bad = 0;
+      std::memcpy(&code, hdiag + g * 16, sizeof(code));
+      std::memcpy(&bad, hdiag + g * 16 + 8, sizeof(bad));
+      if (code == kLsmErrTimeout) {
         out->status = MPC_E_TIMEOUT;
         return fail(ctx, MPC_E_TIMEOUT, "LSM block barrier timed out");
+      }
+      if (code != 0) {
+        static const char* what[] = {"", "", "path matrix", "regression partials", "estimator partials",
+                                     "exercise date", "exercise discount", "job block range", "path coverage"};
+        out->status = MPC_E_CUDA;
+        return fail(ctx, MPC_E_CUDA,
+                    std::string("LSM kernel self-check failed: ") + (code < 9 ? what[code] : "unknown") +
+                        " index " + std::to_string(bad));
       }
       double price, se;
       summarize(h[0], h[1], h[2], &price, &se);

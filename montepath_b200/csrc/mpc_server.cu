@@ -396,7 +396,9 @@ int mpc_server_start(mpc_context_t* ctx, const mpc_server_options_t* options, mp
   if (e == cudaSuccess) e = cudaHostAlloc(&s->h_slots, slots * sizeof(DevReq), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc(&s->h_tiles, size_t(s->wave_tiles) * sizeof(Tile), cudaHostAllocDefault);
   if (e == cudaSuccess) e = cudaHostAlloc(&s->h_moments, slots * MPC_MOMENTS * sizeof(double), cudaHostAllocDefault);
-  if (e == cudaSuccess) e = cudaMemset(s->d_done, 0, slots * sizeof(uint32_t));
+  // zeroed on the server stream (non-blocking, so not ordered after the legacy stream)
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->d_done, 0, slots * sizeof(uint32_t), s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   if (e != cudaSuccess) {
     ctx->last_error = std::string("server allocation: ") + cudaGetErrorString(e);
     mpc_server_stop(s);

@@ -213,6 +213,37 @@ def test_bermudan_fp64(backend):
     assert a.warnings & abi.WARN_SCHEDULE_NORMALISED
 
 
+@pytest.mark.parametrize("precision", ["fp32_path", "fp64_plain"])
+def test_lsm_full_size(backend, precision):
+    """524,288 paths x 50 dates (the American-put benchmark size): a job that
+    spans every SM; repeatable to the bit and within 5 SE of the binomial price."""
+    r = req("american_put", n_paths=524288, n_steps=50, seed=42, r=0.06, basis_degree=3, s0=100.0,
+            precision=precision)
+    a = backend.price(r)
+    b = backend.price(r)
+    assert a.price == b.price and a.early_exercise_count == b.early_exercise_count
+    crr = O.crr_put(100.0, 100, 0.06, 0.2, 1.0, 2048)
+    assert abs(a.price - crr) < 5 * a.stderr + 0.05
+    assert a.regression_steps == 49
+
+
+def test_lsm_batch_equals_individual(backend):
+    """Several LSM requests packed into shared cooperative launches give the
+    same results as one launch each (each job keeps its block partition)."""
+    reqs = [req("american_put", n_paths=20000 + 7000 * i, n_steps=30 + 5 * i, seed=10 + i, r=0.06,
+                basis_degree=1 + i % 3, s0=90.0 + 10 * i) for i in range(3)]
+    reqs += [req("bermudan_put", n_paths=12000, n_steps=40, seed=4, exercise_steps=[10, 20, 30, 40],
+                 precision="fp64_plain"),
+             req("american_put", n_paths=9000, n_steps=25, seed=8, precision="fp64_plain", s0=95.0)]
+    batch = backend.price_batch(reqs)
+    for r, got in zip(reqs, batch):
+        one = backend.price(r)
+        assert got.status == abi.OK
+        assert got.price == one.price, (got.price, one.price)
+        assert got.early_exercise_count == one.early_exercise_count
+        assert got.regression_steps == one.regression_steps
+
+
 # -------------------------------------------------------------------- MLMC --
 def test_mlmc_fp64_plain_matches_oracle(backend):
     r = make_request("arithmetic_asian_mlmc", {"paths_per_level": [4000, 2000, 1000, 500], "seed": 3,
@@ -228,6 +259,21 @@ def test_mlmc_tolerance_fp32(backend):
     a, b = backend.price(r), O.price(r)
     assert abs(a.price - b.price) < 3 * math.hypot(a.stderr, b.stderr)
     assert a.total_step_updates <= r.max_step_updates * 1.01 + 64
+
+
+def test_mlmc_batch_equals_individual(backend):
+    """MLMC requests batched (all pilot levels in one launch, all main levels
+    in another) give the same results as each request alone."""
+    reqs = [make_request("arithmetic_asian_mlmc", {"target_stderr": 0.03, "levels": 4, "seed": 20 + i})
+            for i in range(3)]
+    reqs.append(make_request("arithmetic_asian_mlmc", {"paths_per_level": [4000, 2000, 1000], "levels": 3,
+                                                        "seed": 5, "precision": "fp64_plain"}))
+    batch = backend.price_batch(reqs)
+    for r, got in zip(reqs, batch):
+        one = backend.price(r)
+        assert got.status == abi.OK
+        assert got.price == one.price and got.stderr == one.stderr
+        assert got.total_step_updates == one.total_step_updates
 
 
 # ------------------------------------------------------ batch and serving ---
