@@ -322,7 +322,7 @@ int mpc_measure_peaks(mpc_context_t* ctx, double* fp32_tflops, double* sfu_tops)
  * forbidden.  It has no counterpart in the reference.
  *  - Runs on the current device and `stream` (a cudaStream_t, NULL = legacy
  *    default stream) and returns after the result is on the host.
- *  - Device buffers are file-scope static arrays of fixed size (about 0.6 MB
+ *  - Device buffers are file-scope static arrays of fixed size (about 0.7 MB
  *    per GPU, held until the process exits): at most 16,777,216 paths (or
  *    antithetic pairs) per request; larger requests return MPC_E_OOM_BUDGET.
  *  - Samplers: pseudorandom, counter_hash, scrambled_sobol; path-payoff

@@ -40,13 +40,17 @@ enum Workload : int32_t {
 };
 
 struct SrcCtx {
-  const uint32_t* sobol;
+  const uint32_t* sobol;  // both Sobol table layouts (MPC_SOBOL_TABLE_WORDS)
   const uint64_t* jump;
-  uint32_t* win;  // shared-memory window of Sobol tables (fused kernel), null elsewhere
+  uint32_t* win;  // shared-memory window of Sobol table rows (fused kernel), null elsewhere
 };
 
-// Dimensions of the Sobol tables staged in shared memory at a time (32 KB).
+// Dimensions of the Sobol table rows staged in shared memory at a time, and
+// the row stride in words: kSobolWindow + 4 is 4 mod 32, so the 16 rows one
+// warp touches with a 128-bit load fall into two wavefronts.
 constexpr uint32_t kSobolWindow = 64;
+constexpr uint32_t kSobolRowStride = kSobolWindow + 4;
+constexpr uint32_t kSobolWindowWords = 128 * kSobolRowStride;  // 34,816 bytes
 
 // ------------------------------------------------------------- sources ----
 // A Source yields the samples of one unit (path or antithetic pair) by
@@ -79,36 +83,21 @@ struct Source<SMP_COUNTER> {
 // and its nibble offsets depend only on (point, dimension group of 256), so
 // they are recomputed when a path crosses into the next group; per
 // dimension only the 8 table lookups and the output scramble remain.  The
-// values equal sobol_point() bit for bit.
+// values equal sobol_point() bit for bit.  Reads the [dim][q][v] layout from
+// global memory (generators and the FP64 plain path).
 template <>
 struct Source<SMP_SOBOL> {
   const uint32_t* table;
-  uint32_t* win;        // shared-memory window, or null to read the global table
-  uint32_t win_first;   // first dimension held in the window
   uint32_t local, block_seed, group, seed_g, combine_g;
   uint32_t off[8];
   template <bool FP64>
   __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
     table = c.sobol;
-    win = c.win;
-    win_first = 0xFFFFFFFFu;
     local = (uint32_t)(u & 0xFFFFu);
     block_seed = q.seed32 + (uint32_t)(u >> 16) * 0x9E3779B9u;
     group = 0xFFFFFFFFu;
   }
-  // Block-synchronous: stages the tables of dimensions [d0, d0 + kSobolWindow)
-  // when this step's dimensions are not all in the window.
-  __device__ __forceinline__ void at_step(uint32_t d0, uint32_t count) {
-    if (!win) return;
-    if (win_first != 0xFFFFFFFFu && d0 >= win_first && d0 + count <= win_first + kSobolWindow) return;
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < kSobolWindow * 128; i += blockDim.x) {
-      const uint32_t dim = (d0 + (i >> 7)) & (MPC_SOBOL_TABLE_DIMS - 1);
-      win[i] = __ldg(table + dim * 128 + (i & 127));
-    }
-    __syncthreads();
-    win_first = d0;
-  }
+  __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
   __device__ __forceinline__ uint32_t sample(uint32_t d) {
     const uint32_t g = d / MPC_SOBOL_TABLE_DIMS;
     if (g != group) {
@@ -120,16 +109,10 @@ struct Source<SMP_SOBOL> {
       combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
     }
     const uint32_t dim = d & (MPC_SOBOL_TABLE_DIMS - 1);
+    const uint32_t* td = table + dim * 128;
     uint32_t x = 0;
-    if (win) {
-      const uint32_t* td = win + (d - win_first) * 128;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) x ^= td[off[q]];
-    } else {
-      const uint32_t* td = table + dim * 128;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) x ^= __ldg(td + off[q]);
-    }
+    for (int q = 0; q < 8; ++q) x ^= __ldg(td + off[q]);
     return nested_uniform_scramble(x, seed_g ^ (dim + combine_g));  // hash_combine(seed_g, dim)
   }
   __device__ __forceinline__ float n32(uint32_t d) { return normcdfinvf(sobol_unit_f32(sample(d))); }
@@ -200,6 +183,120 @@ struct Source<SMP_XORSHIFT> {
   __device__ __forceinline__ double n64(uint32_t) { return st.normal_f64(); }
   __device__ __forceinline__ double u64(uint32_t) { return st.next_open01(); }
   __device__ __forceinline__ float u32(uint32_t) { return (float)st.next_open01(); }
+};
+
+// ------------------------------------------------ fused FP32 sources ---
+// The fused kernels draw their samples through FusedSource<SMP>::type:
+// the generic sources except for scrambled Sobol and the counter hash.
+
+// Scrambled Sobol for the fused kernels, bit-identical to Source<SMP_SOBOL>.
+// A block-synchronous window in shared memory holds, for each table row
+// r = 16 q + v, the bit-reversed nibble products of kSobolWindow consecutive
+// dimensions, so one 128-bit load per nibble position serves four
+// dimensions: a quad of dimensions costs 8 shared loads and 28 XORs instead
+// of 32 loads.  XOR commutes with bit reversal, so the quad holds brev(x)
+// and the output scramble skips its first reversal.
+struct SobolQuad {
+  const uint32_t* rows_global;  // [128][256] bit-reversed rows
+  uint32_t* win;                // [128][kSobolRowStride] shared-memory window
+  uint32_t win_first;           // first dimension in the window (multiple of 4)
+  uint32_t local, block_seed, group, seed_g, combine_g, quad;
+  uint32_t rows[8];             // window word offset of this point's row per nibble position
+  uint32_t x0, x1, x2, x3;      // reversed products of the dimensions of `quad`
+  template <bool FP64>
+  __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
+    rows_global = c.sobol + MPC_SOBOL_NIBBLE_WORDS;
+    win = c.win;
+    win_first = 0xFFFFFFFFu;
+    local = (uint32_t)(u & 0xFFFFu);
+    block_seed = q.seed32 + (uint32_t)(u >> 16) * 0x9E3779B9u;
+    group = 0xFFFFFFFFu;
+    quad = 0xFFFFFFFFu;
+  }
+  // Block-synchronous: restages the window at d0 rounded down to a multiple
+  // of 4 when [d0, d0 + count) is not inside it.  Requires
+  // count <= kSobolWindow - 3 so that the step fits the aligned window.
+  __device__ __forceinline__ void at_step(uint32_t d0, uint32_t count) {
+    if (win_first != 0xFFFFFFFFu && d0 >= win_first && d0 + count <= win_first + kSobolWindow) return;
+    __syncthreads();
+    const uint32_t w0 = d0 & ~3u;
+    for (uint32_t i = threadIdx.x; i < 128 * kSobolWindow; i += blockDim.x) {
+      const uint32_t row = i / kSobolWindow, j = i % kSobolWindow;
+      win[row * kSobolRowStride + j] =
+          __ldg(rows_global + row * MPC_SOBOL_TABLE_DIMS + ((w0 + j) & (MPC_SOBOL_TABLE_DIMS - 1)));
+    }
+    __syncthreads();
+    win_first = w0;
+  }
+  __device__ __forceinline__ uint32_t sample(uint32_t d) {
+    const uint32_t g = d / MPC_SOBOL_TABLE_DIMS;
+    if (g != group) {
+      group = g;
+      seed_g = block_seed + g;
+      const uint32_t shuffled = nested_uniform_scramble(local, seed_g);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) rows[k] = (16u * k + ((shuffled >> (4 * k)) & 0xFu)) * kSobolRowStride;
+      combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
+      quad = 0xFFFFFFFFu;
+    }
+    if ((d >> 2) != quad) {
+      quad = d >> 2;
+      const uint32_t* base = win + ((d & ~3u) - win_first);
+      uint4 a = *reinterpret_cast<const uint4*>(base + rows[0]);
+#pragma unroll
+      for (int k = 1; k < 8; ++k) {
+        const uint4 b = *reinterpret_cast<const uint4*>(base + rows[k]);
+        a.x ^= b.x;
+        a.y ^= b.y;
+        a.z ^= b.z;
+        a.w ^= b.w;
+      }
+      x0 = a.x;
+      x1 = a.y;
+      x2 = a.z;
+      x3 = a.w;
+    }
+    const uint32_t k = d & 3u;
+    const uint32_t xr = (k & 2u) ? ((k & 1u) ? x3 : x2) : ((k & 1u) ? x1 : x0);
+    return __brev(lk_permute(xr, seed_g ^ ((d & (MPC_SOBOL_TABLE_DIMS - 1)) + combine_g)));
+  }
+  __device__ __forceinline__ float u32(uint32_t d) { return sobol_unit_f32_bits(sample(d)); }
+  __device__ __forceinline__ float n32(uint32_t d) { return normcdfinvf(u32(d)); }
+  __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sample(d)); }
+  __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
+};
+
+// Counter-hash normals for the fused kernels: the reference's u32 hashes
+// with the short FP32 transform (counter_normal_fast).
+struct CounterFast {
+  uint32_t seed, unit;
+  template <bool FP64>
+  __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx&, uint64_t u) {
+    seed = q.seed32;
+    unit = (uint32_t)u;
+  }
+  __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
+  __device__ __forceinline__ float n32(uint32_t d) { return counter_normal_fast(seed, unit, d); }
+  __device__ __forceinline__ float u32(uint32_t d) {
+    return counter_open01_fast(hash_u32(counter_mix(seed, unit, d, 0u)));
+  }
+  __device__ __forceinline__ double n64(uint32_t d) { return (double)counter_normal_f32(seed, unit, d); }
+  __device__ __forceinline__ double u64(uint32_t d) {
+    return (double)counter_open01(hash_u32(counter_mix(seed, unit, d, 0u)));
+  }
+};
+
+template <int SMP>
+struct FusedSource {
+  using type = Source<SMP>;
+};
+template <>
+struct FusedSource<SMP_SOBOL> {
+  using type = SobolQuad;
+};
+template <>
+struct FusedSource<SMP_COUNTER> {
+  using type = CounterFast;
 };
 
 // Reads materialised samples [dim][unit] (FP64 plain path).
@@ -488,8 +585,8 @@ __device__ __forceinline__ void unit_mlmc(const DevReq& q, Src& src, double& pay
   uint32_t j = 0;
   for (uint64_t c = 0; c < q.coarse_steps; ++c) {
     Real zsum = 0;
-    src.at_step(j, M);
     for (uint32_t m = 0; m < M; ++m) {
+      src.at_step(j, 1);  // one dimension at a time: M may exceed what a window step holds
       const Real z = normal<Real>(src, j++);
       zsum += z;
       fl += fd + fv * z;
@@ -553,7 +650,7 @@ __device__ __forceinline__ void run_family(const DevReq& q, Src& src, double& p,
 
 template <int FAM, int SMP>
 __device__ __forceinline__ void fused_unit(const DevReq& q, const SrcCtx& ctx, uint64_t u, double& p, double& c) {
-  Source<SMP> src;
+  typename FusedSource<SMP>::type src;
   src.template begin<false>(q, ctx, u);
   run_family<float, FAM>(q, src, p, c);
 }
@@ -655,7 +752,7 @@ template <int FAM, int SMP>
 __global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused_kernel(const DevReq* __restrict__ reqs,
                                                             const Tile* __restrict__ tiles, uint32_t n_tiles,
                                                             uint32_t* __restrict__ counter, SrcCtx ctx) {
-  extern __shared__ uint32_t sobol_window[];
+  extern __shared__ __align__(16) uint32_t sobol_window[];
   ctx.win = SMP == SMP_SOBOL ? sobol_window : nullptr;
   __shared__ DevReq sq;
   __shared__ double red[kWarps][5];
@@ -720,7 +817,7 @@ __global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused
 
 template <int SMP>
 constexpr size_t fused_dynamic_smem() {
-  return SMP == SMP_SOBOL ? kSobolWindow * 128 * sizeof(uint32_t) : 0;
+  return SMP == SMP_SOBOL ? kSobolWindowWords * sizeof(uint32_t) : 0;
 }
 
 template <int FAM, int SMP>

@@ -9,7 +9,7 @@
 // needs -- the request descriptor, the tile work list, the per-tile moment
 // partials, the completion counters and the lookup tables -- in file-scope
 // static __device__ arrays of fixed size.  Each GPU that loads the library
-// holds these arrays (about 0.6 MB) until the process exits.
+// holds these arrays (about 0.7 MB) until the process exits.
 
 #include <cuda_runtime.h>
 
@@ -45,7 +45,7 @@ struct NoAllocScratch {
 // host-side stand-ins, not device addresses; device addresses come from
 // cudaGetSymbolAddress in setup_device().
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
-static __device__ __align__(256) uint32_t g_noalloc_sobol[MPC_SOBOL_TABLE_DIMS * 8 * 16];
+static __device__ __align__(256) uint32_t g_noalloc_sobol[MPC_SOBOL_TABLE_WORDS];
 static __device__ __align__(256) uint64_t g_noalloc_jump[64 * 256];
 
 struct DeviceState {

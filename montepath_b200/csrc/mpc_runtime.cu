@@ -867,7 +867,6 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     void* arena = nullptr;
     int st = scratch(ctx, "lsm_arena", bytes, &arena);
     if (st != MPC_OK) return st;
-    size_t host_bytes = bytes - 0;
     std::vector<uint8_t> host(align(group.size() * sizeof(LsmArgs)));
     uint8_t* base = static_cast<uint8_t*>(arena);
     uint32_t block_first = 0;
@@ -908,7 +907,6 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       block_first += j.blocks;
       std::memcpy(host.data() + g * sizeof(LsmArgs), &a, sizeof(LsmArgs));
     }
-    (void)host_bytes;
     MPC_CUDA(ctx, cudaMemcpyAsync(base, host.data(), group.size() * sizeof(LsmArgs), cudaMemcpyHostToDevice,
                                   ctx->stream));
     h2d += group.size() * sizeof(LsmArgs);
@@ -1280,7 +1278,12 @@ static int price_one(mpc_context* ctx, const mpc_request_t* req, mpc_result_t* o
 
 // ----------------------------------------------------------- device setup ---
 void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {
-  sob.assign(size_t(MPC_SOBOL_TABLE_DIMS) * 8 * 16, 0u);
+  sob.assign(size_t(MPC_SOBOL_TABLE_WORDS), 0u);
+  auto reverse = [](uint32_t x) {
+    uint32_t r = 0;
+    for (int b = 0; b < 32; ++b) r |= ((x >> b) & 1u) << (31 - b);
+    return r;
+  };
   for (int d = 0; d < MPC_SOBOL_TABLE_DIMS; ++d)
     for (int q = 0; q < 8; ++q)
       for (int v = 0; v < 16; ++v) {
@@ -1288,6 +1291,7 @@ void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {
         for (int j = 0; j < 4; ++j)
           if ((v >> j) & 1) x ^= kSobolDirections[d][4 * q + j];
         sob[(size_t(d) * 8 + q) * 16 + v] = x;
+        sob[MPC_SOBOL_NIBBLE_WORDS + size_t(q * 16 + v) * MPC_SOBOL_TABLE_DIMS + d] = reverse(x);
       }
   // Columns of the xorshift64* transition T (image of each basis vector), then T^(2^b).
   auto step = [](uint64_t x) {

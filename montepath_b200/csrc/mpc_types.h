@@ -4,6 +4,12 @@
 #include <stdint.h>
 
 #define MPC_SOBOL_TABLE_DIMS 256
+// The device Sobol table holds two layouts of the same nibble products:
+// [dim][q][v] (words 0 .. MPC_SOBOL_NIBBLE_WORDS) for per-sample lookups, and
+// from MPC_SOBOL_NIBBLE_WORDS on the bit-reversed transpose [16 q + v][dim]
+// that the fused kernels stage into shared memory rows.
+#define MPC_SOBOL_NIBBLE_WORDS (MPC_SOBOL_TABLE_DIMS * 8 * 16)
+#define MPC_SOBOL_TABLE_WORDS (2 * MPC_SOBOL_NIBBLE_WORDS)
 // Moments per tile / request: count, sum p, sum p^2, sum c, sum c^2, sum p*c (+2 pad).
 #define MPC_MOMENTS 8
 
