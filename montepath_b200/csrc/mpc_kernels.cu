@@ -40,9 +40,10 @@ enum Workload : int32_t {
 };
 
 struct SrcCtx {
-  const uint32_t* sobol;  // both Sobol table layouts (MPC_SOBOL_TABLE_WORDS)
+  const uint32_t* sobol;  // device lookup table (MPC_SOBOL_TABLE_WORDS words)
   const uint64_t* jump;
-  uint32_t* win;  // shared-memory window of Sobol table rows (fused kernel), null elsewhere
+  uint32_t* win;          // shared-memory window of Sobol table rows (fused kernel), null elsewhere
+  const float4* icdf;     // shared-memory copy of the inverse-normal segments (fused kernel)
 };
 
 // Dimensions of the Sobol table rows staged in shared memory at a time, and
@@ -51,6 +52,21 @@ struct SrcCtx {
 constexpr uint32_t kSobolWindow = 64;
 constexpr uint32_t kSobolRowStride = kSobolWindow + 4;
 constexpr uint32_t kSobolWindowWords = 128 * kSobolRowStride;  // 34,816 bytes
+
+// Phi^-1(u) for a 23-bit midpoint uniform u from the segment table: v =
+// min(u, 1 - u) (exact) selects binade and one of 32 segments from its
+// exponent and top mantissa bits, the remaining 18 mantissa bits give the
+// position t in the segment, and the segment's cubic gives Phi^-1(v).
+// Defined for v in [2^-24, 1/2), which every 23-bit midpoint uniform meets.
+__device__ __forceinline__ float icdf_segments(const float4* __restrict__ seg, float u) {
+  const float v = fminf(u, 1.0f - u);
+  const uint32_t bits = __float_as_uint(v);
+  const uint32_t idx = (bits >> 18) - (103u << 5);  // (exponent - 103) * 32 + top 5 mantissa bits
+  const float t = __int_as_float(((bits << 5) & 0x7FFFFFu) | 0x3F800000u) - 1.0f;
+  const float4 c = seg[idx];
+  const float p = fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x);
+  return u < 0.5f ? p : -p;
+}
 
 // ------------------------------------------------------------- sources ----
 // A Source yields the samples of one unit (path or antithetic pair) by
@@ -199,6 +215,7 @@ struct Source<SMP_XORSHIFT> {
 struct SobolQuad {
   const uint32_t* rows_global;  // [128][256] bit-reversed rows
   uint32_t* win;                // [128][kSobolRowStride] shared-memory window
+  const float4* icdf;           // inverse-normal segments in shared memory
   uint32_t win_first;           // first dimension in the window (multiple of 4)
   uint32_t local, block_seed, group, seed_g, combine_g, quad;
   uint32_t rows[8];             // window word offset of this point's row per nibble position
@@ -207,6 +224,7 @@ struct SobolQuad {
   __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
     rows_global = c.sobol + MPC_SOBOL_NIBBLE_WORDS;
     win = c.win;
+    icdf = c.icdf;
     win_first = 0xFFFFFFFFu;
     local = (uint32_t)(u & 0xFFFFu);
     block_seed = q.seed32 + (uint32_t)(u >> 16) * 0x9E3779B9u;
@@ -228,8 +246,10 @@ struct SobolQuad {
     __syncthreads();
     win_first = w0;
   }
-  __device__ __forceinline__ uint32_t sample(uint32_t d) {
-    const uint32_t g = d / MPC_SOBOL_TABLE_DIMS;
+  // Loads the quad of dimensions [d0, d0 + 4), d0 a multiple of 4 inside
+  // the window (the chunked model loops call it directly).
+  __device__ __forceinline__ void quad_load(uint32_t d0) {
+    const uint32_t g = d0 / MPC_SOBOL_TABLE_DIMS;
     if (g != group) {
       group = g;
       seed_g = block_seed + g;
@@ -237,31 +257,46 @@ struct SobolQuad {
 #pragma unroll
       for (int k = 0; k < 8; ++k) rows[k] = (16u * k + ((shuffled >> (4 * k)) & 0xFu)) * kSobolRowStride;
       combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
-      quad = 0xFFFFFFFFu;
     }
-    if ((d >> 2) != quad) {
-      quad = d >> 2;
-      const uint32_t* base = win + ((d & ~3u) - win_first);
-      uint4 a = *reinterpret_cast<const uint4*>(base + rows[0]);
+    quad = d0 >> 2;
+    const uint32_t* base = win + (d0 - win_first);
+    uint4 a = *reinterpret_cast<const uint4*>(base + rows[0]);
 #pragma unroll
-      for (int k = 1; k < 8; ++k) {
-        const uint4 b = *reinterpret_cast<const uint4*>(base + rows[k]);
-        a.x ^= b.x;
-        a.y ^= b.y;
-        a.z ^= b.z;
-        a.w ^= b.w;
-      }
-      x0 = a.x;
-      x1 = a.y;
-      x2 = a.z;
-      x3 = a.w;
+    for (int k = 1; k < 8; ++k) {
+      const uint4 b = *reinterpret_cast<const uint4*>(base + rows[k]);
+      a.x ^= b.x;
+      a.y ^= b.y;
+      a.z ^= b.z;
+      a.w ^= b.w;
     }
-    const uint32_t k = d & 3u;
-    const uint32_t xr = (k & 2u) ? ((k & 1u) ? x3 : x2) : ((k & 1u) ? x1 : x0);
+    x0 = a.x;
+    x1 = a.y;
+    x2 = a.z;
+    x3 = a.w;
+  }
+  // Scrambled value of dimension d0 + K of the quad loaded at d0.
+  __device__ __forceinline__ uint32_t scramble(uint32_t xr, uint32_t d) const {
     return __brev(lk_permute(xr, seed_g ^ ((d & (MPC_SOBOL_TABLE_DIMS - 1)) + combine_g)));
   }
+  template <int K>
+  __device__ __forceinline__ uint32_t take(uint32_t d0) const {
+    return scramble(K == 0 ? x0 : K == 1 ? x1 : K == 2 ? x2 : x3, d0 + K);
+  }
+  template <int K>
+  __device__ __forceinline__ float take_u(uint32_t d0) const {
+    return sobol_unit_f32_bits(take<K>(d0));
+  }
+  template <int K>
+  __device__ __forceinline__ float take_n(uint32_t d0) const {
+    return icdf_segments(icdf, take_u<K>(d0));
+  }
+  __device__ __forceinline__ uint32_t sample(uint32_t d) {
+    if ((d >> 2) != quad) quad_load(d & ~3u);
+    const uint32_t k = d & 3u;
+    return scramble((k & 2u) ? ((k & 1u) ? x3 : x2) : ((k & 1u) ? x1 : x0), d);
+  }
   __device__ __forceinline__ float u32(uint32_t d) { return sobol_unit_f32_bits(sample(d)); }
-  __device__ __forceinline__ float n32(uint32_t d) { return normcdfinvf(u32(d)); }
+  __device__ __forceinline__ float n32(uint32_t d) { return icdf_segments(icdf, u32(d)); }
   __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sample(d)); }
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
 };
@@ -285,6 +320,12 @@ struct CounterFast {
     return (double)counter_open01(hash_u32(counter_mix(seed, unit, d, 0u)));
   }
 };
+
+// Sources with the explicit-quad interface (quad_load / take_n / take_u).
+template <class S>
+constexpr bool kQuadSource = false;
+template <>
+constexpr bool kQuadSource<SobolQuad> = true;
 
 template <int SMP>
 struct FusedSource {
@@ -366,9 +407,7 @@ __device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double&
   Real acc0 = (W == W_LOOKBACK) ? (Real)q.s0 : (Real)0, acc1 = acc0;
   bool ko0 = (W == W_DAO && q.s0 <= q.barrier) || (W == W_UAO && q.s0 >= q.barrier), ko1 = ko0;
   const uint32_t n = q.n_steps;
-  for (uint32_t s = 0; s < n; ++s) {
-    src.at_step(s, 1);
-    const Real z = normal<Real>(src, s);
+  auto advance = [&](const Real z) {
     ls0 += drift + vol * z;
     if (anti) ls1 += drift - vol * z;
     if constexpr (W == W_ASIAN) {
@@ -394,6 +433,21 @@ __device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double&
         if (anti) ko1 |= ex<Real>(ls1) >= bar;
       }
     }
+  };
+  uint32_t s = 0;
+  if constexpr (kQuadSource<Src>) {
+    for (; s + 4 <= n; s += 4) {  // four steps per quad of dimensions
+      src.at_step(s, 4);
+      src.quad_load(s);
+      advance(src.template take_n<0>(s));
+      advance(src.template take_n<1>(s));
+      advance(src.template take_n<2>(s));
+      advance(src.template take_n<3>(s));
+    }
+  }
+  for (; s < n; ++s) {
+    src.at_step(s, 1);
+    advance(normal<Real>(src, s));
   }
   auto payoff = [&](Real ls, Real acc, bool ko) -> Real {
     Real v;
@@ -447,10 +501,7 @@ __device__ __forceinline__ void unit_heston(const DevReq& q, Src& src, double& p
   const bool anti = q.anti != 0;
   Real ls0 = (Real)q.log_s0, ls1 = ls0, v0 = (Real)q.v0, v1 = v0;
   const uint32_t n = q.n_steps;
-  for (uint32_t s = 0; s < n; ++s) {
-    src.at_step(2 * s, 2);
-    const Real zv = normal<Real>(src, 2 * s);
-    const Real zi = normal<Real>(src, 2 * s + 1);
+  auto step = [&](const Real zv, const Real zi) {
     {
       Real vp = v0 > (Real)0 ? v0 : (Real)0;
       Real sv = sq_root<Real>(vp);
@@ -467,6 +518,22 @@ __device__ __forceinline__ void unit_heston(const DevReq& q, Src& src, double& p
       v1 = v1 + kappa * (theta - vp) * dt + xi * sv * sqdt * (-zv);
       v1 = v1 > (Real)0 ? v1 : (Real)0;
     }
+  };
+  uint32_t s = 0;
+  if constexpr (kQuadSource<Src>) {
+    for (; s + 2 <= n; s += 2) {  // two steps per quad: dimensions 2s .. 2s + 3
+      const uint32_t d0 = 2 * s;
+      src.at_step(d0, 4);
+      src.quad_load(d0);
+      step(src.template take_n<0>(d0), src.template take_n<1>(d0));
+      step(src.template take_n<2>(d0), src.template take_n<3>(d0));
+    }
+  }
+  for (; s < n; ++s) {
+    src.at_step(2 * s, 2);
+    const Real zv = normal<Real>(src, 2 * s);
+    const Real zi = normal<Real>(src, 2 * s + 1);
+    step(zv, zi);
   }
   const Real kk = (Real)q.k, disc = (Real)q.discount;
   Real st = ex<Real>(ls0);
@@ -488,7 +555,36 @@ __device__ __forceinline__ void unit_merton(const DevReq& q, Src& src, double& p
   const Real drift = (Real)q.drift_dt, vol = (Real)q.vol_dt, jm = (Real)q.jump_mean, jv = (Real)q.jump_vol;
   Real ls = (Real)q.log_s0;
   const uint32_t n = STEP ? q.n_steps : 1;
-  for (uint32_t s = 0; s < n; ++s) {
+  uint32_t s0 = 0;
+  if constexpr (kQuadSource<Src>) {
+    // four steps per three quads: step k of the chunk uses dimensions
+    // d0 + 3k (z), d0 + 3k + 1 (Poisson uniform), d0 + 3k + 2 (jump normal)
+    const float lam_p0_f = q.lam_p0_f;
+    auto step = [&](const float z, const float u, auto&& jump_normal) {
+      ls += drift + vol * z;
+      if (u > lam_p0_f) {
+        const uint32_t jumps = poisson_tail((double)u, q.lam_dt, q.lam_p0);
+        if (jumps > 0) ls += (Real)jumps * jm + jv * sq_root<Real>((Real)jumps) * jump_normal();
+      }
+    };
+    for (; s0 + 4 <= n; s0 += 4) {
+      const uint32_t d0 = 3 * s0;
+      src.at_step(d0, 12);
+      src.quad_load(d0);
+      const float z0 = src.template take_n<0>(d0), u0 = src.template take_u<1>(d0);
+      step(z0, u0, [&] { return src.template take_n<2>(d0); });
+      const float z1 = src.template take_n<3>(d0);
+      src.quad_load(d0 + 4);
+      const float u1 = src.template take_u<0>(d0 + 4);
+      step(z1, u1, [&] { return src.template take_n<1>(d0 + 4); });
+      const float z2 = src.template take_n<2>(d0 + 4), u2 = src.template take_u<3>(d0 + 4);
+      src.quad_load(d0 + 8);
+      step(z2, u2, [&] { return src.template take_n<0>(d0 + 8); });
+      step(src.template take_n<1>(d0 + 8), src.template take_u<2>(d0 + 8),
+           [&] { return src.template take_n<3>(d0 + 8); });
+    }
+  }
+  for (uint32_t s = s0; s < n; ++s) {
     src.at_step(3 * s, 3);
     const Real z = normal<Real>(src, 3 * s);
     uint32_t jumps;
@@ -753,7 +849,17 @@ __global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused
                                                             const Tile* __restrict__ tiles, uint32_t n_tiles,
                                                             uint32_t* __restrict__ counter, SrcCtx ctx) {
   extern __shared__ __align__(16) uint32_t sobol_window[];
-  ctx.win = SMP == SMP_SOBOL ? sobol_window : nullptr;
+  if constexpr (SMP == SMP_SOBOL) {
+    // window rows, then the inverse-normal segments (staged once per launch)
+    float4* seg = reinterpret_cast<float4*>(sobol_window + kSobolWindowWords);
+    const float4* src = reinterpret_cast<const float4*>(ctx.sobol + MPC_ICDF_OFFSET);
+    for (uint32_t i = threadIdx.x; i < MPC_ICDF_SEGMENTS; i += blockDim.x) seg[i] = src[i];
+    ctx.win = sobol_window;
+    ctx.icdf = seg;
+  } else {
+    ctx.win = nullptr;
+    ctx.icdf = nullptr;
+  }
   __shared__ DevReq sq;
   __shared__ double red[kWarps][5];
   __shared__ uint32_t s_tile;
@@ -817,7 +923,7 @@ __global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused
 
 template <int SMP>
 constexpr size_t fused_dynamic_smem() {
-  return SMP == SMP_SOBOL ? kSobolWindowWords * sizeof(uint32_t) : 0;
+  return SMP == SMP_SOBOL ? kSobolWindowWords * sizeof(uint32_t) + MPC_ICDF_SEGMENTS * sizeof(float4) : 0;
 }
 
 template <int FAM, int SMP>

