@@ -234,15 +234,22 @@ struct SobolQuad {
   // Block-synchronous: restages the window at d0 rounded down to a multiple
   // of 4 when [d0, d0 + count) is not inside it.  Requires
   // count <= kSobolWindow - 3 so that the step fits the aligned window.
+  // The copy is 16-byte asynchronous global-to-shared transfers (four
+  // dimensions of one row each; an aligned quad never crosses the 256-dimension
+  // wrap), all in flight at once, then one wait.
   __device__ __forceinline__ void at_step(uint32_t d0, uint32_t count) {
     if (win_first != 0xFFFFFFFFu && d0 >= win_first && d0 + count <= win_first + kSobolWindow) return;
     __syncthreads();
     const uint32_t w0 = d0 & ~3u;
-    for (uint32_t i = threadIdx.x; i < 128 * kSobolWindow; i += blockDim.x) {
-      const uint32_t row = i / kSobolWindow, j = i % kSobolWindow;
-      win[row * kSobolRowStride + j] =
-          __ldg(rows_global + row * MPC_SOBOL_TABLE_DIMS + ((w0 + j) & (MPC_SOBOL_TABLE_DIMS - 1)));
+    constexpr uint32_t kQuadsPerRow = kSobolWindow / 4;
+    const uint32_t win_s = (uint32_t)__cvta_generic_to_shared(win);
+    for (uint32_t i = threadIdx.x; i < 128 * kQuadsPerRow; i += blockDim.x) {
+      const uint32_t row = i / kQuadsPerRow, j = 4 * (i % kQuadsPerRow);
+      const uint32_t* src = rows_global + row * MPC_SOBOL_TABLE_DIMS + ((w0 + j) & (MPC_SOBOL_TABLE_DIMS - 1));
+      const uint32_t dst = win_s + 4u * (row * kSobolRowStride + j);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
     win_first = w0;
   }
