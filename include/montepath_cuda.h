@@ -185,6 +185,56 @@ typedef struct mpc_result {
 #define MPC_WARN_SCHEDULE_NORMALISED 0x4u
 #define MPC_WARN_INTRINSIC_FLOOR 0x8u
 
+/* Greeks.  Greek / GreekEstimator / GreekEstimate / GreekReport of the
+ * reference (crates/mc-core/src/runtime/cpu.rs:138-192). */
+typedef enum mpc_greek {
+  MPC_GREEK_DELTA = 0,
+  MPC_GREEK_DELTA2 = 1, /* basket: second spot */
+  MPC_GREEK_VEGA = 2,   /* Heston: sensitivity to sqrt(v0), theta held fixed */
+  MPC_GREEK_VEGA2 = 3,  /* basket: second volatility */
+  MPC_GREEK_RHO = 4,
+  MPC_GREEK_THETA = 5   /* conventional calendar theta (minus d price / d maturity) */
+} mpc_greek_t;
+
+typedef enum mpc_greek_estimator {
+  MPC_GREEKS_BUMP_AND_REVALUE = 0, /* central common-random-number differences, cpu.rs:4938-4983 */
+  MPC_GREEKS_PATHWISE = 1,         /* terminal-GBM European call, cpu.rs:4670-4765 */
+  MPC_GREEKS_LIKELIHOOD_RATIO = 2  /* terminal-GBM European call, cpu.rs:4767-4869 */
+} mpc_greek_estimator_t;
+
+#define MPC_MAX_GREEKS 6
+
+typedef struct mpc_greek_estimate {
+  int32_t greek;     /* mpc_greek_t */
+  int32_t estimator; /* mpc_greek_estimator_t */
+  double value;
+  double stderr;           /* bump: independent-leg propagation; single pass: sample standard error */
+  double bump_size;        /* effective half-width of the central difference (0 for single pass) */
+  double base_price;
+  double bumped_up_price;   /* bump only */
+  double bumped_down_price; /* bump only */
+} mpc_greek_estimate_t;
+
+typedef struct mpc_greek_report {
+  int32_t workload;  /* mpc_workload_t */
+  int32_t estimator; /* mpc_greek_estimator_t */
+  uint64_t paths;
+  uint32_t steps;
+  uint32_t n_estimates;
+  uint64_t seed;
+  double base_price;
+  double base_stderr;
+  double runtime_ms; /* device time of all launches of the report */
+  mpc_greek_estimate_t estimates[MPC_MAX_GREEKS];
+  uint32_t warnings; /* bit set of MPC_GREEK_WARN_* */
+  int32_t status;
+} mpc_greek_report_t;
+
+/* The reference's report warnings, as flags. */
+#define MPC_GREEK_WARN_ESTIMATOR_UNSUPPORTED 0x1u /* no estimates: the estimator is not offered for this workload */
+#define MPC_GREEK_WARN_PSEUDORANDOM_SHOCKS 0x2u   /* single-pass estimators draw the pseudorandom stream whatever the sampling */
+#define MPC_GREEK_WARN_TECHNIQUE_IGNORED 0x4u     /* single-pass estimators ignore the variance-reduction technique */
+
 typedef struct mpc_device_info {
   int32_t index;
   int32_t sm_count;
@@ -245,7 +295,7 @@ typedef struct mpc_server_stats {
 /* ----- library and devices -------------------------------------------- */
 int mpc_abi_version(void);
 /* Sizes of the ABI structs, for binding self-checks (ctypes, cgo). */
-size_t mpc_struct_size(int which); /* 0 request, 1 result, 2 device_info, 3 options, 4 support, 5 artifact, 6 server_options, 7 server_stats */
+size_t mpc_struct_size(int which); /* 0 request, 1 result, 2 device_info, 3 options, 4 support, 5 artifact, 6 server_options, 7 server_stats, 8 greek_report */
 const char* mpc_status_string(int status);
 
 /* Replaces NvidiaCudaBackend::discover_devices' nvidia-smi parsing (cuda.rs:205-241). */
@@ -274,6 +324,21 @@ int mpc_price(mpc_context_t* ctx, const mpc_request_t* req, mpc_result_t* out);
 /* Prices n requests in one graph-captured persistent launch (fused FP32 path)
  * or, for FP64-plain requests, one launch sequence per request. */
 int mpc_price_batch(mpc_context_t* ctx, const mpc_request_t* reqs, size_t n, mpc_result_t* out);
+/* Greeks of one request: european_call_greeks_cpu, arithmetic_asian_call_greeks_cpu,
+ * down_and_out_call_greeks_cpu, lookback_call_greeks_cpu, basket_call_greeks_cpu,
+ * heston_european_call_greeks_cpu (cpu.rs:4036-4356).
+ *  - BUMP_AND_REVALUE: the base request and an up and a down bump per Greek
+ *    (spot 1% (min 0.01), volatility 5% (min 0.005), rate 0.001, maturity
+ *    min(1/365, T/4)), all with the request's seed, priced in one batch (one
+ *    persistent launch on the FP32 path).
+ *  - PATHWISE / LIKELIHOOD_RATIO: European call only; one pass over the
+ *    pseudorandom terminal shocks of the request's seed (the reference's
+ *    MonteCarloRng stream) on the device, base price from the request itself.
+ *    Other workloads return MPC_OK with no estimates and
+ *    MPC_GREEK_WARN_ESTIMATOR_UNSUPPORTED, as the reference does.
+ *  - Merton, LSM and MLMC requests: MPC_E_UNSUPPORTED (the reference has no
+ *    Greeks for them). */
+int mpc_greeks(mpc_context_t* ctx, const mpc_request_t* req, int estimator, mpc_greek_report_t* out);
 /* Per-path discounted payoffs of a (small) request, for same-normals parity
  * checks (the per-path output of mc_cuda_european_call_stepwise_v1).  Writes
  * n_samples doubles (pairs: the block estimate) to host memory. */

@@ -124,6 +124,25 @@ WARN_THREADS_IGNORED = 0x2
 WARN_SCHEDULE_NORMALISED = 0x4
 WARN_INTRINSIC_FLOOR = 0x8
 
+# mpc_greek_t / mpc_greek_estimator_t
+GREEK_DELTA = 0
+GREEK_DELTA2 = 1
+GREEK_VEGA = 2
+GREEK_VEGA2 = 3
+GREEK_RHO = 4
+GREEK_THETA = 5
+GREEK_NAMES = {GREEK_DELTA: "delta", GREEK_DELTA2: "delta2", GREEK_VEGA: "vega", GREEK_VEGA2: "vega2",
+               GREEK_RHO: "rho", GREEK_THETA: "theta"}
+GREEKS_BUMP_AND_REVALUE = 0
+GREEKS_PATHWISE = 1
+GREEKS_LIKELIHOOD_RATIO = 2
+GREEK_ESTIMATORS = {"bump_and_revalue": GREEKS_BUMP_AND_REVALUE, "pathwise": GREEKS_PATHWISE,
+                    "likelihood_ratio": GREEKS_LIKELIHOOD_RATIO}
+MAX_GREEKS = 6
+GREEK_WARN_ESTIMATOR_UNSUPPORTED = 0x1
+GREEK_WARN_PSEUDORANDOM_SHOCKS = 0x2
+GREEK_WARN_TECHNIQUE_IGNORED = 0x4
+
 
 class Request(Structure):
     _fields_ = [
@@ -280,7 +299,37 @@ class ServerStats(Structure):
     ]
 
 
-STRUCTS = [Request, Result, DeviceInfo, Options, Support, Artifact, ServerOptions, ServerStats]
+class GreekEstimate(Structure):
+    _fields_ = [
+        ("greek", c_int32),
+        ("estimator", c_int32),
+        ("value", c_double),
+        ("stderr", c_double),
+        ("bump_size", c_double),
+        ("base_price", c_double),
+        ("bumped_up_price", c_double),
+        ("bumped_down_price", c_double),
+    ]
+
+
+class GreekReport(Structure):
+    _fields_ = [
+        ("workload", c_int32),
+        ("estimator", c_int32),
+        ("paths", c_uint64),
+        ("steps", c_uint32),
+        ("n_estimates", c_uint32),
+        ("seed", c_uint64),
+        ("base_price", c_double),
+        ("base_stderr", c_double),
+        ("runtime_ms", c_double),
+        ("estimates", GreekEstimate * MAX_GREEKS),
+        ("warnings", c_uint32),
+        ("status", c_int32),
+    ]
+
+
+STRUCTS = [Request, Result, DeviceInfo, Options, Support, Artifact, ServerOptions, ServerStats, GreekReport]
 
 # (name, restype, argtypes) of every exported entry point, in header order.
 FUNCTIONS = [
@@ -299,6 +348,7 @@ FUNCTIONS = [
     ("mpc_prepare", c_int, [c_void_p, POINTER(Request), POINTER(Artifact)]),
     ("mpc_price", c_int, [c_void_p, POINTER(Request), POINTER(Result)]),
     ("mpc_price_batch", c_int, [c_void_p, POINTER(Request), c_size_t, POINTER(Result)]),
+    ("mpc_greeks", c_int, [c_void_p, POINTER(Request), c_int, POINTER(GreekReport)]),
     ("mpc_price_paths", c_int, [c_void_p, POINTER(Request), POINTER(c_double), c_uint64]),
     ("mpc_generate_normals", c_int, [c_void_p, c_int, c_uint64, c_uint64, c_uint32, c_int, c_void_p]),
     ("mpc_counter_hash_u32", c_int, [c_void_p, c_uint32, c_uint32, c_uint32, POINTER(c_uint32)]),

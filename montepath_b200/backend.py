@@ -72,6 +72,16 @@ class CudaBackend:
         self._check(self.lib.mpc_price_batch(self.handle, arr, n, out))
         return list(out)
 
+    def greeks(self, req: abi.Request, estimator: int | str = abi.GREEKS_BUMP_AND_REVALUE) -> abi.GreekReport:
+        """GreekReport of one request (the reference's ``*_greeks_cpu``):
+        bump-and-revalue for every workload with Greeks, pathwise and
+        likelihood ratio for the terminal-GBM European call."""
+        if isinstance(estimator, str):
+            estimator = abi.GREEK_ESTIMATORS[estimator]
+        rep = abi.GreekReport()
+        self._check(self.lib.mpc_greeks(self.handle, byref(req), int(estimator), byref(rep)))
+        return rep
+
     def price_paths(self, req: abi.Request) -> np.ndarray:
         units = req.n_paths
         if req.technique == abi.TECHNIQUE_ANTITHETIC:

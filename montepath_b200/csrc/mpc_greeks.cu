@@ -1,0 +1,242 @@
+// mpc_greeks.cu -- Greeks of one pricing request (mpc_greeks).
+//
+// Restates the reference's Greek reports (crates/mc-core/src/runtime/cpu.rs:
+// european_call_greeks_cpu and siblings 4036-4356, bump recipe 4938-5008,
+// single-pass estimators 4670-4869) on the device:
+//  - bump-and-revalue: the base request plus an up and a down bump per Greek,
+//    all with the request's seed (common random numbers), priced by one
+//    mpc_price_batch call -- on the FP32 path that is one persistent launch
+//    for all 9 (13 for a basket) scenarios;
+//  - pathwise / likelihood ratio: one kernel pass over the pseudorandom
+//    terminal shocks of the request's seed, sums in FP64.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "../../include/montepath_cuda.h"
+#include "mpc_launch.h"
+#include "mpc_runtime.h"
+
+namespace mpc {
+namespace {
+
+// Bump sizes and floors (bump_spot / bump_volatility / bump_rate /
+// bump_maturity / parameter_floor, cpu.rs:4985-5008).
+double bump_spot(double spot) { return std::max(std::fabs(spot) * 0.01, 0.01); }
+double bump_volatility(double vol) { return std::max(std::fabs(vol) * 0.05, 0.005); }
+double bump_rate() { return 0.001; }
+double bump_maturity(double t) { return std::min(1.0 / 365.0, t * 0.25); }
+double parameter_floor(int greek) { return greek == MPC_GREEK_RHO ? -1.0 : 2.2250738585072014e-308; }
+
+// The parameter a bump moves.
+enum Param { P_S0, P_SIGMA, P_R, P_T, P_SPOT0, P_SPOT1, P_SIGMA0, P_SIGMA1, P_SQRT_V0 };
+
+struct Bump {
+  int greek;
+  Param param;
+  double center, bump;
+  bool reverse;  // theta: minus the maturity derivative
+};
+
+void set_param(mpc_request_t& q, Param p, double x) {
+  switch (p) {
+    case P_S0: q.s0 = x; break;
+    case P_SIGMA: q.sigma = x; break;
+    case P_R: q.r = x; break;
+    case P_T: q.t = x; break;
+    case P_SPOT0: q.spots[0] = x; break;
+    case P_SPOT1: q.spots[1] = x; break;
+    case P_SIGMA0: q.sigmas[0] = x; break;
+    case P_SIGMA1: q.sigmas[1] = x; break;
+    case P_SQRT_V0: {  // Heston vega moves sqrt(v0), theta fixed (cpu.rs:4610-4626)
+      const double c = std::max(x, 0.0);
+      q.v0 = c * c;
+      break;
+    }
+  }
+}
+
+// The Greeks each workload reports (cpu.rs:4047-4356, 4409-4668); empty when
+// the reference has no Greeks for it (Merton, LSM, MLMC).
+std::vector<Bump> bumps_of(const mpc_request_t& r) {
+  std::vector<Bump> v;
+  const Bump rho{MPC_GREEK_RHO, P_R, r.r, bump_rate(), false};
+  const Bump theta{MPC_GREEK_THETA, P_T, r.t, bump_maturity(r.t), true};
+  switch (r.workload) {
+    case MPC_WORKLOAD_BASKET_CALL:
+      v = {{MPC_GREEK_DELTA, P_SPOT0, r.spots[0], bump_spot(r.spots[0]), false},
+           {MPC_GREEK_DELTA2, P_SPOT1, r.spots[1], bump_spot(r.spots[1]), false},
+           {MPC_GREEK_VEGA, P_SIGMA0, r.sigmas[0], bump_volatility(r.sigmas[0]), false},
+           {MPC_GREEK_VEGA2, P_SIGMA1, r.sigmas[1], bump_volatility(r.sigmas[1]), false},
+           rho,
+           theta};
+      return v;
+    case MPC_WORKLOAD_EUROPEAN_CALL:
+      if (r.model == MPC_MODEL_HESTON) {
+        const double sv = std::sqrt(std::max(r.v0, 0.0));
+        v = {{MPC_GREEK_DELTA, P_S0, r.s0, bump_spot(r.s0), false},
+             {MPC_GREEK_VEGA, P_SQRT_V0, sv, bump_volatility(sv), false},
+             rho,
+             theta};
+        return v;
+      }
+      [[fallthrough]];
+    case MPC_WORKLOAD_ARITHMETIC_ASIAN_CALL:
+    case MPC_WORKLOAD_DOWN_AND_OUT_CALL:
+    case MPC_WORKLOAD_UP_AND_OUT_CALL:
+    case MPC_WORKLOAD_LOOKBACK_CALL:
+      if (r.model != MPC_MODEL_GBM) return v;
+      v = {{MPC_GREEK_DELTA, P_S0, r.s0, bump_spot(r.s0), false},
+           {MPC_GREEK_VEGA, P_SIGMA, r.sigma, bump_volatility(r.sigma), false},
+           rho,
+           theta};
+      return v;
+    default:
+      return v;
+  }
+}
+
+// push_bump_estimate (cpu.rs:4938-4983) for one bump from the priced legs.
+void bump_estimate(const Bump& b, const mpc_result_t& base, const mpc_result_t& up, const mpc_result_t& down,
+                   mpc_greek_estimate_t* e) {
+  const double lo = std::max(b.center - b.bump, parameter_floor(b.greek));
+  const double eff = ((b.center + b.bump) - lo) * 0.5;
+  const double raw = eff > 0.0 ? (up.price - down.price) / (2.0 * eff) : 0.0;
+  e->greek = b.greek;
+  e->estimator = MPC_GREEKS_BUMP_AND_REVALUE;
+  e->value = b.reverse ? -raw : raw;
+  e->stderr = eff > 0.0 ? std::sqrt(up.stderr * up.stderr + down.stderr * down.stderr) / (2.0 * eff) : 0.0;
+  e->bump_size = eff;
+  e->base_price = base.price;
+  e->bumped_up_price = up.price;
+  e->bumped_down_price = down.price;
+}
+
+// MomentAccumulator::mean_stderr (cpu.rs:4846-4869): (n - 1) sample variance.
+void mean_stderr(double sum, double sq, uint64_t count, double* mean, double* se) {
+  if (count == 0) {
+    *mean = *se = 0.0;
+    return;
+  }
+  const double n = double(count);
+  *mean = sum / n;
+  const double var = count > 1 ? std::max((sq - sum * sum / n) / (n - 1.0), 0.0) : 0.0;
+  *se = std::sqrt(var / n);
+}
+
+}  // namespace
+}  // namespace mpc
+
+using namespace mpc;
+
+#define GREEKS_CUDA(call)                                             \
+  do {                                                                \
+    cudaError_t _e = (call);                                          \
+    if (_e != cudaSuccess) return finish(cuda_fail(ctx, _e, #call)); \
+  } while (0)
+
+extern "C" int mpc_greeks(mpc_context_t* ctx, const mpc_request_t* req, int estimator, mpc_greek_report_t* out) {
+  if (!ctx || !req || !out) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  cudaSetDevice(ctx->device);
+  const mpc_request_t& r = *req;
+  std::memset(out, 0, sizeof(*out));
+  out->workload = r.workload;
+  out->estimator = estimator;
+  out->paths = r.n_paths;
+  out->steps = r.workload == MPC_WORKLOAD_BASKET_CALL ? 2u : r.n_steps;
+  out->seed = r.seed;
+  auto finish = [&](int st) {
+    out->status = st;
+    return st;
+  };
+  if (estimator < MPC_GREEKS_BUMP_AND_REVALUE || estimator > MPC_GREEKS_LIKELIHOOD_RATIO)
+    return finish(fail(ctx, MPC_E_INVALID_CONFIG, "unknown Greek estimator"));
+  const std::vector<Bump> bumps = bumps_of(r);
+  if (bumps.empty())
+    return finish(fail(ctx, MPC_E_UNSUPPORTED, "no Greeks for this workload/model (the reference offers none)"));
+
+  if (estimator == MPC_GREEKS_BUMP_AND_REVALUE) {
+    // base, then (up, down) per Greek, every request with the same seed
+    std::vector<mpc_request_t> reqs(1 + 2 * bumps.size(), r);
+    for (size_t i = 0; i < bumps.size(); ++i) {
+      const Bump& b = bumps[i];
+      set_param(reqs[1 + 2 * i], b.param, b.center + b.bump);
+      set_param(reqs[2 + 2 * i], b.param, std::max(b.center - b.bump, parameter_floor(b.greek)));
+    }
+    std::vector<mpc_result_t> res(reqs.size());
+    const int st = mpc_price_batch(ctx, reqs.data(), reqs.size(), res.data());
+    out->runtime_ms = ctx->last_ms;
+    if (st != MPC_OK) return finish(st);
+    out->base_price = res[0].price;
+    out->base_stderr = res[0].stderr;
+    for (size_t i = 0; i < bumps.size(); ++i)
+      bump_estimate(bumps[i], res[0], res[1 + 2 * i], res[2 + 2 * i], &out->estimates[out->n_estimates++]);
+    return finish(MPC_OK);
+  }
+
+  // single-pass estimators: the base price is the request's own price
+  mpc_result_t base;
+  int st = mpc_price(ctx, req, &base);
+  if (st != MPC_OK) return finish(st);
+  double total_ms = ctx->last_ms;
+  out->base_price = base.price;
+  out->base_stderr = base.stderr;
+  const bool terminal_gbm_call = r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.model == MPC_MODEL_GBM;
+  if (!terminal_gbm_call) {  // unsupported_greek_report (cpu.rs:4917-4936)
+    out->warnings |= MPC_GREEK_WARN_ESTIMATOR_UNSUPPORTED;
+    out->runtime_ms = total_ms;
+    return finish(MPC_OK);
+  }
+  if (!(r.s0 > 0.0) || !(r.sigma > 0.0) || !(r.t > 0.0))  // cpu.rs:4671-4674
+    return finish(fail(ctx, MPC_E_INVALID_CONFIG, "single-pass Greeks need s0 > 0, sigma > 0 and t > 0"));
+  GreekArgs a{};
+  a.seed = r.seed;
+  a.n_paths = r.n_paths;
+  a.s0 = r.s0;
+  a.k = r.k;
+  a.r = r.r;
+  a.sigma = r.sigma;
+  a.t = r.t;
+  a.sqrt_t = std::sqrt(r.t);
+  a.drift_t = (r.r - 0.5 * r.sigma * r.sigma) * r.t;
+  a.vol_t = r.sigma * a.sqrt_t;
+  a.discount = std::exp(-r.r * r.t);
+  a.estimator = estimator;
+  a.fp64 = r.precision == MPC_PRECISION_FP64_PLAIN ? 1 : 0;
+  const uint64_t want = (r.n_paths + 255) / 256;
+  const uint32_t grid = uint32_t(std::max<uint64_t>(1, std::min<uint64_t>(want, uint64_t(ctx->sm_count) * 8)));
+  void* d = nullptr;
+  // partials [grid][8] | totals [8] | counter
+  if ((st = scratch(ctx, "greeks", (size_t(grid) * 8 + 8) * sizeof(double) + 64, &d)) != MPC_OK) return finish(st);
+  a.partials = static_cast<double*>(d);
+  a.out = a.partials + size_t(grid) * 8;
+  a.done = reinterpret_cast<unsigned*>(a.out + 8);
+  double host[8];
+  GREEKS_CUDA(cudaMemsetAsync(a.done, 0, sizeof(unsigned), ctx->stream));
+  GREEKS_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+  cudaError_t e = launch_greeks_single_pass(a, grid, ctx->tabs, ctx->stream);
+  if (e != cudaSuccess) return finish(cuda_fail(ctx, e, "single-pass Greeks kernel"));
+  GREEKS_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+  GREEKS_CUDA(cudaMemcpyAsync(host, a.out, sizeof(host), cudaMemcpyDeviceToHost, ctx->stream));
+  GREEKS_CUDA(cudaStreamSynchronize(ctx->stream));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  out->runtime_ms = total_ms + ms;
+  const int names[4] = {MPC_GREEK_DELTA, MPC_GREEK_VEGA, MPC_GREEK_RHO, MPC_GREEK_THETA};
+  const int count = estimator == MPC_GREEKS_PATHWISE ? 4 : 3;
+  for (int g = 0; g < count; ++g) {
+    mpc_greek_estimate_t& est = out->estimates[out->n_estimates++];
+    est.greek = names[g];
+    est.estimator = estimator;
+    mean_stderr(host[2 * g], host[2 * g + 1], r.n_paths, &est.value, &est.stderr);
+    est.base_price = base.price;
+  }
+  if (r.sampling != MPC_SAMPLING_PSEUDORANDOM) out->warnings |= MPC_GREEK_WARN_PSEUDORANDOM_SHOCKS;
+  if (r.technique != MPC_TECHNIQUE_STANDARD) out->warnings |= MPC_GREEK_WARN_TECHNIQUE_IGNORED;
+  return finish(MPC_OK);
+}

@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/montepath_cuda.h"
 #include "mpc_device.cuh"
 #include "mpc_launch.h"
 #include "mpc_types.h"
@@ -1568,6 +1569,82 @@ cudaError_t launch_lsm_batch(const LsmArgs* d_jobs, uint32_t n_jobs, uint32_t to
   }
   if (sampler == SMP_COUNTER) return launch_lsm_t<float, SMP_COUNTER>(d_jobs, n_jobs, total_blocks, ctx, stream);
   return launch_lsm_t<float, SMP_XORSHIFT>(d_jobs, n_jobs, total_blocks, ctx, stream);
+}
+
+// ------------------------------------------------------ single-pass Greeks ---
+// european_call_pathwise_greeks_cpu / european_call_likelihood_ratio_greeks_cpu
+// (cpu.rs:4670-4869): path i draws normal i of MonteCarloRng(seed) (one
+// sequential stream, replayed by jump-ahead), prices the terminal GBM state
+// and records the per-path estimators; sums and sums of squares in FP64,
+// combined in block order by the last block.
+template <class Real>
+__global__ void __launch_bounds__(256) greeks_single_pass_kernel(GreekArgs a, const uint64_t* __restrict__ jump) {
+  __shared__ double red[kWarps][5];
+  __shared__ int s_last;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const Real s0 = (Real)a.s0, k = (Real)a.k, r = (Real)a.r, sigma = (Real)a.sigma, t = (Real)a.t;
+  const Real sqrt_t = (Real)a.sqrt_t, drift_t = (Real)a.drift_t, vol_t = (Real)a.vol_t, disc = (Real)a.discount;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n_paths; i += stride) {
+    XorshiftStream st;
+    st.seek(jump, a.seed, i, sizeof(Real) == 4);
+    const Real z = sizeof(Real) == 4 ? (Real)st.normal_f32() : (Real)st.normal_f64();
+    const Real s = s0 * ex<Real>(drift_t + vol_t * z);
+    Real g[4];
+    if (a.estimator == MPC_GREEKS_PATHWISE) {
+      const Real intrinsic = s - k;
+      const bool active = intrinsic > (Real)0;
+      const Real payoff = intrinsic > (Real)0 ? intrinsic : (Real)0;
+      const Real dpay = disc * payoff;
+      g[0] = active ? disc * s / s0 : (Real)0;
+      g[1] = active ? disc * s * (-sigma * t + sqrt_t * z) : (Real)0;
+      g[2] = active ? disc * (t * s - t * payoff) : -t * dpay;
+      const Real dst_dt = s * (r - (Real)0.5 * sigma * sigma + sigma * z / ((Real)2 * sqrt_t));
+      g[3] = -(active ? disc * (dst_dt - r * payoff) : -r * dpay);
+    } else {
+      const Real dpay = disc * (s - k > (Real)0 ? s - k : (Real)0);
+      g[0] = dpay * z / (s0 * sigma * sqrt_t);
+      g[1] = dpay * ((z * z - (Real)1) / sigma - sqrt_t * z);
+      g[2] = dpay * (z / (sigma * sqrt_t) - t);
+      g[3] = (Real)0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double v = (double)g[j];
+      acc[2 * j] += v;
+      acc[2 * j + 1] += v * v;
+    }
+  }
+  double v0[5] = {acc[0], acc[1], acc[2], acc[3], acc[4]};
+  double v1[5] = {acc[5], acc[6], acc[7], 0.0, 0.0};
+  block_reduce5(v0, red);
+  block_reduce5(v1, red);
+  if (threadIdx.x == 0) {
+    double* pt = a.partials + (size_t)blockIdx.x * 8;
+    for (int j = 0; j < 5; ++j) pt[j] = v0[j];
+    for (int j = 0; j < 3; ++j) pt[5 + j] = v1[j];
+    __threadfence();
+    s_last = atomicAdd(a.done, 1u) == gridDim.x - 1 ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x < 8) {
+    double sum = 0.0;
+    for (uint32_t b = 0; b < gridDim.x; ++b) sum += __ldcg(a.partials + (size_t)b * 8 + threadIdx.x);
+    a.out[threadIdx.x] = sum;
+  }
+  if (threadIdx.x == 0) *a.done = 0u;
+}
+
+cudaError_t launch_greeks_single_pass(const GreekArgs& a, uint32_t grid, const DeviceTables& tabs,
+                                      cudaStream_t stream) {
+  if (a.fp64)
+    greeks_single_pass_kernel<double><<<grid, 256, 0, stream>>>(a, tabs.jump);
+  else
+    greeks_single_pass_kernel<float><<<grid, 256, 0, stream>>>(a, tabs.jump);
+  count_launch();
+  return cudaGetLastError();
 }
 
 // ------------------------------------------------------------ generators ---

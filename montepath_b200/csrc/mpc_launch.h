@@ -82,6 +82,22 @@ uint32_t lsm_capacity(int fp64, int sampler);
 constexpr uint32_t kLsmPathsPerThreadMax = 8;
 constexpr uint32_t kLsmThreads = 256;
 
+// Single-pass Greek estimators of the terminal-GBM European call
+// (pathwise: delta, vega, rho, theta; likelihood ratio: delta, vega, rho)
+// over the pseudorandom terminal shocks of one MonteCarloRng stream.
+struct GreekArgs {
+  uint64_t seed, n_paths;
+  double s0, k, r, sigma, t;
+  double sqrt_t, drift_t, vol_t, discount;
+  int32_t estimator;  // mpc_greek_estimator_t (PATHWISE or LIKELIHOOD_RATIO)
+  int32_t fp64;       // 1: FP64 shocks and arithmetic; 0: FP32 path arithmetic
+  double* partials;   // [grid][8]: sum and sum of squares of 4 estimators
+  double* out;        // [8] totals in block order
+  unsigned* done;     // last-block counter (zero before the launch, zero after)
+};
+cudaError_t launch_greeks_single_pass(const GreekArgs& a, uint32_t grid, const DeviceTables& tabs,
+                                      cudaStream_t stream);
+
 // Device generators for the ABI's sampler entry points.
 cudaError_t launch_generate_normals(const DevReq& q, int sampler, int fp32, void* d_out, uint64_t n_points,
                                     uint32_t dims, const DeviceTables& tabs, cudaStream_t stream);

@@ -1413,6 +1413,8 @@ size_t mpc_struct_size(int which) {
       return sizeof(mpc_server_options_t);
     case 7:
       return sizeof(mpc_server_stats_t);
+    case 8:
+      return sizeof(mpc_greek_report_t);
     default:
       return 0;
   }

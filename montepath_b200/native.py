@@ -237,6 +237,110 @@ def price_european_call_parameter_sweep(config: Mapping[str, Any]) -> dict:
     }
 
 
+# ---------------------------------------------------------------- Greeks --
+_GREEK_WARNINGS = {
+    abi.GREEK_WARN_ESTIMATOR_UNSUPPORTED: "this estimator is not offered for this workload; use bump_and_revalue",
+    abi.GREEK_WARN_PSEUDORANDOM_SHOCKS: "single-pass estimators draw pseudorandom terminal shocks whatever the sampling",
+    abi.GREEK_WARN_TECHNIQUE_IGNORED: "single-pass estimators ignore the configured variance-reduction technique",
+}
+_GREEK_WORKLOADS = {
+    "european_call": ("european_call", {}),
+    "arithmetic_asian_call": ("arithmetic_asian_call", {}),
+    "down_and_out_call": ("down_and_out_call", {}),
+    "up_and_out_call": ("up_and_out_call", {}),
+    "lookback_call": ("lookback_call", {}),
+    "basket_call": ("basket_call", {}),
+    "heston_european_call": ("european_call", {"model": "heston", "method": "stepwise"}),
+}
+
+
+def greek_report_to_dict(rep: abi.GreekReport, workload: str) -> dict:
+    """GreekReport in the field names of the reference's serde shape (cpu.rs:158-182)."""
+
+    estimator = {v: k for k, v in abi.GREEK_ESTIMATORS.items()}[rep.estimator]
+    single = rep.estimator != abi.GREEKS_BUMP_AND_REVALUE
+    estimates = []
+    for i in range(rep.n_estimates):
+        e = rep.estimates[i]
+        estimates.append({
+            "greek": abi.GREEK_NAMES[e.greek],
+            "estimator": estimator,
+            "value": e.value,
+            "stderr": e.stderr,
+            "bump_size": None if single else e.bump_size,
+            "base_price": e.base_price,
+            "bumped_up_price": None if single else e.bumped_up_price,
+            "bumped_down_price": None if single else e.bumped_down_price,
+            "stderr_estimate_kind": "sample standard error of the single-pass estimator" if single
+            else "independent-leg propagation (common random numbers usually make the true error smaller)",
+        })
+    return {
+        "workload": workload,
+        "estimator": estimator,
+        "paths": rep.paths,
+        "steps": rep.steps,
+        "seed": rep.seed,
+        "base_price": rep.base_price,
+        "base_stderr": rep.base_stderr,
+        "estimated_runtime_ms": rep.runtime_ms,
+        "estimates": estimates,
+        "warnings": [text for flag, text in _GREEK_WARNINGS.items() if rep.warnings & flag],
+    }
+
+
+def greeks(config: Mapping[str, Any]) -> dict:
+    """``<workload>_greeks_cpu(cfg, estimator)`` (cpu.rs:4036-4356) on the GPU.
+
+    ``config`` carries ``workload`` (one of european_call, arithmetic_asian_call,
+    down_and_out_call, up_and_out_call, lookback_call, basket_call,
+    heston_european_call), ``estimator`` (bump_and_revalue | pathwise |
+    likelihood_ratio) and the workload's pricing fields.
+    """
+
+    cfg = dict(config or {})
+    workload = cfg.pop("workload", "european_call")
+    estimator = cfg.pop("estimator", "bump_and_revalue")
+    if workload not in _GREEK_WORKLOADS:
+        raise ValueError(f"MC_CONFIG_INVALID: no Greeks for workload {workload!r}")
+    code, extra = _GREEK_WORKLOADS[workload]
+    params = dict(cfg)
+    params.update(extra)
+    try:
+        req = make_request(code, params)
+        rep = backend().greeks(req, estimator)
+    except ConfigError as exc:
+        raise ValueError(f"MC_CONFIG_INVALID: {exc}") from exc
+    except KeyError as exc:
+        raise ValueError(f"MC_CONFIG_INVALID: unknown estimator {estimator!r}") from exc
+    except BackendError as exc:
+        raise ValueError(f"MC_BACKEND_CUDA_{exc.code.replace('MPC_E_', '')}: {exc}") from exc
+    out = greek_report_to_dict(rep, workload)
+    out["manifest"] = _manifest(workload, "greeks", dict(config or {}), req)
+    return out
+
+
+def price_all_current_greeks_bump_and_revalue(config: Mapping[str, Any]) -> list[dict]:
+    """price_all_current_greeks_bump_and_revalue_cpu (cpu.rs:4358-4407): the
+    bump-and-revalue report of every workload with Greeks, at default
+    configs, seeds ``seed`` .. ``seed + 5``."""
+
+    cfg = dict(config or {})
+    n_paths, n_steps, seed = int(cfg.get("n_paths", 10_000)), int(cfg.get("n_steps", 64)), int(cfg.get("seed", 42))
+    order = ["european_call", "arithmetic_asian_call", "down_and_out_call", "lookback_call", "basket_call",
+             "heston_european_call"]
+    reports = []
+    for i, workload in enumerate(order):
+        params = {"workload": workload, "n_paths": n_paths, "seed": (seed + i) % (1 << 64),
+                  "estimator": "bump_and_revalue"}
+        if workload != "basket_call":
+            params["n_steps"] = n_steps
+        for key in ("precision", "sampling"):
+            if key in cfg:
+                params[key] = cfg[key]
+        reports.append(greeks(params))
+    return reports
+
+
 # Aliases in the naming of the Metal bridge.
 price_european_call_cuda = price_european_call
 price_arithmetic_asian_call_cuda = price_arithmetic_asian_call
@@ -249,3 +353,4 @@ price_bermudan_put_cuda = price_bermudan_put
 price_heston_european_call_cuda = price_heston_european_call
 price_merton_jump_diffusion_call_cuda = price_merton_jump_diffusion_call
 arithmetic_asian_mlmc_cuda = arithmetic_asian_mlmc
+greeks_cuda = greeks

@@ -1616,6 +1616,187 @@ void price_from_f32_normals(const mpc_request_t& r, const float* normals, mpc_re
   std::memcpy(res->moments, mom, sizeof mom);
 }
 
+// --------------------------------------------------------------- Greeks ---
+// Bump sizes and floors (cpu.rs:4985-5008).
+static double bump_spot(double spot) { return std::max(std::fabs(spot) * 0.01, 0.01); }
+static double bump_volatility(double vol) { return std::max(std::fabs(vol) * 0.05, 0.005); }
+static double bump_rate() { return 0.001; }
+static double bump_maturity(double t) { return std::min(1.0 / 365.0, t * 0.25); }
+static double parameter_floor(int greek) { return greek == MPC_GREEK_RHO ? -1.0 : kMinPositive; }
+
+// MomentAccumulator::mean_stderr (cpu.rs:4846-4869): (n - 1) sample variance.
+struct GreekMoments {
+  double sum = 0.0, sq = 0.0;
+  uint64_t count = 0;
+  void record(double v) {
+    sum += v;
+    sq += v * v;
+    ++count;
+  }
+  void mean_stderr(double* mean, double* se) const {
+    if (count == 0) {
+      *mean = *se = 0.0;
+      return;
+    }
+    const double n = double(count);
+    *mean = sum / n;
+    const double var = count > 1 ? std::max((sq - sum * sum / n) / (n - 1.0), 0.0) : 0.0;
+    *se = std::sqrt(var / n);
+  }
+};
+
+// One bumped parameter of the bump-and-revalue recipe.
+struct BumpSpec {
+  int greek;
+  double center, bump;
+  bool reverse;
+  std::function<void(mpc_request_t&, double)> set;
+};
+
+// The Greeks a workload offers and how each parameter is bumped
+// (european_call_bump_greeks_cpu, cpu.rs:4409-4482; Asian, barrier and
+// lookback cpu.rs:4047-4323; basket_call_bump_greeks_cpu, cpu.rs:4484-4590;
+// heston_call_bump_greeks_cpu, cpu.rs:4592-4668).  Empty = no Greeks.
+static std::vector<BumpSpec> bump_specs(const mpc_request_t& r) {
+  std::vector<BumpSpec> v;
+  const auto rho = BumpSpec{MPC_GREEK_RHO, r.r, bump_rate(), false, [](mpc_request_t& q, double x) { q.r = x; }};
+  const auto theta =
+      BumpSpec{MPC_GREEK_THETA, r.t, bump_maturity(r.t), true, [](mpc_request_t& q, double x) { q.t = x; }};
+  switch (r.workload) {
+    case MPC_WORKLOAD_BASKET_CALL:
+      v.push_back({MPC_GREEK_DELTA, r.spots[0], bump_spot(r.spots[0]), false,
+                   [](mpc_request_t& q, double x) { q.spots[0] = x; }});
+      v.push_back({MPC_GREEK_DELTA2, r.spots[1], bump_spot(r.spots[1]), false,
+                   [](mpc_request_t& q, double x) { q.spots[1] = x; }});
+      v.push_back({MPC_GREEK_VEGA, r.sigmas[0], bump_volatility(r.sigmas[0]), false,
+                   [](mpc_request_t& q, double x) { q.sigmas[0] = x; }});
+      v.push_back({MPC_GREEK_VEGA2, r.sigmas[1], bump_volatility(r.sigmas[1]), false,
+                   [](mpc_request_t& q, double x) { q.sigmas[1] = x; }});
+      v.push_back(rho);
+      v.push_back(theta);
+      return v;
+    case MPC_WORKLOAD_EUROPEAN_CALL:
+      if (r.model == MPC_MODEL_MERTON) return v;
+      if (r.model == MPC_MODEL_HESTON) {
+        const double sv = std::sqrt(std::max(r.v0, 0.0));
+        v.push_back({MPC_GREEK_DELTA, r.s0, bump_spot(r.s0), false, [](mpc_request_t& q, double x) { q.s0 = x; }});
+        v.push_back({MPC_GREEK_VEGA, sv, bump_volatility(sv), false, [](mpc_request_t& q, double x) {
+                       const double c = std::max(x, 0.0);
+                       q.v0 = c * c;
+                     }});
+        v.push_back(rho);
+        v.push_back(theta);
+        return v;
+      }
+      [[fallthrough]];
+    case MPC_WORKLOAD_ARITHMETIC_ASIAN_CALL:
+    case MPC_WORKLOAD_DOWN_AND_OUT_CALL:
+    case MPC_WORKLOAD_UP_AND_OUT_CALL:
+    case MPC_WORKLOAD_LOOKBACK_CALL:
+      if (r.model != MPC_MODEL_GBM) return v;
+      v.push_back({MPC_GREEK_DELTA, r.s0, bump_spot(r.s0), false, [](mpc_request_t& q, double x) { q.s0 = x; }});
+      v.push_back({MPC_GREEK_VEGA, r.sigma, bump_volatility(r.sigma), false,
+                   [](mpc_request_t& q, double x) { q.sigma = x; }});
+      v.push_back(rho);
+      v.push_back(theta);
+      return v;
+    default:
+      return v;
+  }
+}
+
+// european_call_pathwise_greeks_cpu / european_call_likelihood_ratio_greeks_cpu
+// (cpu.rs:4670-4869): one pass over the terminal shocks of MonteCarloRng(seed).
+static void single_pass(const mpc_request_t& r, int estimator, GreekMoments m[4]) {
+  McRng rng(r.seed);
+  const double sqrt_t = std::sqrt(r.t);
+  const double drift_t = (r.r - 0.5 * r.sigma * r.sigma) * r.t;
+  const double vol_t = r.sigma * sqrt_t;
+  const double discount = std::exp(-r.r * r.t);
+  for (uint64_t i = 0; i < r.n_paths; ++i) {
+    const double z = rng.standard_normal();
+    const double st = r.s0 * std::exp(drift_t + vol_t * z);
+    if (estimator == MPC_GREEKS_PATHWISE) {
+      const double intrinsic = st - r.k;
+      const bool active = intrinsic > 0.0;
+      const double payoff = std::max(intrinsic, 0.0);
+      const double dpay = discount * payoff;
+      m[0].record(active ? discount * st / r.s0 : 0.0);
+      m[1].record(active ? discount * st * (-r.sigma * r.t + sqrt_t * z) : 0.0);
+      m[2].record(active ? discount * (r.t * st - r.t * payoff) : -r.t * dpay);
+      const double dst_dt = st * (r.r - 0.5 * r.sigma * r.sigma + r.sigma * z / (2.0 * sqrt_t));
+      const double dmat = active ? discount * (dst_dt - r.r * payoff) : -r.r * dpay;
+      m[3].record(-dmat);
+    } else {
+      const double dpay = discount * std::max(st - r.k, 0.0);
+      m[0].record(dpay * z / (r.s0 * r.sigma * sqrt_t));
+      const double vega_score = (z * z - 1.0) / r.sigma - sqrt_t * z;
+      m[1].record(dpay * vega_score);
+      m[2].record(dpay * (z / (r.sigma * sqrt_t) - r.t));
+    }
+  }
+}
+
+// GreekReport of one request (european_call_greeks_cpu and siblings,
+// cpu.rs:4036-4356; push_bump_estimate cpu.rs:4938-4983).
+int greeks(const mpc_request_t& r, int estimator, mpc_greek_report_t* out) {
+  std::memset(out, 0, sizeof(*out));
+  out->workload = r.workload;
+  out->estimator = estimator;
+  out->paths = r.n_paths;
+  out->steps = r.workload == MPC_WORKLOAD_BASKET_CALL ? 2u : r.n_steps;
+  out->seed = r.seed;
+  const std::vector<BumpSpec> specs = bump_specs(r);
+  if (specs.empty()) return MPC_E_UNSUPPORTED;
+  mpc_result_t base;
+  price(r, &base, Out{});
+  out->base_price = base.price;
+  out->base_stderr = base.stderr;
+  if (estimator == MPC_GREEKS_BUMP_AND_REVALUE) {
+    for (const BumpSpec& b : specs) {
+      mpc_request_t up = r, down = r;
+      const double lo = std::max(b.center - b.bump, parameter_floor(b.greek));
+      b.set(up, b.center + b.bump);
+      b.set(down, lo);
+      mpc_result_t ru, rd;
+      price(up, &ru, Out{});
+      price(down, &rd, Out{});
+      const double eff = ((b.center + b.bump) - lo) * 0.5;
+      const double raw = eff > 0.0 ? (ru.price - rd.price) / (2.0 * eff) : 0.0;
+      mpc_greek_estimate_t& e = out->estimates[out->n_estimates++];
+      e.greek = b.greek;
+      e.estimator = estimator;
+      e.value = b.reverse ? -raw : raw;
+      e.stderr = eff > 0.0 ? std::sqrt(ru.stderr * ru.stderr + rd.stderr * rd.stderr) / (2.0 * eff) : 0.0;
+      e.bump_size = eff;
+      e.base_price = base.price;
+      e.bumped_up_price = ru.price;
+      e.bumped_down_price = rd.price;
+    }
+    return 0;
+  }
+  const bool terminal_gbm_call = r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.model == MPC_MODEL_GBM;
+  if (!terminal_gbm_call) {
+    out->warnings |= MPC_GREEK_WARN_ESTIMATOR_UNSUPPORTED;
+    return 0;
+  }
+  if (r.n_paths == 0 || !(r.s0 > 0.0) || !(r.sigma > 0.0) || !(r.t > 0.0)) return MPC_E_INVALID_CONFIG;
+  GreekMoments m[4];
+  single_pass(r, estimator, m);
+  const int greeks_pw[4] = {MPC_GREEK_DELTA, MPC_GREEK_VEGA, MPC_GREEK_RHO, MPC_GREEK_THETA};
+  const int count = estimator == MPC_GREEKS_PATHWISE ? 4 : 3;
+  for (int g = 0; g < count; ++g) {
+    mpc_greek_estimate_t& e = out->estimates[out->n_estimates++];
+    e.greek = greeks_pw[g];
+    e.estimator = estimator;
+    m[g].mean_stderr(&e.value, &e.stderr);
+    e.base_price = base.price;
+  }
+  if (r.sampling != MPC_SAMPLING_PSEUDORANDOM) out->warnings |= MPC_GREEK_WARN_PSEUDORANDOM_SHOCKS;
+  if (r.technique != MPC_TECHNIQUE_STANDARD) out->warnings |= MPC_GREEK_WARN_TECHNIQUE_IGNORED;
+  return 0;
+}
+
 }  // namespace orc
 
 // ====================================================== C entry points ====
@@ -1677,6 +1858,9 @@ void or_generate_uniforms(int sampling, uint64_t seed, uint64_t n_points, uint64
 }
 
 int or_price(const mpc_request_t* req, mpc_result_t* res) { return orc::price(*req, res, orc::Out{}); }
+int or_greeks(const mpc_request_t* req, int estimator, mpc_greek_report_t* out) {
+  return orc::greeks(*req, estimator, out);
+}
 int or_price_paths(const mpc_request_t* req, mpc_result_t* res, double* values, uint64_t capacity) {
   orc::Out out;
   out.values = values;

@@ -61,6 +61,7 @@ def lib() -> ctypes.CDLL:
         "or_generate_normals": (None, [c_int, c_uint64, c_uint64, c_uint64, POINTER(c_double)]),
         "or_generate_uniforms": (None, [c_int, c_uint64, c_uint64, c_uint64, POINTER(c_double)]),
         "or_price": (c_int, [POINTER(abi.Request), POINTER(abi.Result)]),
+        "or_greeks": (c_int, [POINTER(abi.Request), c_int, POINTER(abi.GreekReport)]),
         "or_price_paths": (c_int, [POINTER(abi.Request), POINTER(abi.Result), POINTER(c_double), c_uint64]),
         "or_price_from_f32_normals": (
             None,
@@ -120,6 +121,13 @@ def price(req: abi.Request) -> abi.Result:
     res = abi.Result()
     lib().or_price(ctypes.byref(req), ctypes.byref(res))
     return res
+
+
+def greeks(req: abi.Request, estimator: int) -> tuple[int, abi.GreekReport]:
+    """Greek report of the CPU restatement (cpu.rs:4036-5010): (status, report)."""
+    rep = abi.GreekReport()
+    status = lib().or_greeks(ctypes.byref(req), int(estimator), ctypes.byref(rep))
+    return status, rep
 
 
 def price_paths(req: abi.Request, capacity: int | None = None) -> tuple[abi.Result, np.ndarray]:

@@ -244,6 +244,78 @@ def test_lsm_batch_equals_individual(backend):
         assert got.regression_steps == one.regression_steps
 
 
+# ------------------------------------------------------------------ Greeks --
+def _estimates(rep):
+    return {rep.estimates[i].greek: rep.estimates[i] for i in range(rep.n_estimates)}
+
+
+@pytest.mark.parametrize("workload,kw", [
+    ("european_call", {}),
+    ("european_call", {"method": "stepwise", "n_steps": 32}),
+    ("arithmetic_asian_call", {"n_steps": 24}),
+    ("down_and_out_call", {"n_steps": 24, "barrier": 85.0}),
+    ("lookback_call", {"n_steps": 24}),
+    ("basket_call", {}),
+    ("european_call", {"model": "heston", "n_steps": 16}),
+])
+def test_bump_greeks_fp64_match_oracle(backend, workload, kw):
+    """Bump-and-revalue (cpu.rs:4938-4983): every leg is an FP64-plain repricing
+    (prices 1e-10 relative), so each central difference matches to 1e-7."""
+
+    r = req(workload, n_paths=8000, seed=21, precision="fp64_plain", **kw)
+    got = backend.greeks(r, "bump_and_revalue")
+    status, ref = O.greeks(r, abi.GREEKS_BUMP_AND_REVALUE)
+    assert status == 0 and got.n_estimates == ref.n_estimates > 0
+    assert abs(got.base_price - ref.base_price) <= 1e-10 * abs(ref.base_price)
+    for greek, e in _estimates(ref).items():
+        g = _estimates(got)[greek]
+        assert abs(g.bump_size - e.bump_size) <= 1e-15 * abs(e.bump_size)
+        assert abs(g.value - e.value) <= 1e-7 * abs(e.value) + 1e-9, (greek, g.value, e.value)
+        assert abs(g.stderr - e.stderr) <= 1e-7 * e.stderr + 1e-12
+
+
+@pytest.mark.parametrize("estimator", ["pathwise", "likelihood_ratio"])
+def test_single_pass_greeks_fp64_replay_reference_stream(backend, estimator):
+    """european_call_pathwise / likelihood_ratio (cpu.rs:4670-4869): the
+    terminal shocks are normal i of MonteCarloRng(seed), replayed on the device."""
+
+    r = req("european_call", n_paths=50_000, seed=17, precision="fp64_plain")
+    got = backend.greeks(r, estimator)
+    status, ref = O.greeks(r, abi.GREEK_ESTIMATORS[estimator])
+    assert status == 0 and got.n_estimates == ref.n_estimates
+    for greek, e in _estimates(ref).items():
+        g = _estimates(got)[greek]
+        assert abs(g.value - e.value) <= 1e-10 * abs(e.value), (greek, g.value, e.value)
+        assert abs(g.stderr - e.stderr) <= 1e-8 * e.stderr
+
+
+def test_greeks_fp32_within_stderr(backend):
+    bs = O.bs_greeks(100.0, 100.0, 0.03, 0.2, 1.0, exact=True)
+    r = req("european_call", n_paths=1 << 18, seed=5)  # FP32 path, pseudorandom
+    for estimator in ("pathwise", "likelihood_ratio", "bump_and_revalue"):
+        rep = backend.greeks(r, estimator)
+        for greek, key in ((abi.GREEK_DELTA, "delta"), (abi.GREEK_VEGA, "vega"), (abi.GREEK_RHO, "rho")):
+            e = _estimates(rep)[greek]
+            assert abs(e.value - bs[key]) < 4 * e.stderr + 2e-3 * abs(bs[key]), (estimator, key, e.value, bs[key])
+    h = req("european_call", model="heston", n_paths=1 << 16, n_steps=64, seed=3, sampling="scrambled_sobol")
+    got = backend.greeks(h, "bump_and_revalue")
+    h64 = req("european_call", model="heston", n_paths=1 << 16, n_steps=64, seed=3, sampling="scrambled_sobol",
+              precision="fp64_plain")
+    ref = backend.greeks(h64, "bump_and_revalue")
+    for greek, e in _estimates(ref).items():
+        assert abs(_estimates(got)[greek].value - e.value) < 0.5 * e.stderr, greek
+
+
+def test_greeks_unsupported_cases(backend):
+    from montepath_b200.backend import BackendError
+
+    with pytest.raises(BackendError) as err:
+        backend.greeks(req("european_call", model="merton", n_paths=1000, sampling="counter_hash"))
+    assert err.value.status == abi.E_UNSUPPORTED
+    rep = backend.greeks(req("arithmetic_asian_call", n_paths=2000, n_steps=8), "pathwise")
+    assert rep.n_estimates == 0 and rep.warnings & abi.GREEK_WARN_ESTIMATOR_UNSUPPORTED and rep.base_price > 0
+
+
 # -------------------------------------------------------------------- MLMC --
 def test_mlmc_fp64_plain_matches_oracle(backend):
     r = make_request("arithmetic_asian_mlmc", {"paths_per_level": [4000, 2000, 1000, 500], "seed": 3,

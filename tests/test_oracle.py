@@ -292,3 +292,55 @@ def test_same_normals_fp32_functions():
     z = O.stateless_normals_f32(42, 512, 16)
     res, per = O.price_from_f32_normals(req, z)
     assert np.all(per >= 0) and res.price > 0
+
+
+# ----------------------------------------------------------------- Greeks --
+# european_call_greeks_cpu and siblings (cpu.rs:4036-5010), pinned against the
+# Black-Scholes Greeks fixture (reference-fixtures.json:31-58).
+@pytest.mark.parametrize("estimator", [abi.GREEKS_BUMP_AND_REVALUE, abi.GREEKS_PATHWISE, abi.GREEKS_LIKELIHOOD_RATIO])
+def test_european_greeks_against_black_scholes_fixture(estimator):
+    exp = fixture("black_scholes_european_call_greeks_atm_1y")["expected"]
+    bs = dict(exp, theta=exp["theta_calendar_convention"])
+    req = make_request("european_call", n_paths=200_000, seed=17, precision="fp64_plain")
+    status, rep = O.greeks(req, estimator)
+    assert status == 0 and rep.warnings == 0
+    names = {rep.estimates[i].greek: rep.estimates[i] for i in range(rep.n_estimates)}
+    expect = [abi.GREEK_DELTA, abi.GREEK_VEGA, abi.GREEK_RHO] + ([] if estimator == 2 else [abi.GREEK_THETA])
+    assert sorted(names) == sorted(expect)
+    for greek, key in ((abi.GREEK_DELTA, "delta"), (abi.GREEK_VEGA, "vega"), (abi.GREEK_RHO, "rho"),
+                       (abi.GREEK_THETA, "theta")):
+        if greek in names:
+            e = names[greek]
+            assert abs(e.value - bs[key]) < 4 * e.stderr + 1e-3 * abs(bs[key]), (key, e.value, bs[key], e.stderr)
+    assert abs(rep.base_price - 9.413403383853016) < 4 * rep.base_stderr
+
+
+def test_bump_recipe_matches_repricing():
+    """push_bump_estimate (cpu.rs:4938-4983): central difference of two
+    common-seed repricings, theta sign reversed, floors applied."""
+
+    req = make_request("arithmetic_asian_call", n_paths=20_000, n_steps=24, seed=9, precision="fp64_plain")
+    status, rep = O.greeks(req, abi.GREEKS_BUMP_AND_REVALUE)
+    assert status == 0 and rep.n_estimates == 4
+    up, down = abi.Request.from_buffer_copy(req), abi.Request.from_buffer_copy(req)
+    up.sigma, down.sigma = 0.2 + 0.01, 0.2 - 0.01
+    vega = rep.estimates[1]
+    assert vega.greek == abi.GREEK_VEGA and abs(vega.bump_size - 0.01) < 1e-15
+    assert vega.value == (O.price(up).price - O.price(down).price) / (2 * (((0.2 + 0.01) - (0.2 - 0.01)) * 0.5))
+    theta = rep.estimates[3]
+    h = 1.0 / 365.0
+    tu, td = abi.Request.from_buffer_copy(req), abi.Request.from_buffer_copy(req)
+    tu.t, td.t = 1.0 + h, 1.0 - h
+    assert theta.value == -(O.price(tu).price - O.price(td).price) / (2 * (((1.0 + h) - (1.0 - h)) * 0.5))
+
+
+def test_greek_reports_of_other_workloads():
+    basket = make_request("basket_call", n_paths=20_000, seed=3, precision="fp64_plain")
+    status, rep = O.greeks(basket, abi.GREEKS_BUMP_AND_REVALUE)
+    assert status == 0 and rep.steps == 2
+    assert [rep.estimates[i].greek for i in range(rep.n_estimates)] == [0, 1, 2, 3, 4, 5]
+    heston = make_request("european_call", model="heston", n_paths=5_000, n_steps=16, seed=3, precision="fp64_plain")
+    status, rep = O.greeks(heston, abi.GREEKS_PATHWISE)
+    assert status == 0 and rep.n_estimates == 0 and rep.warnings & abi.GREEK_WARN_ESTIMATOR_UNSUPPORTED
+    merton = make_request("european_call", model="merton", n_paths=1_000, seed=3, precision="fp64_plain")
+    assert O.greeks(merton, abi.GREEKS_BUMP_AND_REVALUE)[0] == abi.E_UNSUPPORTED
