@@ -401,12 +401,76 @@ __device__ __forceinline__ uint32_t poisson_tail(double u, double mean, double p
   return k;
 }
 
+// ------------------------------------------------------- Brownian bridge ---
+// fill_step_normals_from_inputs (cpu.rs:5964-5981) as a streaming walk: the
+// reference fills w[0..n] op by op and then differences it; here the same
+// ops run in the same (depth-first) order, but only the right endpoints still
+// needed stay on a small stack, and each leaf yields the next step's
+// increment (w[s] - w[s-1]) / sqrt(dt) at once.  Input dimensions are drawn in
+// increasing order (0 = W(T), then one per op), every thread of a request
+// runs the same event sequence, so block-synchronous sources stay in lockstep.
+// FP64 keeps the reference's two-rounding products and left-to-right sums.
+template <class Real>
+struct BridgeWalk {
+  Real stack[kBridgeDepth];
+  Real w_left;
+  uint32_t sp, ev, op, dim;
+
+  __device__ __forceinline__ static Real mid(Real lw, Real wl, Real rw, Real wr, Real sd, Real z) {
+    if constexpr (sizeof(Real) == 8)
+      return __dadd_rn(__dadd_rn(__dmul_rn(lw, wl), __dmul_rn(rw, wr)), __dmul_rn(sd, z));
+    else
+      return lw * wl + rw * wr + sd * z;
+  }
+  template <class Src>
+  __device__ __forceinline__ void begin(const DevReq& q, Src& src) {
+    src.at_step(0, 1);
+    const Real z0 = normal<Real>(src, 0);
+    if constexpr (sizeof(Real) == 8)
+      stack[0] = __dmul_rn(q.bridge_sqrt_t, z0);
+    else
+      stack[0] = (Real)q.bridge_sqrt_t * z0;
+    sp = 1;
+    w_left = (Real)0;
+    ev = 0;
+    op = 0;
+    dim = 1;
+  }
+  // The increment of the next step (the host checked the program: it ends
+  // every op run with a leaf and never needs more than kBridgeDepth values).
+  template <class Src>
+  __device__ __forceinline__ Real next(const DevReq& q, Src& src) {
+    for (;;) {
+      const uint32_t is_op = (__ldg(q.bridge_events + (ev >> 5)) >> (ev & 31)) & 1u;
+      ++ev;
+      if (!is_op) break;
+      const double* o = q.bridge_ops + 3 * op;
+      ++op;
+      src.at_step(dim, 1);
+      const Real z = normal<Real>(src, dim);
+      ++dim;
+      const Real wr = stack[sp - 1];
+      stack[sp] = mid((Real)__ldg(o), w_left, (Real)__ldg(o + 1), wr, (Real)__ldg(o + 2), z);
+      ++sp;
+    }
+    --sp;
+    const Real wr = stack[sp];
+    Real inc;
+    if constexpr (sizeof(Real) == 8)
+      inc = __dmul_rn(__dsub_rn(wr, w_left), q.bridge_inv_sqrt_dt);
+    else
+      inc = (wr - w_left) * (Real)q.bridge_inv_sqrt_dt;
+    w_left = wr;
+    return inc;
+  }
+};
+
 // ------------------------------------------------------------- models -----
 // GBM stepwise with the payoff observer of workload W (cpu.rs:6443-6591,
 // 7973-8009, 8324-8354; up-and-out mirrors down-and-out).  FP32 compares the
 // barrier in log space; FP64 compares exp(log S) with the barrier as the
 // reference does.
-template <class Real, int W, class Src>
+template <class Real, int W, class Src, bool BRIDGE = false>
 __device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double& pay, double& ctl) {
   const Real drift = (Real)q.drift_dt, vol = (Real)q.vol_dt, kk = (Real)q.k, disc = (Real)q.discount;
   const Real lbar = (Real)q.log_barrier, bar = (Real)q.barrier;
@@ -443,7 +507,11 @@ __device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double&
     }
   };
   uint32_t s = 0;
-  if constexpr (kQuadSource<Src>) {
+  if constexpr (BRIDGE) {  // increments from the Brownian bridge over the inputs
+    BridgeWalk<Real> bw;
+    bw.begin(q, src);
+    for (; s < n; ++s) advance(bw.next(q, src));
+  } else if constexpr (kQuadSource<Src>) {
     for (; s + 4 <= n; s += 4) {  // four steps per quad of dimensions
       src.at_step(s, 4);
       src.quad_load(s);
@@ -719,7 +787,25 @@ __device__ __forceinline__ void unit_mlmc(const DevReq& q, Src& src, double& pay
 
 template <class Real, int FAM, class Src>
 __device__ __forceinline__ void run_family(const DevReq& q, Src& src, double& p, double& c) {
-  if constexpr (FAM == FAM_GBM_STEP) {
+  if constexpr (FAM == FAM_GBM_BRIDGE) {
+    switch (q.workload) {
+      case W_ASIAN:
+        unit_gbm_step<Real, W_ASIAN, Src, true>(q, src, p, c);
+        break;
+      case W_DAO:
+        unit_gbm_step<Real, W_DAO, Src, true>(q, src, p, c);
+        break;
+      case W_UAO:
+        unit_gbm_step<Real, W_UAO, Src, true>(q, src, p, c);
+        break;
+      case W_LOOKBACK:
+        unit_gbm_step<Real, W_LOOKBACK, Src, true>(q, src, p, c);
+        break;
+      default:
+        unit_gbm_step<Real, W_EURO, Src, true>(q, src, p, c);
+        break;
+    }
+  } else if constexpr (FAM == FAM_GBM_STEP) {
     switch (q.workload) {
       case W_ASIAN:
         unit_gbm_step<Real, W_ASIAN>(q, src, p, c);
@@ -777,6 +863,12 @@ __device__ __forceinline__ void fused_unit_any(const DevReq& q, const SrcCtx& ct
       break;
     case FAM_MLMC_LEVEL:
       fused_unit<FAM_MLMC_LEVEL, SMP>(q, ctx, u, p, c);
+      break;
+    case FAM_GBM_BRIDGE:
+      if constexpr (SMP == SMP_SOBOL)
+        fused_unit<FAM_GBM_BRIDGE, SMP>(q, ctx, u, p, c);
+      else
+        p = c = 0.0;
       break;
     default:
       if constexpr (SMP != SMP_XORSHIFT) {
@@ -956,6 +1048,10 @@ static cudaError_t launch_fused_s(int family, const DevReq* reqs, const Tile* ti
       return launch_fused_t<FAM_BASKET, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
     case FAM_MLMC_LEVEL:
       return launch_fused_t<FAM_MLMC_LEVEL, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+    case FAM_GBM_BRIDGE:
+      if constexpr (SMP == SMP_SOBOL)
+        return launch_fused_t<FAM_GBM_BRIDGE, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
+      return cudaErrorInvalidValue;
     case FAM_MERTON_STEP:
       if constexpr (SMP != SMP_XORSHIFT)
         return launch_fused_t<FAM_MERTON_STEP, SMP>(reqs, tiles, n_tiles, counter, ctx, grid, block, stream);
@@ -1009,6 +1105,9 @@ static int occ_s(int family, int block) {
       return occ_t<FAM_BASKET, SMP>(block);
     case FAM_MLMC_LEVEL:
       return occ_t<FAM_MLMC_LEVEL, SMP>(block);
+    case FAM_GBM_BRIDGE:
+      if constexpr (SMP == SMP_SOBOL) return occ_t<FAM_GBM_BRIDGE, SMP>(block);
+      return 1;
     case FAM_MERTON_STEP:
       if constexpr (SMP != SMP_XORSHIFT) return occ_t<FAM_MERTON_STEP, SMP>(block);
       return 1;
@@ -1124,6 +1223,9 @@ cudaError_t launch_plain_simulate(const DevReq& q, const DevReq* d_req, const do
       break;
     case FAM_BASKET:
       plain_simulate_kernel<FAM_BASKET><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
+      break;
+    case FAM_GBM_BRIDGE:
+      plain_simulate_kernel<FAM_GBM_BRIDGE><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);
       break;
     default:
       plain_simulate_kernel<FAM_MLMC_LEVEL><<<grid, 256, 0, stream>>>(d_req, d_buf, d_payoff, d_control);

@@ -127,6 +127,8 @@ extern "C" int mpc_price_fused_noalloc(const mpc_request_t* req, mpc_result_t* o
   if (p.sampler != mpc::SMP_XORSHIFT && p.sampler != mpc::SMP_COUNTER && p.sampler != mpc::SMP_SOBOL)
     return reject(MPC_E_UNSUPPORTED,
                   "the no-allocation entry point supports pseudorandom, counter_hash and scrambled_sobol sampling");
+  if (p.q.bridge)  // the bridge program lives in a per-request device table
+    return reject(MPC_E_UNSUPPORTED, "the no-allocation entry point does not run Brownian-bridge paths");
   if (p.q.n_units > kNoAllocMaxUnits)
     return reject(MPC_E_OOM_BUDGET, "request has " + std::to_string(p.q.n_units) +
                                         " paths (or antithetic pairs); the no-allocation scratch holds at most " +

@@ -193,8 +193,8 @@ int validate(const mpc_request_t& r, std::string* msg) {
   if (r.n_paths > (1ull << 32)) return unsupported(msg, "n_paths above 2^32 is not supported");
   if (r.n_steps == 0) return invalid(msg, "n_steps must be > 0");
   if (!(r.t > 0.0)) return invalid(msg, "t must be > 0");
-  if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE)
-    return unsupported(msg, "Brownian-bridge Sobol sampling runs on the CPU reference only");
+  if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE && r.n_steps > kBridgeMaxSteps)
+    return unsupported(msg, "Brownian-bridge sampling supports at most 65,536 steps");
   if (is_lsm(r.workload)) {
     if (r.n_steps < 2) return invalid(msg, "n_steps must be >= 2 for LSM regression");
     if (r.n_steps > 511) return unsupported(msg, "LSM supports at most 511 steps");
@@ -306,6 +306,43 @@ static int sampler_of(int sampling) {
     default:
       return SMP_SOBOL;
   }
+}
+
+// BrownianBridgePlan::new (cpu.rs:5923-5962) flattened into the event
+// program the device walks: the reference's interval stack is replayed and
+// every pop becomes an event -- an op (midpoint of an interval longer than
+// one step, consuming the next input dimension) or a leaf (one step).  Ops
+// carry the reference's weights and stddev, computed the same way.  Returns
+// false if the walk would need a deeper stack than the device holds.
+static bool build_bridge_program(Prepared* p, uint32_t n, double maturity) {
+  const double dt = maturity / double(n);
+  p->bridge_ops.clear();
+  p->bridge_events.assign((2ull * n - 1 + 31) / 32, 0u);
+  std::vector<std::pair<uint32_t, uint32_t>> intervals{{0u, n}};
+  uint32_t event = 0, depth = 1, max_depth = 1;  // depth: values on the device stack (starts with W(T))
+  while (!intervals.empty()) {
+    const auto [left, right] = intervals.back();
+    intervals.pop_back();
+    if (right <= left + 1) {  // leaf: pops one value
+      ++event;
+      --depth;
+      continue;
+    }
+    const uint32_t mid = (left + right) / 2;
+    const double t_left = double(left) * dt, t_mid = double(mid) * dt, t_right = double(right) * dt;
+    const double denom = t_right - t_left;
+    p->bridge_ops.push_back((t_right - t_mid) / denom);
+    p->bridge_ops.push_back((t_mid - t_left) / denom);
+    p->bridge_ops.push_back(std::sqrt((t_mid - t_left) * (t_right - t_mid) / denom));
+    p->bridge_events[event >> 5] |= 1u << (event & 31);
+    ++event;
+    max_depth = std::max(max_depth, ++depth);  // op: pushes the midpoint
+    intervals.push_back({mid, right});
+    intervals.push_back({left, mid});
+  }
+  p->q.bridge_sqrt_t = std::sqrt(maturity);
+  p->q.bridge_inv_sqrt_dt = 1.0 / std::sqrt(dt);
+  return event == 2 * n - 1 && depth == 0 && max_depth <= kBridgeDepth && p->bridge_ops.size() == 3ull * (n - 1);
 }
 
 static std::vector<uint32_t> first_primes(size_t n) {
@@ -466,6 +503,16 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
     // simulate_stepwise_antithetic (European) is single-stream (cpu.rs:7807-7835)
     if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && q.anti) chunkable = false;
     p->path_steps = r.n_paths * r.n_steps;
+    // the bridge applies to the stepwise GBM workloads (cpu.rs:7113-7501); the
+    // other families read bridge Sobol as plain Sobol, as the reference does
+    if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE) {
+      if (!build_bridge_program(p, r.n_steps, r.t)) {
+        if (msg) *msg = "Brownian-bridge program exceeds the device stack";
+        return MPC_E_UNSUPPORTED;
+      }
+      q.bridge = 1;
+      q.family = FAM_GBM_BRIDGE;
+    }
   }
   p->family = q.family;
   p->cv_expectation = q.cv_expectation;
@@ -547,8 +594,11 @@ static int upload_aux(mpc_context* ctx, std::vector<Prepared*>& reqs) {
     bytes += p->halton_primes.size() * 4 + 16;
     bytes += p->halton_shifts.size() * 8 + 16;
     bytes += p->lhs.size() * sizeof(LhsDim) + 16;
+    bytes += p->bridge_ops.size() * 8 + p->bridge_events.size() * 4 + 32;
   }
-  if (bytes <= 48 * reqs.size()) return MPC_OK;
+  bool any = false;  // per-request tables to place
+  for (Prepared* p : reqs) any = any || !p->halton_primes.empty() || !p->lhs.empty() || p->q.bridge;
+  if (!any) return MPC_OK;
   void* d_aux = nullptr;
   int st = scratch(ctx, "aux", bytes, &d_aux);
   if (st != MPC_OK) return st;
@@ -567,6 +617,12 @@ static int upload_aux(mpc_context* ctx, std::vector<Prepared*>& reqs) {
       p->q.halton_shifts = static_cast<const double*>(place(p->halton_shifts.data(), p->halton_shifts.size() * 8));
     }
     if (!p->lhs.empty()) p->q.lhs = static_cast<const LhsDim*>(place(p->lhs.data(), p->lhs.size() * sizeof(LhsDim)));
+    if (p->q.bridge) {  // a one-step program has a leaf event and no op
+      if (!p->bridge_ops.empty())
+        p->q.bridge_ops = static_cast<const double*>(place(p->bridge_ops.data(), p->bridge_ops.size() * 8));
+      p->q.bridge_events =
+          static_cast<const uint32_t*>(place(p->bridge_events.data(), p->bridge_events.size() * 4));
+    }
   }
   MPC_CUDA(ctx, cudaMemcpyAsync(d_aux, host.data(), off, cudaMemcpyHostToDevice, ctx->stream));
   MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

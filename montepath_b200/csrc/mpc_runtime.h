@@ -40,6 +40,8 @@ struct Prepared {
   std::vector<uint32_t> halton_primes;
   std::vector<double> halton_shifts;
   std::vector<LhsDim> lhs;
+  std::vector<double> bridge_ops;
+  std::vector<uint32_t> bridge_events;
   uint64_t path_steps = 0;
 };
 

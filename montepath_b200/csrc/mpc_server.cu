@@ -421,8 +421,8 @@ int mpc_submit(mpc_server_t* s, const mpc_request_t* req, uint64_t* ticket) {
       req->workload != MPC_WORKLOAD_BERMUDAN_PUT) {
     st = prepare(s->ctx, *req, &t.prep, &msg);
     if (st == MPC_OK && !t.prep.plain && s->opt.mode == 0) {
-      if (!t.prep.halton_primes.empty() || !t.prep.lhs.empty())
-        t.prep.plain = true;  // structured-table samplers run as their own launch
+      if (!t.prep.halton_primes.empty() || !t.prep.lhs.empty() || t.prep.q.bridge)
+        t.prep.plain = true;  // samplers with per-request tables run as their own launch
       else {
         Shape sh = choose_shape(s->ctx, t.prep);
         t.prep.q.tile_units = sh.block * sh.ppt;

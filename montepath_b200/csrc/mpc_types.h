@@ -19,6 +19,12 @@
 
 namespace mpc {
 
+// Brownian bridge: the device walks the bisection tree with a stack of at
+// most kBridgeDepth values, which holds every program of up to
+// kBridgeMaxSteps steps (tree depth 16 plus W(T)).
+constexpr uint32_t kBridgeDepth = 20;
+constexpr uint32_t kBridgeMaxSteps = 65536;
+
 // Kernel families: the model-specific loop a tile runs.
 enum Family : int32_t {
   FAM_GBM_STEP = 0,
@@ -28,6 +34,7 @@ enum Family : int32_t {
   FAM_MERTON_TERMINAL = 4,
   FAM_BASKET = 5,
   FAM_MLMC_LEVEL = 6,
+  FAM_GBM_BRIDGE = 7,  // GBM stepwise driven through the Brownian bridge (bridge Sobol)
   FAM_COUNT = 7
 };
 
@@ -72,6 +79,15 @@ struct alignas(16) DevReq {
   uint32_t level, refinement;
   uint64_t coarse_steps;
   double f_drift, f_vol, c_drift, c_vol, inv_sqrt_m, inv_fine, inv_coarse;
+  // Brownian-bridge path construction (GBM stepwise with bridge Sobol): a
+  // program of 2 n_steps - 1 events in the reference's depth-first order;
+  // event e is an op (a midpoint, weights and stddev in bridge_ops) when bit
+  // e of bridge_events is set, else a leaf (one step increment).
+  const double* bridge_ops;       // [n_steps - 1][3]: left weight, right weight, stddev
+  const uint32_t* bridge_events;  // [(2 n_steps - 1 + 31) / 32]
+  double bridge_sqrt_t, bridge_inv_sqrt_dt;
+  uint32_t bridge;                // 1: normals come through the bridge
+  uint32_t _pad_b;
   // samplers
   const uint32_t* halton_primes;
   const double* halton_shifts;

@@ -83,7 +83,9 @@ def validate(r):
         ("european_call", dict(model="heston", vol_of_vol=-0.1), abi.E_INVALID_CONFIG),
         ("european_call", dict(model="merton", sampling="pseudorandom"), abi.E_UNSUPPORTED),
         ("european_call", dict(model="merton", sampling="scrambled_sobol", technique="antithetic"), abi.E_UNSUPPORTED),
-        ("european_call", dict(sampling="scrambled_sobol_brownian_bridge"), abi.E_UNSUPPORTED),
+        ("european_call", dict(method="stepwise", n_steps=70_000, sampling="scrambled_sobol_brownian_bridge"),
+         abi.E_UNSUPPORTED),
+        ("arithmetic_asian_mlmc", dict(sampling="scrambled_sobol_brownian_bridge"), abi.E_UNSUPPORTED),
         ("down_and_out_call", dict(barrier=0.0), abi.E_INVALID_CONFIG),
         ("american_put", dict(n_steps=1), abi.E_INVALID_CONFIG),
         ("american_put", dict(sampling="scrambled_sobol"), abi.E_UNSUPPORTED),

@@ -244,6 +244,51 @@ def test_lsm_batch_equals_individual(backend):
         assert got.regression_steps == one.regression_steps
 
 
+# --------------------------------------------------------- Brownian bridge --
+@pytest.mark.parametrize("workload,steps,technique", [
+    ("european_call", 64, "standard"),
+    ("european_call", 37, "antithetic"),
+    ("arithmetic_asian_call", 50, "control_variate"),
+    ("down_and_out_call", 33, "standard"),
+    ("lookback_call", 1, "standard"),
+    ("arithmetic_asian_call", 365, "standard"),
+])
+def test_bridge_fp64_per_path_matches_oracle(backend, workload, steps, technique):
+    """BrownianBridgePlan (cpu.rs:5886-5981): the device walks the same op
+    program depth-first; FP64 per-path payoffs within 1e-10 of the oracle."""
+
+    kw = {"method": "stepwise"} if workload == "european_call" else {}
+    r = req(workload, n_paths=3000, n_steps=steps, seed=13, sampling="scrambled_sobol_brownian_bridge",
+            technique=technique, precision="fp64_plain", barrier=85.0, **kw)
+    _, ref = O.price_paths(r)
+    got = backend.price_paths(r)
+    assert np.allclose(got, ref, rtol=1e-10, atol=1e-10), float(np.max(np.abs(got - ref)))
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) <= 1e-10 * abs(b.price)
+
+
+def test_bridge_fp32_fused_matches_oracle(backend):
+    r = req("arithmetic_asian_call", n_paths=8192, n_steps=96, seed=7, sampling="scrambled_sobol_brownian_bridge")
+    _, ref = O.price_paths(r)
+    got = backend.price_paths(r)
+    assert np.allclose(got, ref, rtol=2e-4, atol=1e-3)
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) < 0.05 * b.stderr
+    # in a mixed batch the bridge request keeps its own launch and its result
+    plain_sobol = req("arithmetic_asian_call", n_paths=8192, n_steps=96, seed=7, sampling="scrambled_sobol")
+    both = backend.price_batch([r, plain_sobol])
+    assert both[0].price == a.price and both[1].price == backend.price(plain_sobol).price
+
+
+def test_bridge_sampling_reads_as_sobol_outside_gbm_steps(backend):
+    """Non-stepwise families take bridge Sobol as plain Sobol, as the reference does."""
+
+    kw = dict(model="heston", n_paths=4096, n_steps=16, seed=3, precision="fp64_plain")
+    a = backend.price(req("european_call", sampling="scrambled_sobol_brownian_bridge", **kw))
+    b = backend.price(req("european_call", sampling="scrambled_sobol", **kw))
+    assert a.price == b.price
+
+
 # ------------------------------------------------------------------ Greeks --
 def _estimates(rep):
     return {rep.estimates[i].greek: rep.estimates[i] for i in range(rep.n_estimates)}
