@@ -222,3 +222,35 @@ def test_reference_pricing_surface_accepts_module(monkeypatch):
     heston = montepath.price_heston_european_call(native_module="montepath_b200.native", n_paths=2000, n_steps=8)
     assert heston.price > 0
     assert "montepath_b200.native" in sys.modules
+
+
+def test_mc_bench_rows_have_the_harness_shape(monkeypatch):
+    """mc_cuda_* rows carry the fields of BenchmarkResult (crates/mc-bench/src/result.rs:3-17);
+    the device calls are replaced by the oracle on the host, at a small size."""
+
+    from montepath_b200 import mc_bench
+    from oracle import oracle as O
+
+    class OracleBackend:
+        def price(self, req):
+            return O.price(req)
+
+        def price_batch(self, reqs):
+            return [O.price(r) for r in reqs]
+
+        def greeks(self, req):
+            return O.greeks(req, abi.GREEKS_BUMP_AND_REVALUE)[1]
+
+    monkeypatch.setattr(mc_bench, "MC_PATHS", 600)
+    monkeypatch.setattr(mc_bench, "MC_STEPS", 8)
+    monkeypatch.setattr(mc_bench, "GREEK_PATHS", 600)
+    report = mc_bench.run(OracleBackend(), compact=False, precision="fp64_plain", repeats=2)
+    fields = {"benchmark_name", "benchmark_version", "implementation", "backend", "methodology", "planner_mode",
+              "iterations", "total_runtime_ms", "per_iteration_us", "throughput_per_sec", "metric_name",
+              "metric_value"}
+    assert set(report) == {"generated_at_unix_ms", "results"}
+    names = [r["benchmark_name"] for r in report["results"]]
+    assert len(names) == len(set(names)) and all(n.startswith("mc_cuda_") and n.endswith("_fp64_plain") for n in names)
+    for row in report["results"]:
+        assert set(row) == fields and row["backend"] == "nvidia_cuda" and row["iterations"] == 2
+        assert row["throughput_per_sec"] > 0 and row["metric_value"] > 0

@@ -462,3 +462,16 @@ def test_reference_v1_kernel_contract(backend):
     assert status == abi.OK
     ref = np.maximum(np.exp(math.log(100.0) + np.cumsum(drift + vol * z.reshape(n_paths, n_steps), axis=1)[:, -1]) - 100.0, 0) * disc
     assert np.allclose(payoffs.cpu().numpy(), ref, rtol=1e-12, atol=1e-12)
+
+
+# ---------------------------------------------------------- harness rows --
+def test_mc_bench_compact_rows(backend):
+    """mc_cuda_* rows (BenchmarkResult shape) from the real device, compact suite."""
+
+    from montepath_b200 import mc_bench
+
+    report = mc_bench.run(backend, compact=True, repeats=2)
+    rows = {r["benchmark_name"]: r for r in report["results"]}
+    assert set(rows) == mc_bench._COMPACT
+    assert abs(rows["mc_cuda_european_call_terminal"]["metric_value"] - 9.413403383853016) < 0.1
+    assert all(r["throughput_per_sec"] > 1e6 for r in rows.values())
