@@ -128,6 +128,101 @@ void mean_stderr(double sum, double sq, uint64_t count, double* mean, double* se
   *se = std::sqrt(var / n);
 }
 
+// Whether the legs of a bump report can share their normals in one
+// scenario launch: FP32 path, standard technique, a family the scenario
+// kernel runs, a sampler whose normals depend only on (point, dimension).
+bool scenario_eligible(const Prepared& p, const mpc_request_t& r, size_t legs) {
+  if (r.precision != MPC_PRECISION_FP32_PATH || r.technique != MPC_TECHNIQUE_STANDARD) return false;
+  if (legs > size_t(kMaxScen) || p.q.bridge) return false;
+  if (p.family != FAM_GBM_STEP && p.family != FAM_GBM_TERMINAL && p.family != FAM_HESTON) return false;
+  return p.sampler == SMP_XORSHIFT || p.sampler == SMP_SOBOL || p.sampler == SMP_COUNTER;
+}
+
+// Prices every leg (same seed, same dimensions) in one scenario launch.
+int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, std::vector<mpc_result_t>& res) {
+  std::vector<Prepared> preps(legs.size());
+  std::string msg;
+  for (size_t i = 0; i < legs.size(); ++i) {
+    const int st = prepare(ctx, legs[i], &preps[i], &msg);
+    if (st != MPC_OK) return fail(ctx, st, msg);
+  }
+  const Prepared& base = preps[0];
+  const int n_scen = int(legs.size());
+  float scen[kScenFields * kMaxScen];
+  for (int s = 0; s < kMaxScen; ++s) {
+    const DevReq& q = preps[s < n_scen ? s : 0].q;
+    float f[kScenFields];
+    if (base.family == FAM_HESTON) {
+      const float v[kScenFields] = {float(q.log_s0), float(q.v0), float(q.rate), float(q.dt), float(q.sqrt_dt),
+                                    float(q.discount)};
+      std::memcpy(f, v, sizeof(f));
+    } else {
+      const bool ko = (q.workload == MPC_WORKLOAD_DOWN_AND_OUT_CALL && q.s0 <= q.barrier) ||
+                      (q.workload == MPC_WORKLOAD_UP_AND_OUT_CALL && q.s0 >= q.barrier);
+      const float v[kScenFields] = {float(q.log_s0),   float(q.s0),       float(q.drift_dt),
+                                    float(q.vol_dt),   float(q.discount), ko ? 1.0f : 0.0f};
+      std::memcpy(f, v, sizeof(f));
+    }
+    for (int k = 0; k < kScenFields; ++k) scen[k * kMaxScen + s] = f[k];
+  }
+  DevReq q = base.q;
+  q.n_scen = uint32_t(n_scen);
+  q.tile_units = 256;
+  const uint64_t n_tiles = (q.n_units + q.tile_units - 1) / q.tile_units;
+  if (n_tiles > (1ull << 31)) return fail(ctx, MPC_E_UNSUPPORTED, "too many tiles for one scenario launch");
+  q.n_tiles = uint32_t(n_tiles);
+  // device layout: descriptor | leg parameters | partials | moments | counters (done, tile counter)
+  const size_t o_scen = 256 * ((sizeof(DevReq) + 255) / 256);
+  const size_t o_part = o_scen + 256;
+  const size_t o_mom = o_part + ((n_tiles * kMaxScen * 2 * sizeof(double) + 255) / 256) * 256;
+  const size_t o_cnt = o_mom + 256;
+  void* d = nullptr;
+  int st = scratch(ctx, "scenarios", o_cnt + 256, &d);
+  if (st != MPC_OK) return st;
+  uint8_t* base_ptr = static_cast<uint8_t*>(d);
+  q.scen = reinterpret_cast<const float*>(base_ptr + o_scen);
+  q.partials = reinterpret_cast<double*>(base_ptr + o_part);
+  q.moments = reinterpret_cast<double*>(base_ptr + o_mom);
+  q.tiles_done = reinterpret_cast<uint32_t*>(base_ptr + o_cnt);
+  q.per_unit = nullptr;
+  uint32_t* counter = q.tiles_done + 1;
+  double host_mom[kMaxScen * 2];
+  auto fin = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? MPC_OK : cuda_fail(ctx, e, what); };
+  if ((st = fin(cudaMemsetAsync(q.tiles_done, 0, 2 * sizeof(uint32_t), ctx->stream), "memset counters"))) return st;
+  if ((st = fin(cudaMemcpyAsync(base_ptr, &q, sizeof(q), cudaMemcpyHostToDevice, ctx->stream), "descriptor"))) return st;
+  if ((st = fin(cudaMemcpyAsync(base_ptr + o_scen, scen, sizeof(scen), cudaMemcpyHostToDevice, ctx->stream),
+                "leg parameters")))
+    return st;
+  const int occ = std::max(1, scenario_max_blocks_per_sm(base.family, base.sampler));
+  const int grid = int(std::min<uint64_t>(n_tiles, uint64_t(ctx->sm_count) * occ));
+  if ((st = fin(cudaEventRecord(ctx->ev_start, ctx->stream), "event"))) return st;
+  if ((st = fin(launch_scenarios(reinterpret_cast<const DevReq*>(base_ptr), q.n_tiles, counter, base.family,
+                                 base.sampler, ctx->tabs, grid, ctx->stream),
+                "scenario kernel")))
+    return st;
+  if ((st = fin(cudaEventRecord(ctx->ev_stop, ctx->stream), "event"))) return st;
+  if ((st = fin(cudaMemcpyAsync(host_mom, q.moments, sizeof(host_mom), cudaMemcpyDeviceToHost, ctx->stream),
+                "moments")))
+    return st;
+  if ((st = fin(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"))) return st;
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  ctx->last_ms = ms;
+  res.assign(legs.size(), mpc_result_t{});
+  const double n = double(q.n_units);
+  for (int s = 0; s < n_scen; ++s) {  // summarize_payoffs (cpu.rs:7641-7652)
+    const double mean = host_mom[2 * s] / n;
+    const double var = std::max(host_mom[2 * s + 1] / n - mean * mean, 0.0);
+    res[s].price = mean;
+    res[s].stderr = std::sqrt(var) / std::sqrt(n);
+    res[s].n_samples = q.n_units;
+    res[s].path_steps = preps[s].path_steps;
+    res[s].runtime_ms = ms;
+    res[s].status = MPC_OK;
+  }
+  return MPC_OK;
+}
+
 }  // namespace
 }  // namespace mpc
 
@@ -169,7 +264,14 @@ extern "C" int mpc_greeks(mpc_context_t* ctx, const mpc_request_t* req, int esti
       set_param(reqs[2 + 2 * i], b.param, std::max(b.center - b.bump, parameter_floor(b.greek)));
     }
     std::vector<mpc_result_t> res(reqs.size());
-    const int st = mpc_price_batch(ctx, reqs.data(), reqs.size(), res.data());
+    Prepared base_prep;
+    std::string msg;
+    int st = prepare(ctx, r, &base_prep, &msg);
+    if (st != MPC_OK) return finish(fail(ctx, st, msg));
+    if (scenario_eligible(base_prep, r, reqs.size()))  // all legs share each normal: one launch
+      st = run_scenario_legs(ctx, reqs, res);
+    else
+      st = mpc_price_batch(ctx, reqs.data(), reqs.size(), res.data());
     out->runtime_ms = ctx->last_ms;
     if (st != MPC_OK) return finish(st);
     out->base_price = res[0].price;

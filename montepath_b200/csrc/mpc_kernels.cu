@@ -1133,6 +1133,275 @@ int fused_max_blocks_per_sm(int family, int sampler, int block) {
   }
 }
 
+// ------------------------------------------------ scenario (bump) kernel ---
+// Bump-and-revalue Greeks with common random numbers: every leg of the
+// recipe (base, then up and down per Greek) has the same seed, so every leg
+// sees the same normals.  Here one thread draws each normal once and advances
+// all legs' paths with it; each leg keeps its own FP32 state and payoff, with
+// the same arithmetic as the single-request unit of its family.  Per unit the
+// legs' payoffs are warp-summed (FP64 sum and sum of squares) into per-warp
+// shared slots; per tile the slots are summed in warp order into tile
+// partials [tile][leg][2], and the last tile sums those in tile order.
+// Scenario parameters, struct of arrays [field][kMaxScen] (float):
+//   GBM:    log_s0, s0, drift_dt, vol_dt, discount, knocked-out-at-start (0/1)
+//   Heston: log_s0, v0, rate, dt, sqrt_dt, discount
+template <int W, class Src>
+__device__ __forceinline__ void scen_gbm_step(const DevReq& q, Src& src, const float* __restrict__ sp, int n_scen,
+                                              float pay[kMaxScen]) {
+  float ls[kMaxScen], acc[kMaxScen], drift[kMaxScen], vol[kMaxScen];
+  bool ko[kMaxScen];
+#pragma unroll
+  for (int s = 0; s < kMaxScen; ++s) {
+    ls[s] = __ldg(sp + 0 * kMaxScen + s);
+    acc[s] = (W == W_LOOKBACK) ? __ldg(sp + 1 * kMaxScen + s) : 0.0f;
+    drift[s] = __ldg(sp + 2 * kMaxScen + s);
+    vol[s] = __ldg(sp + 3 * kMaxScen + s);
+    ko[s] = __ldg(sp + 5 * kMaxScen + s) != 0.0f;
+  }
+  const float lbar = (float)q.log_barrier;
+  const uint32_t n = q.n_steps;
+  for (uint32_t st = 0; st < n; ++st) {
+    src.at_step(st, 1);
+    const float z = normal<float>(src, st);
+#pragma unroll
+    for (int s = 0; s < kMaxScen; ++s) {
+      if (s >= n_scen) break;
+      ls[s] += drift[s] + vol[s] * z;
+      if constexpr (W == W_ASIAN) acc[s] += __expf(ls[s]);
+      else if constexpr (W == W_LOOKBACK) acc[s] = acc[s] > __expf(ls[s]) ? acc[s] : __expf(ls[s]);
+      else if constexpr (W == W_DAO) ko[s] |= ls[s] <= lbar;
+      else if constexpr (W == W_UAO) ko[s] |= ls[s] >= lbar;
+    }
+  }
+  const float kk = (float)q.k, inv_n = (float)(1.0 / (double)n);
+#pragma unroll
+  for (int s = 0; s < kMaxScen; ++s) {
+    float v;
+    if constexpr (W == W_ASIAN) v = acc[s] * inv_n - kk;
+    else if constexpr (W == W_LOOKBACK) v = acc[s] - kk;
+    else {
+      v = __expf(ls[s]) - kk;
+      if (ko[s]) v = 0.0f;
+    }
+    pay[s] = (v > 0.0f ? v : 0.0f) * __ldg(sp + 4 * kMaxScen + s);
+  }
+}
+
+template <class Src>
+__device__ __forceinline__ void scen_gbm_terminal(const DevReq& q, Src& src, const float* __restrict__ sp, int n_scen,
+                                                  float pay[kMaxScen]) {
+  src.at_step(0, 1);
+  const float z = normal<float>(src, 0);
+  const float kk = (float)q.k;
+#pragma unroll
+  for (int s = 0; s < kMaxScen; ++s) {
+    const float st = __ldg(sp + 1 * kMaxScen + s) * __expf(__ldg(sp + 2 * kMaxScen + s) + __ldg(sp + 3 * kMaxScen + s) * z);
+    pay[s] = (st - kk > 0.0f ? st - kk : 0.0f) * __ldg(sp + 4 * kMaxScen + s);
+  }
+  (void)n_scen;
+}
+
+template <class Src>
+__device__ __forceinline__ void scen_heston(const DevReq& q, Src& src, const float* __restrict__ sp, int n_scen,
+                                            float pay[kMaxScen]) {
+  const float kappa = (float)q.kappa, theta = (float)q.theta, xi = (float)q.xi, rho = (float)q.rho,
+              rho_perp = (float)q.rho_perp;
+  float ls[kMaxScen], v[kMaxScen], rate[kMaxScen], dt[kMaxScen], sqdt[kMaxScen];
+#pragma unroll
+  for (int s = 0; s < kMaxScen; ++s) {
+    ls[s] = __ldg(sp + 0 * kMaxScen + s);
+    v[s] = __ldg(sp + 1 * kMaxScen + s);
+    rate[s] = __ldg(sp + 2 * kMaxScen + s);
+    dt[s] = __ldg(sp + 3 * kMaxScen + s);
+    sqdt[s] = __ldg(sp + 4 * kMaxScen + s);
+  }
+  const uint32_t n = q.n_steps;
+  for (uint32_t st = 0; st < n; ++st) {
+    src.at_step(2 * st, 2);
+    const float zv = normal<float>(src, 2 * st);
+    const float zi = normal<float>(src, 2 * st + 1);
+    const float zp = rho * zv + rho_perp * zi;
+#pragma unroll
+    for (int s = 0; s < kMaxScen; ++s) {
+      if (s >= n_scen) break;
+      const float vp = v[s] > 0.0f ? v[s] : 0.0f;
+      const float sv = sqrt_approx(vp);
+      ls[s] += (rate[s] - 0.5f * vp) * dt[s] + sv * sqdt[s] * zp;
+      v[s] = v[s] + kappa * (theta - vp) * dt[s] + xi * sv * sqdt[s] * zv;
+      v[s] = v[s] > 0.0f ? v[s] : 0.0f;
+    }
+  }
+  const float kk = (float)q.k;
+#pragma unroll
+  for (int s = 0; s < kMaxScen; ++s) {
+    const float stv = __expf(ls[s]);
+    pay[s] = (stv - kk > 0.0f ? stv - kk : 0.0f) * __ldg(sp + 5 * kMaxScen + s);
+  }
+}
+
+template <int FAM, class Src>
+__device__ __forceinline__ void scen_unit(const DevReq& q, Src& src, int n_scen, float pay[kMaxScen]) {
+  const float* sp = q.scen;
+  if constexpr (FAM == FAM_HESTON) {
+    scen_heston(q, src, sp, n_scen, pay);
+  } else if constexpr (FAM == FAM_GBM_TERMINAL) {
+    scen_gbm_terminal(q, src, sp, n_scen, pay);
+  } else {
+    switch (q.workload) {
+      case W_ASIAN:
+        scen_gbm_step<W_ASIAN>(q, src, sp, n_scen, pay);
+        break;
+      case W_DAO:
+        scen_gbm_step<W_DAO>(q, src, sp, n_scen, pay);
+        break;
+      case W_UAO:
+        scen_gbm_step<W_UAO>(q, src, sp, n_scen, pay);
+        break;
+      case W_LOOKBACK:
+        scen_gbm_step<W_LOOKBACK>(q, src, sp, n_scen, pay);
+        break;
+      default:
+        scen_gbm_step<W_EURO>(q, src, sp, n_scen, pay);
+        break;
+    }
+  }
+}
+
+// One request (reqs[0]) split into n_tiles tiles of q.tile_units units.
+template <int FAM, int SMP>
+__global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* __restrict__ reqs, uint32_t n_tiles,
+                                                                 uint32_t* __restrict__ counter, SrcCtx ctx) {
+  extern __shared__ __align__(16) uint32_t sobol_window[];
+  if constexpr (SMP == SMP_SOBOL) {
+    float4* seg = reinterpret_cast<float4*>(sobol_window + kSobolWindowWords);
+    const float4* src = reinterpret_cast<const float4*>(ctx.sobol + MPC_ICDF_OFFSET);
+    for (uint32_t i = threadIdx.x; i < MPC_ICDF_SEGMENTS; i += blockDim.x) seg[i] = src[i];
+    ctx.win = sobol_window;
+    ctx.icdf = seg;
+  } else {
+    ctx.win = nullptr;
+    ctx.icdf = nullptr;
+  }
+  __shared__ DevReq sq;
+  __shared__ double slots[kWarps][kMaxScen][2];
+  __shared__ uint32_t s_tile;
+  __shared__ int s_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= n_tiles) break;
+    {
+      const uint4* src = reinterpret_cast<const uint4*>(reqs);
+      uint4* dst = reinterpret_cast<uint4*>(&sq);
+      for (uint32_t i = threadIdx.x; i < sizeof(DevReq) / sizeof(uint4); i += blockDim.x) dst[i] = src[i];
+    }
+    for (uint32_t i = threadIdx.x; i < kWarps * kMaxScen * 2; i += blockDim.x) (&slots[0][0][0])[i] = 0.0;
+    __syncthreads();
+    const int n_scen = (int)sq.n_scen;
+    const uint64_t first = (uint64_t)t * sq.tile_units;
+    const uint64_t last = min(first + (uint64_t)sq.tile_units, sq.n_units);
+    const uint32_t iters = (uint32_t)((last - first + blockDim.x - 1) / blockDim.x);
+    for (uint32_t it = 0; it < iters; ++it) {
+      uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
+      const bool valid = u < last;
+      if (!valid) u = first;  // keeps block-synchronous sources in lockstep; discarded below
+      typename FusedSource<SMP>::type src;
+      src.template begin<false>(sq, ctx, u);
+      float pay[kMaxScen];
+      scen_unit<FAM>(sq, src, n_scen, pay);
+#pragma unroll
+      for (int s = 0; s < kMaxScen; ++s) {
+        if (s >= n_scen) break;
+        const double p = valid ? (double)pay[s] : 0.0;
+        const double a = warp_sum(p), b = warp_sum(p * p);
+        if (lane == 0) {
+          slots[warp][s][0] += a;
+          slots[warp][s][1] += b;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < (uint32_t)(2 * n_scen)) {
+      const int s = threadIdx.x >> 1, k = threadIdx.x & 1;
+      double sum = 0.0;
+      for (int w = 0; w < kWarps; ++w) sum += slots[w][s][k];
+      sq.partials[((size_t)t * kMaxScen + s) * 2 + k] = sum;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(sq.tiles_done, 1u) == n_tiles - 1) ? 1 : 0;
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      if (threadIdx.x < (uint32_t)(2 * n_scen)) {
+        const int s = threadIdx.x >> 1, k = threadIdx.x & 1;
+        double sum = 0.0;
+        for (uint32_t tt = 0; tt < n_tiles; ++tt) sum += __ldcg(sq.partials + ((size_t)tt * kMaxScen + s) * 2 + k);
+        sq.moments[s * 2 + k] = sum;
+      }
+      if (threadIdx.x == 0) *sq.tiles_done = 0u;
+    }
+    __syncthreads();
+  }
+}
+
+template <int SMP>
+static cudaError_t launch_scen_s(int family, const DevReq* d_req, uint32_t n_tiles, uint32_t* counter,
+                                 const SrcCtx& ctx, int grid, cudaStream_t stream) {
+  const size_t smem = fused_dynamic_smem<SMP>();
+  switch (family) {
+    case FAM_GBM_STEP:
+      scenario_kernel<FAM_GBM_STEP, SMP><<<grid, kFusedBlock, smem, stream>>>(d_req, n_tiles, counter, ctx);
+      break;
+    case FAM_GBM_TERMINAL:
+      scenario_kernel<FAM_GBM_TERMINAL, SMP><<<grid, kFusedBlock, smem, stream>>>(d_req, n_tiles, counter, ctx);
+      break;
+    case FAM_HESTON:
+      scenario_kernel<FAM_HESTON, SMP><<<grid, kFusedBlock, smem, stream>>>(d_req, n_tiles, counter, ctx);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <int SMP>
+static int scen_occ_s(int family) {
+  int n = 0;
+  const size_t smem = fused_dynamic_smem<SMP>();
+  if (family == FAM_GBM_STEP)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scenario_kernel<FAM_GBM_STEP, SMP>, kFusedBlock, smem);
+  else if (family == FAM_GBM_TERMINAL)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scenario_kernel<FAM_GBM_TERMINAL, SMP>, kFusedBlock, smem);
+  else if (family == FAM_HESTON)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scenario_kernel<FAM_HESTON, SMP>, kFusedBlock, smem);
+  return n;
+}
+int scenario_max_blocks_per_sm(int family, int sampler) {
+  if (sampler == SMP_XORSHIFT) return scen_occ_s<SMP_XORSHIFT>(family);
+  if (sampler == SMP_SOBOL) return scen_occ_s<SMP_SOBOL>(family);
+  if (sampler == SMP_COUNTER) return scen_occ_s<SMP_COUNTER>(family);
+  return 0;
+}
+
+cudaError_t launch_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_counter, int family, int sampler,
+                             const DeviceTables& tabs, int grid, cudaStream_t stream) {
+  SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
+  switch (sampler) {
+    case SMP_XORSHIFT:
+      return launch_scen_s<SMP_XORSHIFT>(family, d_req, n_tiles, d_counter, ctx, grid, stream);
+    case SMP_SOBOL:
+      return launch_scen_s<SMP_SOBOL>(family, d_req, n_tiles, d_counter, ctx, grid, stream);
+    case SMP_COUNTER:
+      return launch_scen_s<SMP_COUNTER>(family, d_req, n_tiles, d_counter, ctx, grid, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 // ------------------------------------------------------ FP64 plain path ---
 __device__ __forceinline__ bool is_uniform_dim(const DevReq& q, uint32_t d) {
   return (q.family == FAM_MERTON_STEP || q.family == FAM_MERTON_TERMINAL) && (d % 3u) == 1u;

@@ -82,6 +82,14 @@ uint32_t lsm_capacity(int fp64, int sampler);
 constexpr uint32_t kLsmPathsPerThreadMax = 8;
 constexpr uint32_t kLsmThreads = 256;
 
+// Bump-and-revalue legs sharing every normal: one request d_req (GBM step,
+// GBM terminal or Heston; xorshift, Sobol or counter-hash samples) whose
+// q.scen holds the legs' parameters; q.partials must hold
+// [n_tiles][kMaxScen][2] doubles and q.moments [kMaxScen][2].
+cudaError_t launch_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_counter, int family, int sampler,
+                             const DeviceTables& tabs, int grid, cudaStream_t stream);
+int scenario_max_blocks_per_sm(int family, int sampler);
+
 // Single-pass Greek estimators of the terminal-GBM European call
 // (pathwise: delta, vega, rho, theta; likelihood ratio: delta, vega, rho)
 // over the pseudorandom terminal shocks of one MonteCarloRng stream.

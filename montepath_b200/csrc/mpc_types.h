@@ -25,6 +25,11 @@ namespace mpc {
 constexpr uint32_t kBridgeDepth = 20;
 constexpr uint32_t kBridgeMaxSteps = 65536;
 
+// Scenario (bump-and-revalue) kernel: up to kMaxScen legs share every normal;
+// kScenFields float parameters per leg, stored [field][kMaxScen].
+constexpr int kMaxScen = 9;
+constexpr int kScenFields = 6;
+
 // Kernel families: the model-specific loop a tile runs.
 enum Family : int32_t {
   FAM_GBM_STEP = 0,
@@ -87,7 +92,8 @@ struct alignas(16) DevReq {
   const uint32_t* bridge_events;  // [(2 n_steps - 1 + 31) / 32]
   double bridge_sqrt_t, bridge_inv_sqrt_dt;
   uint32_t bridge;                // 1: normals come through the bridge
-  uint32_t _pad_b;
+  uint32_t n_scen;                // scenario kernel: legs in `scen` (0 elsewhere)
+  const float* scen;              // scenario kernel: [kScenFields][kMaxScen] leg parameters
   // samplers
   const uint32_t* halton_primes;
   const double* halton_shifts;

@@ -351,6 +351,32 @@ def test_greeks_fp32_within_stderr(backend):
         assert abs(_estimates(got)[greek].value - e.value) < 0.5 * e.stderr, greek
 
 
+@pytest.mark.parametrize("workload,kw", [
+    ("european_call", {"method": "stepwise", "n_steps": 64, "sampling": "scrambled_sobol"}),
+    ("european_call", {"sampling": "counter_hash"}),
+    ("arithmetic_asian_call", {"n_steps": 32}),
+    ("up_and_out_call", {"n_steps": 32, "barrier": 130.0, "sampling": "counter_hash"}),
+    ("lookback_call", {"n_steps": 32, "sampling": "scrambled_sobol"}),
+    ("european_call", {"model": "heston", "n_steps": 32, "sampling": "scrambled_sobol"}),
+])
+def test_scenario_bump_legs_equal_separate_pricing(backend, workload, kw):
+    """FP32 bump legs that share each normal in one scenario launch price like
+    the same legs priced as separate requests: the same FP32 expressions per
+    leg, but the two kernels may contract a*b+c into FMAs differently (1 ulp
+    on a path) and sum in a different order, so prices agree to 1e-7."""
+
+    r = req(workload, n_paths=20000, seed=31, **kw)
+    rep = backend.greeks(r, "bump_and_revalue")
+    base = backend.price(r)
+    assert abs(rep.base_price - base.price) <= 1e-7 * abs(base.price)
+    assert abs(rep.base_stderr - base.stderr) <= 1e-6 * base.stderr
+    delta = _estimates(rep)[abi.GREEK_DELTA]
+    up, down = abi.Request.from_buffer_copy(r), abi.Request.from_buffer_copy(r)
+    up.s0, down.s0 = r.s0 + delta.bump_size, r.s0 - delta.bump_size
+    assert abs(delta.bumped_up_price - backend.price(up).price) <= 1e-7 * abs(delta.bumped_up_price)
+    assert abs(delta.bumped_down_price - backend.price(down).price) <= 1e-7 * abs(delta.bumped_down_price)
+
+
 def test_greeks_unsupported_cases(backend):
     from montepath_b200.backend import BackendError
 
