@@ -321,8 +321,12 @@ const char* mpc_last_error_message(const mpc_context_t* ctx);
 int mpc_prepare(mpc_context_t* ctx, const mpc_request_t* req, mpc_artifact_t* out);
 /* NvidiaCudaBackend::execute (cuda.rs:187-193): prices one request on the GPU. */
 int mpc_price(mpc_context_t* ctx, const mpc_request_t* req, mpc_result_t* out);
-/* Prices n requests in one graph-captured persistent launch (fused FP32 path)
- * or, for FP64-plain requests, one launch sequence per request. */
+/* Prices n requests: the FP32-path requests in one persistent launch per
+ * (sampler, family) group, the FP64-plain requests one launch sequence each,
+ * LSM and MLMC requests in shared launches.  When a fused batch of the same
+ * shape (sizes, launch shapes, buffers) comes twice in a row, the second call
+ * captures its copy/launch sequence in a CUDA graph and later calls of that
+ * shape replay the graph (one launch call). */
 int mpc_price_batch(mpc_context_t* ctx, const mpc_request_t* reqs, size_t n, mpc_result_t* out);
 /* Greeks of one request: european_call_greeks_cpu, arithmetic_asian_call_greeks_cpu,
  * down_and_out_call_greeks_cpu, lookback_call_greeks_cpu, basket_call_greeks_cpu,

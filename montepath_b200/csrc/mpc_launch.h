@@ -117,5 +117,7 @@ cudaError_t launch_flush(void* d_buf, size_t bytes, cudaStream_t stream);
 
 // Kernel launches issued by the wrappers above since process start.
 uint64_t kernel_launch_count();
+// Adds the kernels of a replayed CUDA graph to the count.
+void count_graph_launches(uint64_t kernels);
 
 }  // namespace mpc

@@ -73,9 +73,15 @@ struct mpc_context {
   void* pinned = nullptr;                   // pinned staging for descriptors and results
   size_t pinned_bytes = 0;
   mpc::Autotuner tuner;
-  // graph cache of the last fused batch
+  // CUDA graph of the fused batch sequence (copies in, launches, copy out):
+  // captured when the same batch shape comes twice in a row, replayed while
+  // it repeats.  The key holds every address, size and launch shape the graph
+  // bakes in.
   cudaGraphExec_t graph_exec = nullptr;
-  uint64_t graph_key = 0;
+  std::vector<uint64_t> graph_key;      // key of graph_exec
+  std::vector<uint64_t> last_batch_key;  // key of the previous fused batch
+  uint64_t graph_kernels = 0;           // kernels in graph_exec
+  uint64_t graph_replays = 0;
 };
 
 namespace mpc {
