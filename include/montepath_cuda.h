@@ -235,6 +235,20 @@ typedef struct mpc_greek_report {
 #define MPC_GREEK_WARN_PSEUDORANDOM_SHOCKS 0x2u   /* single-pass estimators draw the pseudorandom stream whatever the sampling */
 #define MPC_GREEK_WARN_TECHNIQUE_IGNORED 0x4u     /* single-pass estimators ignore the variance-reduction technique */
 
+/* Cost estimate of one request on the GPU: CostEstimate of the reference
+ * (crates/mc-core/src/backend/mod.rs:55-63) for NvidiaCudaBackend::estimate_cost
+ * (cuda.rs:121-152), from device rates measured per kernel family, sampler and
+ * precision on a B200 (148 SMs) and scaled by the SM count given. */
+typedef struct mpc_cost {
+  double estimated_compile_ms;  /* first call of a shape: lookup tables, autotuner, buffers */
+  double estimated_runtime_ms;  /* device time of the request's launches */
+  double estimated_total_ms;    /* compile + runtime + per-call overhead */
+  double estimated_peak_memory_mb;
+  double path_steps_per_sec;    /* modelled device rate */
+  uint64_t path_steps;
+  char confidence[16];          /* "measured": a measured rate; "derived": scaled from one */
+} mpc_cost_t;
+
 typedef struct mpc_device_info {
   int32_t index;
   int32_t sm_count;
@@ -295,7 +309,7 @@ typedef struct mpc_server_stats {
 /* ----- library and devices -------------------------------------------- */
 int mpc_abi_version(void);
 /* Sizes of the ABI structs, for binding self-checks (ctypes, cgo). */
-size_t mpc_struct_size(int which); /* 0 request, 1 result, 2 device_info, 3 options, 4 support, 5 artifact, 6 server_options, 7 server_stats, 8 greek_report */
+size_t mpc_struct_size(int which); /* 0 request, 1 result, 2 device_info, 3 options, 4 support, 5 artifact, 6 server_options, 7 server_stats, 8 greek_report, 9 cost */
 const char* mpc_status_string(int status);
 
 /* Replaces NvidiaCudaBackend::discover_devices' nvidia-smi parsing (cuda.rs:205-241). */
@@ -311,6 +325,9 @@ int mpc_validate(const mpc_request_t* req, char* message, size_t message_len);
 int mpc_supports(const mpc_request_t* req, mpc_support_t* out);
 /* Device bytes a request holds while it runs (estimate_gpu_bytes_per_path, backend/mod.rs:399-405). */
 int mpc_estimate_bytes(const mpc_request_t* req, uint64_t* bytes);
+/* NvidiaCudaBackend::estimate_cost (cuda.rs:121-152) from the measured cost
+ * model (host only).  sm_count 0 = 148. */
+int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out);
 
 /* ----- context ---------------------------------------------------------- */
 int mpc_create(const mpc_options_t* options, mpc_context_t** out);

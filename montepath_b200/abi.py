@@ -329,7 +329,19 @@ class GreekReport(Structure):
     ]
 
 
-STRUCTS = [Request, Result, DeviceInfo, Options, Support, Artifact, ServerOptions, ServerStats, GreekReport]
+class Cost(Structure):
+    _fields_ = [
+        ("estimated_compile_ms", c_double),
+        ("estimated_runtime_ms", c_double),
+        ("estimated_total_ms", c_double),
+        ("estimated_peak_memory_mb", c_double),
+        ("path_steps_per_sec", c_double),
+        ("path_steps", c_uint64),
+        ("confidence", c_char * 16),
+    ]
+
+
+STRUCTS = [Request, Result, DeviceInfo, Options, Support, Artifact, ServerOptions, ServerStats, GreekReport, Cost]
 
 # (name, restype, argtypes) of every exported entry point, in header order.
 FUNCTIONS = [
@@ -342,6 +354,7 @@ FUNCTIONS = [
     ("mpc_validate", c_int, [POINTER(Request), c_char_p, c_size_t]),
     ("mpc_supports", c_int, [POINTER(Request), POINTER(Support)]),
     ("mpc_estimate_bytes", c_int, [POINTER(Request), POINTER(c_uint64)]),
+    ("mpc_estimate_cost", c_int, [POINTER(Request), c_int, POINTER(Cost)]),
     ("mpc_create", c_int, [POINTER(Options), POINTER(c_void_p)]),
     ("mpc_destroy", c_int, [c_void_p]),
     ("mpc_last_error_message", c_char_p, [c_void_p]),

@@ -31,6 +31,7 @@ namespace mpc {
 static std::atomic<uint64_t> g_launches{0};
 uint64_t kernel_launch_count() { return g_launches.load(); }
 void count_graph_launches(uint64_t kernels) { g_launches.fetch_add(kernels); }
+void discount_captured_launches(uint64_t kernels) { g_launches.fetch_sub(kernels); }
 static inline void count_launch() { g_launches.fetch_add(1); }
 
 enum Workload : int32_t {

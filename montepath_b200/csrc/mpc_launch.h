@@ -119,5 +119,7 @@ cudaError_t launch_flush(void* d_buf, size_t bytes, cudaStream_t stream);
 uint64_t kernel_launch_count();
 // Adds the kernels of a replayed CUDA graph to the count.
 void count_graph_launches(uint64_t kernels);
+// Takes back the counts of launches that were only captured into a graph.
+void discount_captured_launches(uint64_t kernels);
 
 }  // namespace mpc

@@ -738,12 +738,8 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
     key.insert(key.end(), {uint64_t(int64_t(gl[g].family)), uint64_t(gl[g].sampler), grids[g], group_first[g],
                            group_count[g]});
   uint64_t launches_before = kernel_launch_count();
-  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
-  if (ctx->graph_exec && key == ctx->graph_key) {  // same shape again: replay
-    MPC_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
-    count_graph_launches(ctx->graph_kernels);
-    ++ctx->graph_replays;
-  } else if (key == ctx->last_batch_key) {  // second time in a row: capture, then replay
+  bool replay = ctx->graph_exec && key == ctx->graph_key;
+  if (!replay && key == ctx->last_batch_key) {  // second time in a row: capture (host only), then replay
     if (ctx->graph_exec) {
       cudaGraphExecDestroy(ctx->graph_exec);
       ctx->graph_exec = nullptr;
@@ -759,6 +755,7 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
       return cuda_fail(ctx, e != cudaSuccess ? e : e_end, "capture of the fused batch");
     }
     const uint64_t kernels = kernel_launch_count() - counted;
+    discount_captured_launches(kernels);  // captured, not run: the replay below counts them
     cudaGraphExec_t exec = nullptr;
     const cudaError_t e_inst = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
@@ -766,8 +763,13 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
     ctx->graph_exec = exec;
     ctx->graph_key = key;
     ctx->graph_kernels = kernels;
+    replay = true;
+  }
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));  // device time excludes capture on the host
+  if (replay) {
     MPC_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
-    launches_before = kernel_launch_count() - kernels;  // the captured launches ran once, in the graph
+    count_graph_launches(ctx->graph_kernels);
+    ++ctx->graph_replays;
   } else {
     const cudaError_t e = enqueue();
     if (e != cudaSuccess) return cuda_fail(ctx, e, "fused pricing batch");
@@ -1495,6 +1497,105 @@ void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {
 // ======================================================= C entry points ====
 extern "C" {
 
+// ------------------------------------------------------------ cost model ---
+// Device rates in units per second (path-steps for stepwise families, paths
+// for terminal ones), steady-state CUDA-event time of one request of
+// 1,048,576 paths x 64 steps on a B200 (148 SMs, 1965 MHz), per sampler
+// {pseudorandom, counter hash, scrambled Sobol, Halton/LHS}.
+namespace {
+struct RateRow {
+  double fp32[4], fp64[4];
+};
+const RateRow kRateGbmStep = {{2.24e11, 3.25e11, 3.85e11, 9.05e10}, {1.31e11, 1.35e11, 5.96e10, 5.38e10}};
+const RateRow kRateAsian = {{2.12e11, 2.93e11, 3.50e11, 8.84e10}, {1.12e11, 1.16e11, 5.59e10, 5.02e10}};
+const RateRow kRateGbmTerminal = {{6.68e9, 1.83e10, 1.53e10, 1.11e10}, {7.38e9, 2.45e10, 1.98e10, 1.12e10}};
+const RateRow kRateHeston = {{1.45e11, 1.93e11, 2.23e11, 5.37e10}, {7.09e10, 6.85e10, 3.02e10, 3.14e10}};
+const RateRow kRateMertonStep = {{1.05e11, 1.05e11, 1.97e11, 4.30e10}, {4.16e10, 4.16e10, 2.65e10, 2.63e10}};
+const RateRow kRateMertonTerminal = {{1.70e10, 1.70e10, 1.44e10, 7.09e9}, {1.83e10, 1.83e10, 1.30e10, 6.60e9}};
+const RateRow kRateBasket2 = {{5.46e9, 1.53e10, 1.28e10, 7.74e9}, {5.49e9, 1.58e10, 1.13e10, 6.77e9}};
+const double kRateBridge[2] = {1.41e11, 4.59e10};  // GBM stepwise through the bridge, fp32 / fp64
+const double kLsmFixedMs = 0.72, kLsmRate = 1.8e10; // 49 date barriers, then path-steps
+const double kCallOverheadMs = 0.035;               // events, copies, one launch
+const double kFirstCallMs = 2.0;                    // tables and buffers of a new shape
+
+int rate_column(int sampling) {
+  switch (sampling) {
+    case MPC_SAMPLING_PSEUDORANDOM:
+      return 0;
+    case MPC_SAMPLING_COUNTER_HASH:
+      return 1;
+    case MPC_SAMPLING_SCRAMBLED_SOBOL:
+    case MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE:
+      return 2;
+    default:
+      return 3;
+  }
+}
+}  // namespace
+
+int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out) {
+  if (!req || !out) return MPC_E_INVALID_CONFIG;
+  std::memset(out, 0, sizeof(*out));
+  std::string msg;
+  int st = validate(*req, &msg);
+  if (st != MPC_OK) return st;
+  const mpc_request_t& r = *req;
+  const bool fp64 = r.precision == MPC_PRECISION_FP64_PLAIN;
+  const int col = rate_column(r.sampling);
+  const double scale = double(sm_count > 0 ? sm_count : 148) / 148.0;
+  auto pick = [&](const RateRow& row) { return (fp64 ? row.fp64[col] : row.fp32[col]) * scale; };
+  double units = double(r.n_paths) * double(r.n_steps), rate = 0.0, fixed_ms = 0.0;
+  const char* confidence = "measured";
+  if (is_lsm(r.workload)) {
+    rate = kLsmRate * scale;
+    fixed_ms = kLsmFixedMs * double(std::max<uint32_t>(r.n_steps, 2) - 1) / 49.0;
+    if (r.workload == MPC_WORKLOAD_BERMUDAN_PUT) fixed_ms *= double(std::max<uint32_t>(r.n_exercise, 1)) / 49.0;
+    confidence = "derived";
+  } else if (r.workload == MPC_WORKLOAD_ASIAN_MLMC) {
+    // the level budget bounds the work: explicit paths per level, else the solver's cap
+    double updates = 0.0;
+    uint64_t fine = r.base_steps;
+    for (uint32_t l = 0; l < r.levels; ++l, fine *= std::max<uint32_t>(r.refinement_factor, 2))
+      updates += double(r.paths_per_level[l]) * double(fine) * (l ? 1.5 : 1.0);
+    if (r.target_stderr > 0.0) updates = double(r.max_step_updates);
+    units = updates;
+    rate = pick(kRateAsian);
+    fixed_ms = 2.0 * kCallOverheadMs * double(std::max<uint32_t>(r.levels, 1));
+    confidence = "derived";
+  } else if (r.workload == MPC_WORKLOAD_BASKET_CALL) {
+    units = double(r.n_paths) * double(std::max<uint32_t>(r.n_steps, 1)) * double(std::max<uint32_t>(r.n_assets, 2)) / 2.0;
+    rate = pick(kRateBasket2);
+    if (r.n_assets > 2 || r.n_steps > 1) confidence = "derived";
+  } else if (r.model == MPC_MODEL_HESTON) {
+    rate = pick(kRateHeston);
+  } else if (r.model == MPC_MODEL_MERTON) {
+    if (r.method == MPC_METHOD_STEPWISE) {
+      rate = pick(kRateMertonStep);
+    } else {
+      units = double(r.n_paths);
+      rate = pick(kRateMertonTerminal);
+    }
+  } else if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.method != MPC_METHOD_STEPWISE) {
+    units = double(r.n_paths);
+    rate = pick(kRateGbmTerminal);
+  } else if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE) {
+    rate = kRateBridge[fp64 ? 1 : 0] * scale;
+  } else {
+    rate = pick(r.workload == MPC_WORKLOAD_ARITHMETIC_ASIAN_CALL ? kRateAsian : kRateGbmStep);
+  }
+  if (r.technique == MPC_TECHNIQUE_ANTITHETIC) rate *= 1.6;  // one draw drives two paths
+  uint64_t bytes = 0;
+  mpc_estimate_bytes(req, &bytes);
+  out->estimated_compile_ms = kFirstCallMs;
+  out->estimated_runtime_ms = fixed_ms + units / rate * 1e3;
+  out->estimated_total_ms = out->estimated_runtime_ms + kCallOverheadMs + out->estimated_compile_ms;
+  out->estimated_peak_memory_mb = double(bytes) / (1024.0 * 1024.0);
+  out->path_steps_per_sec = rate;
+  out->path_steps = uint64_t(units);
+  std::snprintf(out->confidence, sizeof(out->confidence), "%s", confidence);
+  return MPC_OK;
+}
+
 int mpc_abi_version(void) { return MPC_ABI_VERSION; }
 
 size_t mpc_struct_size(int which) {
@@ -1517,6 +1618,8 @@ size_t mpc_struct_size(int which) {
       return sizeof(mpc_server_stats_t);
     case 8:
       return sizeof(mpc_greek_report_t);
+    case 9:
+      return sizeof(mpc_cost_t);
     default:
       return 0;
   }

@@ -158,3 +158,55 @@ def execute_workload(workload: str, config: Mapping[str, Any] | None = None, *, 
         "manifest": result["manifest"],
         "warnings": list(result["warnings"]),
     }
+
+
+def estimate_cost(workload: str, config: Mapping[str, Any] | None = None, *, sm_count: int = 0) -> dict[str, Any]:
+    """NvidiaCudaBackend::estimate_cost (crates/mc-core/src/backend/cuda.rs:121-152)
+    from the measured cost model (``mpc_estimate_cost``; host only, no GPU needed)."""
+
+    from .requests import make_request
+
+    params = dict(config or {})
+    code = {"heston_european_call": "european_call", "merton_jump_diffusion_call": "european_call"}.get(workload, workload)
+    if workload == "heston_european_call":
+        params.setdefault("model", "heston")
+        params.setdefault("method", "stepwise")
+    if workload == "merton_jump_diffusion_call":
+        params.setdefault("model", "merton")
+        params.setdefault("sampling", "counter_hash")
+    req = make_request(code, params)
+    cost = abi.Cost()
+    status = abi.load_library().mpc_estimate_cost(ctypes.byref(req), int(sm_count), ctypes.byref(cost))
+    if status != abi.OK:
+        raise ValueError(f"MC_CONFIG_INVALID: {abi.status_name(status)}")
+    return {
+        "backend_id": "nvidia_cuda",
+        "estimated_compile_ms": cost.estimated_compile_ms,
+        "estimated_runtime_ms": cost.estimated_runtime_ms,
+        "estimated_total_ms": cost.estimated_total_ms,
+        "estimated_peak_memory_mb": cost.estimated_peak_memory_mb,
+        "confidence": cost.confidence.decode(),
+        "path_steps": cost.path_steps,
+        "path_steps_per_sec": cost.path_steps_per_sec,
+    }
+
+
+def planner_priority(workload: str, config: Mapping[str, Any] | None = None, *,
+                     cuda_available: bool | None = None) -> list[str]:
+    """Backend order for one run, by estimated total time: the CUDA estimate
+    from the measured cost model against the reference's CPU estimate
+    (CpuNativeBackend::estimate_cost, backend/mod.rs:292-305: n_paths x n_steps
+    / 5e6 per ms).  Stands in for the fixed thresholds of backend_priority
+    (planner/mod.rs:509-549) when the CUDA backend is present; Apple Metal is
+    never available on this hardware and goes last."""
+
+    cfg = dict(config or {})
+    paths = int(cfg.get("n_paths", 10_000))
+    steps = int(cfg.get("n_steps", 1)) if workload not in ("european_call",) or cfg.get("method") == "stepwise" else 1
+    cpu_ms = max(paths * max(steps, 1) / 5_000_000.0, 0.01)
+    if cuda_available is None:
+        cuda_available = cuda_capability()["status"] == "available"
+    if not cuda_available:
+        return ["cpu_native", "nvidia_cuda", "apple_metal"]
+    cuda_ms = estimate_cost(workload, cfg)["estimated_total_ms"]
+    return (["nvidia_cuda", "cpu_native"] if cuda_ms < cpu_ms else ["cpu_native", "nvidia_cuda"]) + ["apple_metal"]

@@ -254,3 +254,25 @@ def test_mc_bench_rows_have_the_harness_shape(monkeypatch):
     for row in report["results"]:
         assert set(row) == fields and row["backend"] == "nvidia_cuda" and row["iterations"] == 2
         assert row["throughput_per_sec"] > 0 and row["metric_value"] > 0
+
+
+def test_cost_model_and_planner_priority():
+    """mpc_estimate_cost (host only) and the planner order it feeds."""
+
+    from montepath_b200 import production
+
+    big = production.estimate_cost("heston_european_call", {"n_paths": 1 << 20, "n_steps": 256,
+                                                             "sampling": "scrambled_sobol"})
+    # measured headline rate: 268,435,456 path-steps in about 1 ms of device time
+    assert 0.6 < big["estimated_runtime_ms"] < 2.0 and big["confidence"] == "measured"
+    small = production.estimate_cost("european_call", {"n_paths": 1000})
+    assert small["estimated_runtime_ms"] < 0.01 < small["estimated_total_ms"]
+    plain = production.estimate_cost("european_call", {"n_paths": 1 << 20, "n_steps": 64, "method": "stepwise",
+                                                       "precision": "fp64_plain", "sampling": "scrambled_sobol"})
+    fused = production.estimate_cost("european_call", {"n_paths": 1 << 20, "n_steps": 64, "method": "stepwise",
+                                                       "sampling": "scrambled_sobol"})
+    assert plain["estimated_runtime_ms"] > 5 * fused["estimated_runtime_ms"]
+    assert production.planner_priority("heston_european_call", {"n_paths": 1 << 20, "n_steps": 256},
+                                       cuda_available=True)[0] == "nvidia_cuda"
+    assert production.planner_priority("european_call", {"n_paths": 100}, cuda_available=True)[0] == "cpu_native"
+    assert production.planner_priority("european_call", {"n_paths": 10**6}, cuda_available=False)[0] == "cpu_native"

@@ -509,6 +509,29 @@ def test_reference_v1_kernel_contract(backend):
     assert np.allclose(payoffs.cpu().numpy(), ref, rtol=1e-12, atol=1e-12)
 
 
+# ------------------------------------------------------------ cost model --
+@pytest.mark.parametrize("workload,kw", [
+    ("european_call", dict(model="heston", method="stepwise", n_steps=128, sampling="scrambled_sobol")),
+    ("arithmetic_asian_call", dict(n_steps=96, sampling="counter_hash")),
+    ("european_call", dict(method="stepwise", n_steps=64, precision="fp64_plain", sampling="scrambled_sobol")),
+    ("american_put", dict(n_steps=50)),
+])
+def test_cost_model_predicts_device_time(backend, workload, kw):
+    """mpc_estimate_cost against the measured device time of the same request (within 2x)."""
+
+    import ctypes
+
+    r = req(workload, n_paths=1 << 19 if workload != "american_put" else 200_000, seed=3, **kw)
+    cost = abi.Cost()
+    assert abi.load_library().mpc_estimate_cost(ctypes.byref(r), 0, ctypes.byref(cost)) == abi.OK
+    times = []
+    for _ in range(3):
+        backend.price(r)
+        times.append(backend.last_timing()[0])
+    measured = min(times)
+    assert 0.5 < cost.estimated_runtime_ms / measured < 2.0, (cost.estimated_runtime_ms, measured)
+
+
 # ---------------------------------------------------------- harness rows --
 def test_mc_bench_compact_rows(backend):
     """mc_cuda_* rows (BenchmarkResult shape) from the real device, compact suite."""
