@@ -1595,38 +1595,6 @@ __device__ __forceinline__ uint64_t global_ns() {
   return t;
 }
 
-// Barrier over the `nblocks` blocks of one job of a cooperative launch.  The
-// wait is bounded: after timeout_ns the block records the failure in *error
-// and every block of the job leaves the kernel at the next check.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* error, uint64_t timeout_ns, uint32_t nblocks) {
-  __shared__ int s_ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned* gen = bar + 1;
-    const unsigned g = *gen;
-    __threadfence();
-    if (atomicAdd(bar, 1u) == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      const uint64_t start = global_ns();
-      while (*gen == g) {
-        if (*((volatile int*)error) != 0) break;
-        if (global_ns() - start > timeout_ns) {
-          atomicCAS(error, 0, kLsmErrTimeout);
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-    s_ok = *((volatile int*)error) == 0;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
 template <class Real>
 __device__ __forceinline__ void laguerre4(Real x, Real b[4]) {
   // laguerre_lsm_basis (cpu.rs:7667-7682); degrees above `degree` are unused
@@ -1637,44 +1605,59 @@ __device__ __forceinline__ void laguerre4(Real x, Real b[4]) {
   b[3] = (Real)1 - (Real)3 * x + (Real)1.5 * x2 - x3 / (Real)6;
 }
 
-// solve_lsm_normal_equations (cpu.rs:7684-7736), FP64 Gauss-Jordan.
-__device__ bool solve4(double a[4][4], double rhs[4], int dim) {
-  for (int piv = 0; piv < dim; ++piv) {
+// solve_lsm_normal_equations (cpu.rs:7684-7736) for a compile-time size:
+// Gauss-Jordan with partial pivoting in FP64, the reference's operations in
+// its order, with every index static (the pivot row swap is a predicated exchange), so the
+// system stays in registers.
+template <int DIM>
+__device__ __forceinline__ bool solve_fixed(double a[4][4], double rhs[4]) {
+#pragma unroll
+  for (int piv = 0; piv < DIM; ++piv) {
     int best = piv;
     double best_abs = fabs(a[piv][piv]);
-    for (int row = piv + 1; row < dim; ++row) {
-      double c = fabs(a[row][piv]);
+#pragma unroll
+    for (int row = piv + 1; row < DIM; ++row) {
+      const double c = fabs(a[row][piv]);
       if (c > best_abs) {
         best = row;
         best_abs = c;
       }
     }
     if (best_abs <= 1e-12) return false;
-    if (best != piv) {
-      for (int c = 0; c < 4; ++c) {
-        double t = a[piv][c];
-        a[piv][c] = a[best][c];
-        a[best][c] = t;
+#pragma unroll
+    for (int row = piv + 1; row < DIM; ++row) {
+      if (row == best) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const double t = a[piv][c];
+          a[piv][c] = a[row][c];
+          a[row][c] = t;
+        }
+        const double t = rhs[piv];
+        rhs[piv] = rhs[row];
+        rhs[row] = t;
       }
-      double t = rhs[piv];
-      rhs[piv] = rhs[best];
-      rhs[best] = t;
     }
-    double pv = a[piv][piv];
-    for (int c = piv; c < dim; ++c) a[piv][c] /= pv;
+    const double pv = a[piv][piv];
+#pragma unroll
+    for (int c = piv; c < DIM; ++c) a[piv][c] /= pv;
     rhs[piv] /= pv;
-    for (int row = 0; row < dim; ++row) {
+#pragma unroll
+    for (int row = 0; row < DIM; ++row) {
       if (row == piv) continue;
-      double f = a[row][piv];
+      const double f = a[row][piv];
       if (f == 0.0) continue;
-      for (int c = piv; c < dim; ++c) a[row][c] -= f * a[piv][c];
+#pragma unroll
+      for (int c = piv; c < DIM; ++c) a[row][c] -= f * a[piv][c];
       rhs[row] -= f * rhs[piv];
     }
   }
   return true;
 }
 
+
 constexpr int kLsmBlock = (int)kLsmThreads;
+
 constexpr int kLsmMaxP = (int)kLsmPathsPerThreadMax;
 constexpr int kLsmMom = 15;  // 10 unique A^T A, 4 A^T b, ITM count
 
@@ -1688,8 +1671,104 @@ __device__ __forceinline__ bool lsm_ok(const LsmArgs& a, uint64_t index, uint64_
   return false;
 }
 
+// One exercise date's regression across the job's blocks.  Every block has
+// written its 15 moments to partials[buf][lb]; thread 0 takes a ticket; the
+// block with the last ticket sums all partials in block order (strided per
+// thread, then the fixed block tree), solves, writes (ok, beta) to
+// out[8 + 5 buf ..] and bumps the generation; the other blocks spin until the
+// generation moves and then read the published coefficients.  The spin is
+// bounded: after timeout_ns the block records kLsmErrTimeout and every block
+// of the job leaves at its next check.  Returns false when the job's error
+// flag is set.
+__device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint32_t nb, int coeffs,
+                                                 double (*red)[5], double* s_mom, double* s_beta, int* s_ok) {
+  __shared__ int s_last, s_good;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = a.barrier + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    s_last = atomicAdd(a.barrier, 1u) == nb - 1 ? 1 : 0;
+    s_good = 1;
+    if (!s_last) {
+      const uint64_t start = global_ns();
+      while (*gen == g) {
+        if (*((volatile int*)a.error) != 0) break;
+        if (global_ns() - start > a.timeout_ns) {
+          atomicCAS(a.error, 0, kLsmErrTimeout);
+          break;
+        }
+      }
+      __threadfence();
+      s_good = *((volatile int*)a.error) == 0;
+    }
+  }
+  __syncthreads();
+  if (!s_good) return false;
+  double* pub = a.out + 8 + 5 * buf;  // published (ok, beta0..3) of this date
+  if (s_last) {
+    __threadfence();
+    double acc[kLsmMom];
+#pragma unroll
+    for (int i = 0; i < kLsmMom; ++i) acc[i] = 0.0;
+    const uint64_t base_at = (uint64_t)buf * nb * 16;
+    const double* base = a.partials + base_at;
+    for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
+      if (!lsm_ok(a, base_at + (uint64_t)blk * 16 + kLsmMom - 1, a.partials_len, kLsmErrPartials)) break;
+#pragma unroll
+      for (int i = 0; i < kLsmMom; ++i) acc[i] += __ldcg(base + (size_t)blk * 16 + i);
+    }
+    for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
+      double v[5] = {acc[r0], acc[r0 + 1], acc[r0 + 2], acc[r0 + 3], acc[r0 + 4]};
+      block_reduce5(v, red);
+      if (threadIdx.x == 0)
+        for (int i = 0; i < 5; ++i) s_mom[r0 + i] = v[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double ata[4][4], atb[4];
+      int idx = 0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = r; c < 4; ++c) {
+          ata[r][c] = s_mom[idx];
+          ata[c][r] = s_mom[idx];
+          ++idx;
+        }
+#pragma unroll
+      for (int r = 0; r < 4; ++r) atb[r] = s_mom[10 + r];
+      // the reference zeroes rows/columns beyond the basis degree
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        if (r < coeffs) continue;
+        atb[r] = 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) ata[r][c] = ata[c][r] = 0.0;
+      }
+      int ok = s_mom[14] >= (double)coeffs ? 1 : 0;
+      if (ok) ok = (coeffs == 2 ? solve_fixed<2>(ata, atb) : coeffs == 3 ? solve_fixed<3>(ata, atb) : solve_fixed<4>(ata, atb)) ? 1 : 0;
+      pub[0] = ok ? 1.0 : 0.0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r) pub[1 + r] = (ok && r < coeffs) ? atb[r] : 0.0;
+      __threadfence();
+      atomicExch(a.barrier, 0u);
+      __threadfence();
+      atomicAdd(a.barrier + 1, 1u);  // release the waiting blocks
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const double ok = __ldcg(pub);
+    for (int r = 0; r < 4; ++r) s_beta[r] = __ldcg(pub + 1 + r);
+    *s_ok = ok != 0.0 ? 1 : 0;
+  }
+  __syncthreads();
+  return true;
+}
+
 template <class Real, int SMP>
-__global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restrict__ jobs, uint32_t n_jobs, SrcCtx ctx) {
+__global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __restrict__ jobs, uint32_t n_jobs, SrcCtx ctx) {
   __shared__ double red[kWarps][5];
   __shared__ double s_mom[16];
   __shared__ double s_beta[4];
@@ -1796,48 +1875,10 @@ __global__ void __launch_bounds__(kLsmBlock) lsm_kernel(const LsmArgs* __restric
         for (int i = 0; i < 5; ++i) part[r0 + i] = v[i];
       __syncthreads();
     }
-    if (!grid_barrier(a.barrier, a.error, a.timeout_ns, nb)) return;
-    // every block sums the block partials in the same fixed order (identical result everywhere)
-    {
-      double acc[kLsmMom];
-#pragma unroll
-      for (int i = 0; i < kLsmMom; ++i) acc[i] = 0.0;
-      const uint64_t base_at = (uint64_t)buf * nb * 16;
-      const double* base = a.partials + base_at;
-      for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
-        if (!lsm_ok(a, base_at + (uint64_t)blk * 16 + kLsmMom - 1, a.partials_len, kLsmErrPartials)) break;
-#pragma unroll
-        for (int i = 0; i < kLsmMom; ++i) acc[i] += __ldcg(base + (size_t)blk * 16 + i);
-      }
-      for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
-        double v[5] = {acc[r0], acc[r0 + 1], acc[r0 + 2], acc[r0 + 3], acc[r0 + 4]};
-        block_reduce5(v, red);
-        if (threadIdx.x == 0)
-          for (int i = 0; i < 5; ++i) s_mom[r0 + i] = v[i];
-      }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double ata[4][4] = {{0}}, atb[4] = {0};
-      int idx = 0;
-      for (int r = 0; r < 4; ++r)
-        for (int c = r; c < 4; ++c) {
-          ata[r][c] = s_mom[idx];
-          ata[c][r] = s_mom[idx];
-          ++idx;
-        }
-      for (int r = 0; r < 4; ++r) atb[r] = s_mom[10 + r];
-      // the reference zeroes rows/columns beyond the basis degree
-      for (int r = coeffs; r < 4; ++r) {
-        atb[r] = 0.0;
-        for (int c = 0; c < 4; ++c) ata[r][c] = ata[c][r] = 0.0;
-      }
-      int ok = s_mom[14] >= (double)coeffs ? 1 : 0;
-      if (ok) ok = solve4(ata, atb, coeffs) ? 1 : 0;
-      for (int r = 0; r < 4; ++r) s_beta[r] = (ok && r < coeffs) ? atb[r] : 0.0;
-      s_ok = ok;
-    }
-    __syncthreads();
+    // The last block to arrive sums the block partials in block order, solves
+    // the normal equations once and publishes the coefficients; the others
+    // wait (bounded) for the publication and read 5 doubles.
+    if (!lsm_gather_solve(a, buf, nb, coeffs, red, s_mom, s_beta, &s_ok)) return;
     if (s_ok) {
       ++regressions;
       const Real b0 = (Real)s_beta[0], b1 = (Real)s_beta[1], b2 = (Real)s_beta[2], b3 = (Real)s_beta[3];

@@ -46,8 +46,9 @@ struct LsmArgs {
   void* paths;               // [n_steps][n_paths] float or double
   double* partials;          // [2][grid][16]
   double* final_partials;    // [grid][4]
-  double* out;               // [8]: n, sum, sumsq, early, maturity, regressions
-  unsigned* barrier;         // [2]: count, generation
+  double* out;               // [24]: n, sum, sumsq, early, maturity, regressions, -, -; then per date
+                             // parity two published (ok, beta0..3) of the regression
+  unsigned* barrier;         // counter area (kLsmCounterBytes): arrival count, generation, ...
   unsigned* done;            // last-block counter
   int* error;                // first failure: kLsmErr* code (0 = none)
   unsigned long long* diag;  // offending index of a failed self-check
@@ -81,6 +82,8 @@ cudaError_t launch_lsm_batch(const LsmArgs* d_jobs, uint32_t n_jobs, uint32_t to
 uint32_t lsm_capacity(int fp64, int sampler);
 constexpr uint32_t kLsmPathsPerThreadMax = 8;
 constexpr uint32_t kLsmThreads = 256;
+// Counter area of an LSM job (zeroed per launch).
+constexpr size_t kLsmCounterBytes = 64;
 
 // Bump-and-revalue legs sharing every normal: one request d_req (GBM step,
 // GBM terminal or Heston; xorshift, Sobol or counter-hash samples) whose

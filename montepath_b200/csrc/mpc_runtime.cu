@@ -966,7 +966,7 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       const size_t elem = j.fp64 ? 8 : 4;
       bytes += align(j.args.n_paths * j.args.n_steps * elem) + align(j.sched.size() * 4) +
                align(j.disc_pow.size() * 8) + align(2ull * j.blocks * 16 * 8) + align(j.blocks * 4ull * 8) +
-               align(8 * 8) + align(64);
+               align(24 * 8) + align(kLsmCounterBytes);
     }
     void* arena = nullptr;
     int st = scratch(ctx, "lsm_arena", bytes, &arena);
@@ -995,14 +995,14 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       a.final_partials = reinterpret_cast<double*>(base + o);
       o += align(j.blocks * 4ull * 8);
       a.out = reinterpret_cast<double*>(base + o);
-      o += align(8 * 8);
-      // counters (64 bytes, zeroed per launch): barrier count and generation
-      // at 0, block-done counter at 16, error code at 32, failed index at 40
+      o += align(24 * 8);
+      // counters (zeroed per launch): arrival count and generation at 0,
+      // block-done counter at 16, error code at 32, failed index at 40
       a.barrier = reinterpret_cast<unsigned*>(base + o);
       a.done = a.barrier + 4;
       a.error = reinterpret_cast<int*>(a.barrier + 8);
       a.diag = reinterpret_cast<unsigned long long*>(a.barrier + 10);
-      MPC_CUDA(ctx, cudaMemsetAsync(a.barrier, 0, 64, ctx->stream));
+      MPC_CUDA(ctx, cudaMemsetAsync(a.barrier, 0, kLsmCounterBytes, ctx->stream));
       a.paths_len = a.n_paths * a.n_steps;
       a.partials_len = 2u * j.blocks * 16u;
       a.final_len = j.blocks * 4u;
