@@ -1774,6 +1774,7 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
   __shared__ double s_beta[4];
   __shared__ int s_ok;
   __shared__ uint32_t s_job;
+  __shared__ double s_red15[kWarps][16];
   __shared__ Real s_disc[512];
   if (threadIdx.x == 0) {
     uint32_t j = 0;
@@ -1828,6 +1829,21 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
     cash[j] = k - s > (Real)0 ? k - s : (Real)0;
   }
   uint32_t regressions = 0;
+  // The path values of a date are loaded one date ahead, before the
+  // cross-block wait of the current date, so their latency hides behind it.
+  Real sv_next[kLsmMaxP];
+  auto load_date = [&](int si_load) {
+    const uint32_t step_load = a.sched[si_load];
+#pragma unroll
+    for (int j = 0; j < kLsmMaxP; ++j) {
+      const uint64_t path = gtid + (uint64_t)j * nthreads;
+      sv_next[j] = (Real)0;
+      if (path >= n || step_load == 0 || step_load > steps) continue;
+      const uint64_t at = (uint64_t)(step_load - 1) * n + path;
+      if (lsm_ok(a, at, a.paths_len, kLsmErrPaths)) sv_next[j] = __ldcg(paths + at);
+    }
+  };
+  if (a.n_sched >= 2) load_date((int)a.n_sched - 2);
   for (int si = (int)a.n_sched - 2; si >= 0; --si) {
     const uint32_t step = a.sched[si];
     if (step == 0 || step > steps) {
@@ -1839,14 +1855,12 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
     for (int i = 0; i < kLsmMom; ++i) m[i] = 0.0;
     Real sv[kLsmMaxP];
 #pragma unroll
+    for (int j = 0; j < kLsmMaxP; ++j) sv[j] = sv_next[j];
+#pragma unroll
     for (int j = 0; j < kLsmMaxP; ++j) {
       const uint64_t path = gtid + (uint64_t)j * nthreads;
-      sv[j] = (Real)0;
       if (path >= n || step == 0 || step > steps) continue;
-      const uint64_t at = (uint64_t)(step - 1) * n + path;
-      if (!lsm_ok(a, at, a.paths_len, kLsmErrPaths)) continue;
-      const Real s = paths[at];
-      sv[j] = s;
+      const Real s = sv[j];
       const Real imm = k - s;
       if (!(imm > (Real)0)) continue;
       if (exd[j] < step || exd[j] > steps) {
@@ -1865,16 +1879,22 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
       for (int r = 0; r < 4; ++r) m[10 + r] += (double)(b[r] * cont);
       m[14] += 1.0;
     }
-    // block reduction of the 15 moments in three rounds of five
+    // block reduction of the 15 moments: warp sums, then one thread per
+    // moment folds the warps in order (the order of block_reduce5)
     const uint64_t part_at = ((uint64_t)buf * nb + lb) * 16;
-    double* part = a.partials + part_at;
-    for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
-      double v[5] = {m[r0], m[r0 + 1], m[r0 + 2], m[r0 + 3], m[r0 + 4]};
-      block_reduce5(v, red);
-      if (threadIdx.x == 0 && lsm_ok(a, part_at + r0 + 4, a.partials_len, kLsmErrPartials))
-        for (int i = 0; i < 5; ++i) part[r0 + i] = v[i];
-      __syncthreads();
+#pragma unroll
+    for (int i = 0; i < kLsmMom; ++i) {
+      const double w = warp_sum(m[i]);
+      if ((threadIdx.x & 31) == 0) s_red15[threadIdx.x >> 5][i] = w;
     }
+    __syncthreads();
+    if (threadIdx.x < (uint32_t)kLsmMom) {
+      double t = 0.0;
+      for (int w = 0; w < kWarps; ++w) t += s_red15[w][threadIdx.x];
+      if (lsm_ok(a, part_at + threadIdx.x, a.partials_len, kLsmErrPartials)) a.partials[part_at + threadIdx.x] = t;
+      __threadfence();
+    }
+    if (si > 0) load_date(si - 1);  // next date's values, in flight during the wait
     // The last block to arrive sums the block partials in block order, solves
     // the normal equations once and publishes the coefficients; the others
     // wait (bounded) for the publication and read 5 doubles.
