@@ -1681,7 +1681,7 @@ __device__ __forceinline__ bool lsm_ok(const LsmArgs& a, uint64_t index, uint64_
 // of the job leaves at its next check.  Returns false when the job's error
 // flag is set.
 __device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint32_t nb, int coeffs,
-                                                 double (*red)[5], double* s_mom, double* s_beta, int* s_ok) {
+                                                 double* fold, double* s_mom, double* s_beta, int* s_ok) {
   __shared__ int s_last, s_good;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1708,21 +1708,21 @@ __device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint
   double* pub = a.out + 8 + 5 * buf;  // published (ok, beta0..3) of this date
   if (s_last) {
     __threadfence();
-    double acc[kLsmMom];
-#pragma unroll
-    for (int i = 0; i < kLsmMom; ++i) acc[i] = 0.0;
+    // thread t sums moment t % 16 over blocks t / 16, t / 16 + 16, ... (all
+    // loads independent), then one thread per moment folds the 16 lanes in
+    // order: a fixed order, the same on every call
     const uint64_t base_at = (uint64_t)buf * nb * 16;
-    const double* base = a.partials + base_at;
-    for (uint32_t blk = threadIdx.x; blk < nb; blk += blockDim.x) {
-      if (!lsm_ok(a, base_at + (uint64_t)blk * 16 + kLsmMom - 1, a.partials_len, kLsmErrPartials)) break;
-#pragma unroll
-      for (int i = 0; i < kLsmMom; ++i) acc[i] += __ldcg(base + (size_t)blk * 16 + i);
-    }
-    for (int r0 = 0; r0 < kLsmMom; r0 += 5) {
-      double v[5] = {acc[r0], acc[r0 + 1], acc[r0 + 2], acc[r0 + 3], acc[r0 + 4]};
-      block_reduce5(v, red);
-      if (threadIdx.x == 0)
-        for (int i = 0; i < 5; ++i) s_mom[r0 + i] = v[i];
+    const uint32_t mom = threadIdx.x & 15u, lane_grp = threadIdx.x >> 4, n_grp = blockDim.x >> 4;
+    double acc = 0.0;
+    if (mom < (uint32_t)kLsmMom && lsm_ok(a, base_at + (uint64_t)nb * 16 - 1, a.partials_len, kLsmErrPartials))
+      for (uint32_t blk = lane_grp; blk < nb; blk += n_grp) acc += __ldcg(a.partials + base_at + (size_t)blk * 16 + mom);
+    __syncthreads();
+    fold[lane_grp * 16 + mom] = acc;
+    __syncthreads();
+    if (threadIdx.x < (uint32_t)kLsmMom) {
+      double t = 0.0;
+      for (uint32_t g = 0; g < n_grp; ++g) t += fold[g * 16 + threadIdx.x];
+      s_mom[threadIdx.x] = t;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1775,6 +1775,7 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
   __shared__ int s_ok;
   __shared__ uint32_t s_job;
   __shared__ double s_red15[kWarps][16];
+  __shared__ double s_fold[kLsmBlock];  // 16 lanes x 16 moments of the last block's fold
   __shared__ Real s_disc[512];
   if (threadIdx.x == 0) {
     uint32_t j = 0;
@@ -1898,7 +1899,7 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
     // The last block to arrive sums the block partials in block order, solves
     // the normal equations once and publishes the coefficients; the others
     // wait (bounded) for the publication and read 5 doubles.
-    if (!lsm_gather_solve(a, buf, nb, coeffs, red, s_mom, s_beta, &s_ok)) return;
+    if (!lsm_gather_solve(a, buf, nb, coeffs, s_fold, s_mom, s_beta, &s_ok)) return;
     if (s_ok) {
       ++regressions;
       const Real b0 = (Real)s_beta[0], b1 = (Real)s_beta[1], b2 = (Real)s_beta[2], b3 = (Real)s_beta[3];
