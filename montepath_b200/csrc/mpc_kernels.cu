@@ -685,37 +685,42 @@ __device__ __forceinline__ void unit_merton(const DevReq& q, Src& src, double& p
   ctl = (double)(st * disc);
 }
 
-// d-asset basket, terminal or stepwise (basket_terminal_payoff, cpu.rs:7616-7635).
-template <class Real, class Src>
-__device__ __forceinline__ void unit_basket(const DevReq& q, Src& src, double& pay, double& ctl) {
-  const uint32_t d = q.n_assets, n = q.n_steps;
+// d-asset basket, terminal or stepwise (basket_terminal_payoff, cpu.rs:7616-7635),
+// for a compile-time asset count D: the Cholesky factor and per-asset step
+// constants are converted to Real once per unit and kept in registers, and
+// every asset loop unrolls without predicates.
+template <class Real, int D, class Src>
+__device__ __forceinline__ void unit_basket_d(const DevReq& q, Src& src, double& pay, double& ctl) {
+  const uint32_t n = q.n_steps;
   const bool anti = q.anti != 0;
-  Real x0[8], x1[8];
+  Real L[D][D], dr[D], vo[D], x0[D], x1[D];
 #pragma unroll
-  for (int a = 0; a < 8; ++a) x0[a] = x1[a] = (Real)0;
+  for (int a = 0; a < D; ++a) {
+    dr[a] = (Real)q.b_drift[a];
+    vo[a] = (Real)q.b_vol[a];
+    x0[a] = x1[a] = (Real)0;
+#pragma unroll
+    for (int b = 0; b <= a; ++b) L[a][b] = (Real)q.chol[a * D + b];
+  }
   uint32_t dim = 0;
   for (uint32_t s = 0; s < n; ++s) {
-    Real z[8];
-    src.at_step(dim, d);
+    Real z[D];
+    src.at_step(dim, D);
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
-      if (a < (int)d) z[a] = normal<Real>(src, dim++);
+    for (int a = 0; a < D; ++a) z[a] = normal<Real>(src, dim + a);
+    dim += D;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      if (a >= (int)d) break;
+    for (int a = 0; a < D; ++a) {
       Real zc = (Real)0;
 #pragma unroll
-      for (int b = 0; b < 8; ++b)
-        if (b <= a) zc += (Real)q.chol[a * d + b] * z[b];
-      const Real dr = (Real)q.b_drift[a], vo = (Real)q.b_vol[a];
-      x0[a] += dr + vo * zc;
-      if (anti) x1[a] += dr + vo * (-zc);
+      for (int b = 0; b <= a; ++b) zc += L[a][b] * z[b];
+      x0[a] += dr[a] + vo[a] * zc;
+      if (anti) x1[a] += dr[a] + vo[a] * (-zc);
     }
   }
   Real b0 = 0, b1 = 0;
 #pragma unroll
-  for (int a = 0; a < 8; ++a) {
-    if (a >= (int)d) break;
+  for (int a = 0; a < D; ++a) {
     b0 += (Real)q.weights[a] * ((Real)q.spots[a] * ex<Real>(x0[a]));
     if (anti) b1 += (Real)q.weights[a] * ((Real)q.spots[a] * ex<Real>(x1[a]));
   }
@@ -728,6 +733,36 @@ __device__ __forceinline__ void unit_basket(const DevReq& q, Src& src, double& p
     pay = (double)p;
   }
   ctl = (double)(b0 * disc);
+}
+
+template <class Real, class Src>
+__device__ __forceinline__ void unit_basket(const DevReq& q, Src& src, double& pay, double& ctl) {
+  switch (q.n_assets) {
+    case 1:
+      unit_basket_d<Real, 1>(q, src, pay, ctl);
+      break;
+    case 2:
+      unit_basket_d<Real, 2>(q, src, pay, ctl);
+      break;
+    case 3:
+      unit_basket_d<Real, 3>(q, src, pay, ctl);
+      break;
+    case 4:
+      unit_basket_d<Real, 4>(q, src, pay, ctl);
+      break;
+    case 5:
+      unit_basket_d<Real, 5>(q, src, pay, ctl);
+      break;
+    case 6:
+      unit_basket_d<Real, 6>(q, src, pay, ctl);
+      break;
+    case 7:
+      unit_basket_d<Real, 7>(q, src, pay, ctl);
+      break;
+    default:
+      unit_basket_d<Real, 8>(q, src, pay, ctl);
+      break;
+  }
 }
 
 // Coupled MLMC level of the arithmetic Asian (cpu.rs:6641-6894): level 0 is
