@@ -267,8 +267,10 @@ __device__ __forceinline__ float sobol_unit_f32(uint32_t x) {
 }
 // The same value assembled from bits: 1 + (x >> 9) 2^-23 in [1, 2) minus
 // (1 - 2^-24); the difference is exact (Sterbenz), so no conversion is needed.
+// (x >> 9) has no bit in common with the exponent, so + equals | here and
+// lets the shift and the add issue as one instruction.
 __device__ __forceinline__ float sobol_unit_f32_bits(uint32_t x) {
-  return __fsub_rn(__int_as_float((x >> 9) | 0x3F800000u), 0.99999994f);
+  return __fsub_rn(__int_as_float((x >> 9) + 0x3F800000u), 0.99999994f);
 }
 __device__ __forceinline__ double sobol_unit_f64(uint32_t x) {
   return ((double)(x >> 9) + 0.5) * 1.1920928955078125e-07;

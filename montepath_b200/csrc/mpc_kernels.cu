@@ -70,6 +70,22 @@ __device__ __forceinline__ float icdf_segments(const float4* __restrict__ seg, f
   const float p = fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x);
   return u < 0.5f ? p : -p;
 }
+// icdf_segments(seg, sobol_unit_f32_bits(x)) from the Sobol sample's bits.
+// With m = x >> 9 the uniform is u = (m + 0.5) 2^-23, and its mirror 1 - u
+// is the same expression of the 23-bit complement of m, so
+// v = min(u, 1 - u) is built from x ^ (x >> 31, arithmetic): the complement
+// exactly when bit 31 (u > 1/2) is set, which also gives the result's sign.
+// Equal bit for bit to the two-step form, with no compare or select.
+__device__ __forceinline__ float icdf_sobol_bits(const float4* __restrict__ seg, uint32_t x) {
+  const uint32_t xm = x ^ (uint32_t)((int32_t)x >> 31);
+  const float v = __fsub_rn(__uint_as_float((xm >> 9) + 0x3F800000u), 0.99999994f);
+  const uint32_t bits = __float_as_uint(v);
+  const uint32_t idx = (bits >> 18) - (103u << 5);
+  const float t = __int_as_float(((bits << 5) & 0x7FFFFFu) | 0x3F800000u) - 1.0f;
+  const float4 c = seg[idx];
+  const float p = fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x);
+  return __uint_as_float(__float_as_uint(p) ^ (x & 0x80000000u));
+}
 
 // ------------------------------------------------------------- sources ----
 // A Source yields the samples of one unit (path or antithetic pair) by
@@ -221,6 +237,7 @@ struct SobolQuad {
   const float4* icdf;           // inverse-normal segments in shared memory
   uint32_t win_first;           // first dimension in the window (multiple of 4)
   uint32_t local, block_seed, group, seed_g, combine_g, quad;
+  uint32_t qbase;               // (quad's first dimension mod 256) + combine_g
   uint32_t rows[8];             // window word offset of this point's row per nibble position
   uint32_t x0, x1, x2, x3;      // reversed products of the dimensions of `quad`
   template <bool FP64>
@@ -269,6 +286,7 @@ struct SobolQuad {
       combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
     }
     quad = d0 >> 2;
+    qbase = (d0 & (MPC_SOBOL_TABLE_DIMS - 1)) + combine_g;
     const uint32_t* base = win + (d0 - win_first);
     uint4 a = *reinterpret_cast<const uint4*>(base + rows[0]);
 #pragma unroll
@@ -284,13 +302,15 @@ struct SobolQuad {
     x2 = a.z;
     x3 = a.w;
   }
-  // Scrambled value of dimension d0 + K of the quad loaded at d0.
+  // Scrambled value of dimension d (any dimension of the loaded quad).
   __device__ __forceinline__ uint32_t scramble(uint32_t xr, uint32_t d) const {
     return __brev(lk_permute(xr, seed_g ^ ((d & (MPC_SOBOL_TABLE_DIMS - 1)) + combine_g)));
   }
+  // Scrambled value of dimension d0 + K of the quad loaded at d0 (d0 is a
+  // multiple of 4, so (d0 + K) mod 256 + combine_g = qbase + K).
   template <int K>
-  __device__ __forceinline__ uint32_t take(uint32_t d0) const {
-    return scramble(K == 0 ? x0 : K == 1 ? x1 : K == 2 ? x2 : x3, d0 + K);
+  __device__ __forceinline__ uint32_t take(uint32_t) const {
+    return __brev(lk_permute(K == 0 ? x0 : K == 1 ? x1 : K == 2 ? x2 : x3, seed_g ^ (qbase + K)));
   }
   template <int K>
   __device__ __forceinline__ float take_u(uint32_t d0) const {
@@ -298,7 +318,7 @@ struct SobolQuad {
   }
   template <int K>
   __device__ __forceinline__ float take_n(uint32_t d0) const {
-    return icdf_segments(icdf, take_u<K>(d0));
+    return icdf_sobol_bits(icdf, take<K>(d0));
   }
   __device__ __forceinline__ uint32_t sample(uint32_t d) {
     if ((d >> 2) != quad) quad_load(d & ~3u);
@@ -306,7 +326,7 @@ struct SobolQuad {
     return scramble((k & 2u) ? ((k & 1u) ? x3 : x2) : ((k & 1u) ? x1 : x0), d);
   }
   __device__ __forceinline__ float u32(uint32_t d) { return sobol_unit_f32_bits(sample(d)); }
-  __device__ __forceinline__ float n32(uint32_t d) { return icdf_segments(icdf, u32(d)); }
+  __device__ __forceinline__ float n32(uint32_t d) { return icdf_sobol_bits(icdf, sample(d)); }
   __device__ __forceinline__ double u64(uint32_t d) { return sobol_unit_f64(sample(d)); }
   __device__ __forceinline__ double n64(uint32_t d) { return icdf_f64(u64(d)); }
 };
