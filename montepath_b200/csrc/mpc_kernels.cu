@@ -86,6 +86,24 @@ __device__ __forceinline__ float icdf_sobol_bits(const float4* __restrict__ seg,
   const float p = fmaf(fmaf(fmaf(c.w, t, c.z), t, c.y), t, c.x);
   return __uint_as_float(__float_as_uint(p) ^ (x & 0x80000000u));
 }
+// Two samples at once: the floating-point steps as packed FP32 pairs
+// (FADD2 / FFMA2, each lane rounded exactly as the scalar operation), so the
+// pair equals two icdf_sobol_bits calls bit for bit.
+__device__ __forceinline__ float2 icdf_sobol_bits2(const float4* __restrict__ seg, uint32_t xa, uint32_t xb) {
+  const uint32_t ma = xa ^ (uint32_t)((int32_t)xa >> 31), mb = xb ^ (uint32_t)((int32_t)xb >> 31);
+  const float2 v = __fadd2_rn(make_float2(__uint_as_float((ma >> 9) + 0x3F800000u), __uint_as_float((mb >> 9) + 0x3F800000u)),
+                              make_float2(-0.99999994f, -0.99999994f));
+  const uint32_t ba = __float_as_uint(v.x), bb = __float_as_uint(v.y);
+  const float4 ca = seg[(ba >> 18) - (103u << 5)], cb = seg[(bb >> 18) - (103u << 5)];
+  const float2 t = __fadd2_rn(make_float2(__int_as_float(((ba << 5) & 0x7FFFFFu) | 0x3F800000u),
+                                          __int_as_float(((bb << 5) & 0x7FFFFFu) | 0x3F800000u)),
+                              make_float2(-1.0f, -1.0f));
+  float2 p = __ffma2_rn(make_float2(ca.w, cb.w), t, make_float2(ca.z, cb.z));
+  p = __ffma2_rn(p, t, make_float2(ca.y, cb.y));
+  p = __ffma2_rn(p, t, make_float2(ca.x, cb.x));
+  return make_float2(__uint_as_float(__float_as_uint(p.x) ^ (xa & 0x80000000u)),
+                     __uint_as_float(__float_as_uint(p.y) ^ (xb & 0x80000000u)));
+}
 
 // ------------------------------------------------------------- sources ----
 // A Source yields the samples of one unit (path or antithetic pair) by
@@ -320,6 +338,10 @@ struct SobolQuad {
   __device__ __forceinline__ float take_n(uint32_t d0) const {
     return icdf_sobol_bits(icdf, take<K>(d0));
   }
+  template <int K0, int K1>
+  __device__ __forceinline__ float2 take_n2(uint32_t d0) const {
+    return icdf_sobol_bits2(icdf, take<K0>(d0), take<K1>(d0));
+  }
   __device__ __forceinline__ uint32_t sample(uint32_t d) {
     if ((d >> 2) != quad) quad_load(d & ~3u);
     const uint32_t k = d & 3u;
@@ -537,10 +559,11 @@ __device__ __forceinline__ void unit_gbm_step(const DevReq& q, Src& src, double&
     for (; s + 4 <= n; s += 4) {  // four steps per quad of dimensions
       src.at_step(s, 4);
       src.quad_load(s);
-      advance(src.template take_n<0>(s));
-      advance(src.template take_n<1>(s));
-      advance(src.template take_n<2>(s));
-      advance(src.template take_n<3>(s));
+      const float2 z01 = src.template take_n2<0, 1>(s), z23 = src.template take_n2<2, 3>(s);
+      advance(z01.x);
+      advance(z01.y);
+      advance(z23.x);
+      advance(z23.y);
     }
   }
   for (; s < n; ++s) {
@@ -623,8 +646,9 @@ __device__ __forceinline__ void unit_heston(const DevReq& q, Src& src, double& p
       const uint32_t d0 = 2 * s;
       src.at_step(d0, 4);
       src.quad_load(d0);
-      step(src.template take_n<0>(d0), src.template take_n<1>(d0));
-      step(src.template take_n<2>(d0), src.template take_n<3>(d0));
+      const float2 z01 = src.template take_n2<0, 1>(d0), z23 = src.template take_n2<2, 3>(d0);
+      step(z01.x, z01.y);
+      step(z23.x, z23.y);
     }
   }
   for (; s < n; ++s) {
