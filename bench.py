@@ -21,6 +21,7 @@ exchange, so there is no data-path collective.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -48,6 +49,11 @@ MERTON = dict(model="merton", method="stepwise", s0=100.0, k=100.0, r=0.03, sigm
 # Merton step 4 flops (+ the Sobol uniform of the Poisson dimension, no inverse CDF).
 FLOPS_PER_STEP = {"heston": 2 * 24 + 16, "merton": 24 + 4}
 SFU_PER_STEP = {"heston": 2 * 1 + 1, "merton": 1}
+# Warp instructions the two fused kernels issue per 32 path-steps
+# (smsp__inst_executed.sum of the quarter-size ncu capture in profiles/): the
+# kernels are issue-bound, so this gives the fraction of the SMs' issue slots
+# (4 warp instructions per cycle per SM) the measured rate uses.
+WARP_INSTR_PER_32_STEPS = {"heston": 109.5, "merton": 103.4}
 
 
 def requests(precision: str):
@@ -236,6 +242,7 @@ def run_reference(args) -> None:
 
 def run_ours(args) -> None:
     rank, world, local, pg = dist_setup(args.gpus)
+    from montepath_b200 import abi
     from montepath_b200.backend import CudaBackend
 
     backend = CudaBackend(local)
@@ -296,6 +303,12 @@ def run_ours(args) -> None:
     fr_fp32 = flops / 1e12 / fp32_peak if fp32_peak else None
     fr_sfu = sfu / 1e12 / sfu_peak if sfu_peak else None
     traffic = load_traffic().get("fused_heston_merton_sobol", {}).get("bytes_per_step")
+    fr_issue = None
+    info = abi.DeviceInfo()
+    sm_mhz = clock_info.get("sm_mhz") or clock_info.get("sm_max_mhz")
+    if backend.lib.mpc_device_info(local, ctypes.byref(info)) == abi.OK and sm_mhz:
+        warp_instr = sum(WARP_INSTR_PER_32_STEPS.values()) / 32.0 * (per_rank_rate / 2)
+        fr_issue = warp_instr / (info.sm_count * 4 * sm_mhz * 1e6)
     bound, achieved, peak, unit, frac = "fp32", flops / 1e12, fp32_peak, "TFLOP/s", fr_fp32
     if fr_sfu is not None and fr_fp32 is not None and fr_sfu > fr_fp32:
         bound, achieved, peak, unit, frac = "sfu", sfu / 1e12, sfu_peak, "Tops/s", fr_sfu
@@ -337,7 +350,7 @@ def run_ours(args) -> None:
                 "unit": unit,
                 "frac": frac,
                 "traffic": traffic,
-                "fractions": {"fp32": fr_fp32, "sfu": fr_sfu},
+                "fractions": {"fp32": fr_fp32, "sfu": fr_sfu, "issue": fr_issue},
                 "peak_source": "measured by mpc_measure_peaks on this GPU (FP32 FMA chains / MUFU ex2 chains)",
                 "hbm_peak_gbs": load_peaks().get("hbm_gbs"),
             },

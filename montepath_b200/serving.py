@@ -76,4 +76,8 @@ def replay(backend: CudaBackend, stream: Sequence[tuple[float, str, abi.Request]
         "peak_bytes": stats.peak_bytes,
         "mlmc_target_met": sum(1 for k, _, r in results if k == "asian_mlmc" and r.target_met),
         "mlmc_requests": sum(1 for k, _, _ in results if k == "asian_mlmc"),
+        # requests whose allocation the step-update cap cut (cpu.rs:3390-3403), and the
+        # standard error they reached instead of the target
+        "mlmc_step_cap_hit": sum(1 for k, _, r in results if k == "asian_mlmc" and r.max_step_updates_hit),
+        "mlmc_stderr_p50": pct(sorted(r.stderr for k, _, r in results if k == "asian_mlmc"), 0.5),
     }
