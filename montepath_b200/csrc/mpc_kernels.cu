@@ -1750,97 +1750,85 @@ __device__ __forceinline__ bool lsm_ok(const LsmArgs& a, uint64_t index, uint64_
   return false;
 }
 
-// One exercise date's regression across the job's blocks.  Every block has
-// written its 15 moments to partials[buf][lb]; thread 0 takes a ticket; the
-// block with the last ticket sums all partials in block order (strided per
-// thread, then the fixed block tree), solves, writes (ok, beta) to
-// out[8 + 5 buf ..] and bumps the generation; the other blocks spin until the
-// generation moves and then read the published coefficients.  The spin is
-// bounded: after timeout_ns the block records kLsmErrTimeout and every block
-// of the job leaves at its next check.  Returns false when the job's error
-// flag is set.
-__device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint32_t nb, int coeffs,
+// One exercise date's regression across the job's blocks (round = the date's
+// position in the backward pass).  Every block has written its 15 moments to
+// partials[buf][lb]; thread 0 adds one to the job's arrival count, which the
+// host zeroes before the launch and which only grows, and waits until it
+// reaches nb (round + 1).  Then every block sums the partials itself in the
+// same fixed order (thread t: moment t % 16 over blocks t / 16, t / 16 + 16,
+// ...; then one thread per moment over the 16 lanes) and solves the normal
+// equations in thread 0: the same operations on the same data, so every block
+// holds the same coefficients, with no publication round trip after the
+// solve (~35 KB of L2 reads per block and date instead).  The partials of
+// date round + 1 go to the other buffer, and no block writes this buffer
+// again before every block has arrived at round + 1, i.e. finished reading
+// it.  The wait is bounded: after timeout_ns the block records
+// kLsmErrTimeout and every block of the job leaves at its next check.
+// Returns false when the job's error flag is set.
+__device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint32_t nb, uint32_t round, int coeffs,
                                                  double* fold, double* s_mom, double* s_beta, int* s_ok) {
-  __shared__ int s_last, s_good;
+  __shared__ int s_good;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* gen = a.barrier + 1;
-    const unsigned g = *gen;
+    const unsigned target = nb * (round + 1u);
     __threadfence();
-    s_last = atomicAdd(a.barrier, 1u) == nb - 1 ? 1 : 0;
-    s_good = 1;
-    if (!s_last) {
+    if (atomicAdd(a.barrier, 1u) + 1u != target) {
+      volatile unsigned* count = a.barrier;
       const uint64_t start = global_ns();
-      while (*gen == g) {
+      while (*count < target) {
         if (*((volatile int*)a.error) != 0) break;
         if (global_ns() - start > a.timeout_ns) {
           atomicCAS(a.error, 0, kLsmErrTimeout);
           break;
         }
       }
-      __threadfence();
-      s_good = *((volatile int*)a.error) == 0;
     }
+    __threadfence();
+    s_good = *((volatile int*)a.error) == 0;
   }
   __syncthreads();
   if (!s_good) return false;
-  double* pub = a.out + 8 + 5 * buf;  // published (ok, beta0..3) of this date
-  if (s_last) {
-    __threadfence();
-    // thread t sums moment t % 16 over blocks t / 16, t / 16 + 16, ... (all
-    // loads independent), then one thread per moment folds the 16 lanes in
-    // order: a fixed order, the same on every call
-    const uint64_t base_at = (uint64_t)buf * nb * 16;
-    const uint32_t mom = threadIdx.x & 15u, lane_grp = threadIdx.x >> 4, n_grp = blockDim.x >> 4;
-    double acc = 0.0;
-    if (mom < (uint32_t)kLsmMom && lsm_ok(a, base_at + (uint64_t)nb * 16 - 1, a.partials_len, kLsmErrPartials))
-      for (uint32_t blk = lane_grp; blk < nb; blk += n_grp) acc += __ldcg(a.partials + base_at + (size_t)blk * 16 + mom);
-    __syncthreads();
-    fold[lane_grp * 16 + mom] = acc;
-    __syncthreads();
-    if (threadIdx.x < (uint32_t)kLsmMom) {
-      double t = 0.0;
-      for (uint32_t g = 0; g < n_grp; ++g) t += fold[g * 16 + threadIdx.x];
-      s_mom[threadIdx.x] = t;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double ata[4][4], atb[4];
-      int idx = 0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = r; c < 4; ++c) {
-          ata[r][c] = s_mom[idx];
-          ata[c][r] = s_mom[idx];
-          ++idx;
-        }
-#pragma unroll
-      for (int r = 0; r < 4; ++r) atb[r] = s_mom[10 + r];
-      // the reference zeroes rows/columns beyond the basis degree
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        if (r < coeffs) continue;
-        atb[r] = 0.0;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) ata[r][c] = ata[c][r] = 0.0;
-      }
-      int ok = s_mom[14] >= (double)coeffs ? 1 : 0;
-      if (ok) ok = (coeffs == 2 ? solve_fixed<2>(ata, atb) : coeffs == 3 ? solve_fixed<3>(ata, atb) : solve_fixed<4>(ata, atb)) ? 1 : 0;
-      pub[0] = ok ? 1.0 : 0.0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r) pub[1 + r] = (ok && r < coeffs) ? atb[r] : 0.0;
-      __threadfence();
-      atomicExch(a.barrier, 0u);
-      __threadfence();
-      atomicAdd(a.barrier + 1, 1u);  // release the waiting blocks
-    }
+  const uint64_t base_at = (uint64_t)buf * nb * 16;
+  const uint32_t mom = threadIdx.x & 15u, lane_grp = threadIdx.x >> 4, n_grp = blockDim.x >> 4;
+  double acc = 0.0;
+  if (mom < (uint32_t)kLsmMom && lsm_ok(a, base_at + (uint64_t)nb * 16 - 1, a.partials_len, kLsmErrPartials)) {
+#pragma unroll 4
+    for (uint32_t blk = lane_grp; blk < nb; blk += n_grp) acc += __ldcg(a.partials + base_at + (size_t)blk * 16 + mom);
   }
+  fold[lane_grp * 16 + mom] = acc;
+  __syncthreads();
+  if (threadIdx.x < (uint32_t)kLsmMom) {
+    double t = 0.0;
+    for (uint32_t g = 0; g < n_grp; ++g) t += fold[g * 16 + threadIdx.x];
+    s_mom[threadIdx.x] = t;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    __threadfence();
-    const double ok = __ldcg(pub);
-    for (int r = 0; r < 4; ++r) s_beta[r] = __ldcg(pub + 1 + r);
-    *s_ok = ok != 0.0 ? 1 : 0;
+    double ata[4][4], atb[4];
+    int idx = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = r; c < 4; ++c) {
+        ata[r][c] = s_mom[idx];
+        ata[c][r] = s_mom[idx];
+        ++idx;
+      }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) atb[r] = s_mom[10 + r];
+    // the reference zeroes rows/columns beyond the basis degree
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (r < coeffs) continue;
+      atb[r] = 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) ata[r][c] = ata[c][r] = 0.0;
+    }
+    int ok = s_mom[14] >= (double)coeffs ? 1 : 0;
+    if (ok) ok = (coeffs == 2 ? solve_fixed<2>(ata, atb) : coeffs == 3 ? solve_fixed<3>(ata, atb) : solve_fixed<4>(ata, atb)) ? 1 : 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) s_beta[r] = (ok && r < coeffs) ? atb[r] : 0.0;
+    *s_ok = ok;
   }
   __syncthreads();
   return true;
@@ -1908,7 +1896,7 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
     }
     cash[j] = k - s > (Real)0 ? k - s : (Real)0;
   }
-  uint32_t regressions = 0;
+  uint32_t regressions = 0, round = 0;
   // The path values of a date are loaded one date ahead, before the
   // cross-block wait of the current date, so their latency hides behind it.
   Real sv_next[kLsmMaxP];
@@ -1975,10 +1963,9 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
       __threadfence();
     }
     if (si > 0) load_date(si - 1);  // next date's values, in flight during the wait
-    // The last block to arrive sums the block partials in block order, solves
-    // the normal equations once and publishes the coefficients; the others
-    // wait (bounded) for the publication and read 5 doubles.
-    if (!lsm_gather_solve(a, buf, nb, coeffs, s_fold, s_mom, s_beta, &s_ok)) return;
+    // Every block waits (bounded) for all blocks' partials of this date, then
+    // sums them in block order and solves the normal equations itself.
+    if (!lsm_gather_solve(a, buf, nb, round++, coeffs, s_fold, s_mom, s_beta, &s_ok)) return;
     if (s_ok) {
       ++regressions;
       const Real b0 = (Real)s_beta[0], b1 = (Real)s_beta[1], b2 = (Real)s_beta[2], b3 = (Real)s_beta[3];

@@ -46,9 +46,8 @@ struct LsmArgs {
   void* paths;               // [n_steps][n_paths] float or double
   double* partials;          // [2][grid][16]
   double* final_partials;    // [grid][4]
-  double* out;               // [24]: n, sum, sumsq, early, maturity, regressions, -, -; then per date
-                             // parity two published (ok, beta0..3) of the regression
-  unsigned* barrier;         // counter area (kLsmCounterBytes): arrival count, generation, ...
+  double* out;               // [8]: n, sum, sumsq, early, maturity, regressions, -, -
+  unsigned* barrier;         // counter area (kLsmCounterBytes): arrival count (all dates), ...
   unsigned* done;            // last-block counter
   int* error;                // first failure: kLsmErr* code (0 = none)
   unsigned long long* diag;  // offending index of a failed self-check
