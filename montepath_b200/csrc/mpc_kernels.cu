@@ -1834,14 +1834,17 @@ __device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint
   return true;
 }
 
+// One 512-thread block per SM: the same warps per SM as two 256-thread
+// blocks, but half the block partials to fold and arrivals to count per date
+// (the per-date cross-block round is this kernel's critical path).
 template <class Real, int SMP>
-__global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __restrict__ jobs, uint32_t n_jobs, SrcCtx ctx) {
-  __shared__ double red[kWarps][5];
+__global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __restrict__ jobs, uint32_t n_jobs, SrcCtx ctx) {
+  __shared__ double red[kLsmBlock / 32][5];
   __shared__ double s_mom[16];
   __shared__ double s_beta[4];
   __shared__ int s_ok;
   __shared__ uint32_t s_job;
-  __shared__ double s_red15[kWarps][16];
+  __shared__ double s_red15[kLsmBlock / 32][16];
   __shared__ double s_fold[kLsmBlock];  // 16 lanes x 16 moments of the last block's fold
   __shared__ Real s_disc[512];
   if (threadIdx.x == 0) {
@@ -1958,7 +1961,7 @@ __global__ void __launch_bounds__(kLsmBlock, 2) lsm_kernel(const LsmArgs* __rest
     __syncthreads();
     if (threadIdx.x < (uint32_t)kLsmMom) {
       double t = 0.0;
-      for (int w = 0; w < kWarps; ++w) t += s_red15[w][threadIdx.x];
+      for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red15[w][threadIdx.x];
       if (lsm_ok(a, part_at + threadIdx.x, a.partials_len, kLsmErrPartials)) a.partials[part_at + threadIdx.x] = t;
       __threadfence();
     }

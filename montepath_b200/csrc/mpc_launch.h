@@ -80,7 +80,7 @@ cudaError_t launch_lsm_batch(const LsmArgs* d_jobs, uint32_t n_jobs, uint32_t to
 // Co-resident LSM blocks on the device for (fp64, sampler); 0 if the kernel cannot launch.
 uint32_t lsm_capacity(int fp64, int sampler);
 constexpr uint32_t kLsmPathsPerThreadMax = 8;
-constexpr uint32_t kLsmThreads = 256;
+constexpr uint32_t kLsmThreads = 512;
 // Counter area of an LSM job (zeroed per launch).
 constexpr size_t kLsmCounterBytes = 64;
 

@@ -918,7 +918,8 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     const uint64_t need = (r.n_paths + per_block_max - 1) / per_block_max;
     if (cap == 0 || need > cap)
       return fail(ctx, MPC_E_UNSUPPORTED, "LSM path count exceeds the co-resident capacity of the device");
-    // about four paths per thread, at most two blocks per SM for one job
+    // about four paths per thread, at most one block per SM for one job (the
+    // capacity is one 512-thread block per SM)
     uint64_t want = (r.n_paths + 4 * kLsmThreads - 1) / (4 * kLsmThreads);
     want = std::min<uint64_t>(want, std::min<uint64_t>(cap, 2ull * uint64_t(ctx->sm_count)));
     j.blocks = uint32_t(std::max<uint64_t>(need, want));
@@ -1514,8 +1515,8 @@ const RateRow kRateMertonStep = {{1.05e11, 1.05e11, 1.97e11, 4.30e10}, {4.16e10,
 const RateRow kRateMertonTerminal = {{1.70e10, 1.70e10, 1.44e10, 7.09e9}, {1.83e10, 1.83e10, 1.30e10, 6.60e9}};
 const RateRow kRateBasket2 = {{5.46e9, 1.53e10, 1.28e10, 7.74e9}, {5.49e9, 1.58e10, 1.13e10, 6.77e9}};
 const double kRateBridge[2] = {1.41e11, 4.59e10};  // GBM stepwise through the bridge, fp32 / fp64
-const double kLsmFixedMs = 0.46, kLsmRate = 6.4e10; // 49 cross-block date rounds, then path-steps
-                                                      // (fit to 200,000 and 524,288 paths x 50 dates)
+const double kLsmFixedMs = 0.28, kLsmRate = 6.4e10; // 49 cross-block date rounds, then path-steps
+                                                      // (fit to 524,288 paths x 50 dates)
 const double kCallOverheadMs = 0.035;               // events, copies, one launch
 const double kFirstCallMs = 2.0;                    // tables and buffers of a new shape
 
