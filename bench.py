@@ -370,7 +370,10 @@ def run_ours(args) -> None:
         if legs:
             line["configs"] = {}
             for leg in legs:
-                line["configs"][leg] = LEGS[leg](backend)
+                if leg == "config4":
+                    line["configs"][leg] = leg_config4(backend, args.book_contracts)
+                else:
+                    line["configs"][leg] = LEGS[leg](backend)
         if not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -433,15 +436,16 @@ def leg_config3(backend) -> dict:
     return out
 
 
-def leg_config4(backend) -> dict:
+def leg_config4(backend, contracts: int = 4096) -> dict:
     """4,096-contract heterogeneous book in one batched launch vs plain FP64
     per-request launches (timed on every 63rd contract, which cycles through
-    the four contract kinds, and extrapolated by path-steps)."""
+    the four contract kinds, and extrapolated by path-steps).  `contracts`
+    takes the first contracts of the same book (smaller profiling cases)."""
 
     from montepath_b200 import workloads
     from montepath_b200.requests import copy_request
 
-    book = workloads.book(42)
+    book = workloads.book(42)[:contracts]
     total = workloads.book_path_steps(book)
     backend.price_batch(book)
     res, ms = _timed(backend, lambda: backend.price_batch(book))
@@ -490,6 +494,8 @@ def main() -> None:
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain comparison of the headline")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling cases)")
     ap.add_argument("--legs", default="all", help="comma list of config1,config3,config4,config5, all or none")
+    ap.add_argument("--book-contracts", type=int, default=4096,
+                    help="first contracts of the book in the config4 leg (profiling cases)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
