@@ -355,7 +355,8 @@ struct SobolQuad {
 
 // Counter-hash normals for the fused kernels: the reference's u32 hashes
 // with the short FP32 transform (counter_normal_fast).
-struct CounterFast {
+template <bool HWCOS>
+struct CounterFastT {
   uint32_t seed, unit;
   template <bool FP64>
   __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx&, uint64_t u) {
@@ -363,7 +364,7 @@ struct CounterFast {
     unit = (uint32_t)u;
   }
   __device__ __forceinline__ void at_step(uint32_t, uint32_t) {}
-  __device__ __forceinline__ float n32(uint32_t d) { return counter_normal_fast(seed, unit, d); }
+  __device__ __forceinline__ float n32(uint32_t d) { return counter_normal_fast<HWCOS>(seed, unit, d); }
   __device__ __forceinline__ float u32(uint32_t d) {
     return counter_open01_fast(hash_u32(counter_mix(seed, unit, d, 0u)));
   }
@@ -389,7 +390,18 @@ struct FusedSource<SMP_SOBOL> {
 };
 template <>
 struct FusedSource<SMP_COUNTER> {
-  using type = CounterFast;
+  using type = CounterFastT<false>;
+};
+// Per family: the single-asset GBM families (one normal per step, the MUFU
+// pipe about a third busy) take the hardware cosine; the others keep the
+// polynomial.
+template <int FAM, int SMP>
+struct FusedUnitSource {
+  using type = typename FusedSource<SMP>::type;
+};
+template <int FAM>
+struct FusedUnitSource<FAM, SMP_COUNTER> {
+  using type = CounterFastT<FAM == FAM_GBM_STEP || FAM == FAM_GBM_TERMINAL>;
 };
 
 // Reads materialised samples [dim][unit] (FP64 plain path).
@@ -921,7 +933,7 @@ __device__ __forceinline__ void run_family(const DevReq& q, Src& src, double& p,
 
 template <int FAM, int SMP>
 __device__ __forceinline__ void fused_unit(const DevReq& q, const SrcCtx& ctx, uint64_t u, double& p, double& c) {
-  typename FusedSource<SMP>::type src;
+  typename FusedUnitSource<FAM, SMP>::type src;
   src.template begin<false>(q, ctx, u);
   run_family<float, FAM>(q, src, p, c);
 }
@@ -1388,7 +1400,7 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
       uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
       const bool valid = u < last;
       if (!valid) u = first;  // keeps block-synchronous sources in lockstep; discarded below
-      typename FusedSource<SMP>::type src;
+      typename FusedUnitSource<FAM, SMP>::type src;  // the samples fused_unit<FAM, SMP> draws
       src.template begin<false>(sq, ctx, u);
       float pay[kMaxScen];
       scen_unit<FAM>(sq, src, n_scen, pay);
