@@ -40,7 +40,7 @@ enum Family : int32_t {
   FAM_BASKET = 5,
   FAM_MLMC_LEVEL = 6,
   FAM_GBM_BRIDGE = 7,  // GBM stepwise driven through the Brownian bridge (bridge Sobol)
-  FAM_COUNT = 7
+  FAM_COUNT = 8        // number of families above
 };
 
 // Device samplers.
