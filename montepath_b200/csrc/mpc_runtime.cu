@@ -1688,7 +1688,8 @@ int mpc_device_info(int index, mpc_device_info_t* info) {
   if (cudaSetDevice(index) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
     info->free_memory_bytes = free_b;
   cudaSetDevice(cur);
-  std::snprintf(info->name, sizeof(info->name), "%s", prop.name);
+  // the device name, cut to the ABI field (cudaDeviceProp holds up to 256 bytes)
+  std::snprintf(info->name, sizeof(info->name), "%.*s", int(sizeof(info->name) - 1), prop.name);
   return MPC_OK;
 }
 
