@@ -1762,6 +1762,31 @@ __device__ __forceinline__ bool lsm_ok(const LsmArgs& a, uint64_t index, uint64_
   return false;
 }
 
+// Warp sums of 16 values per lane by reduce-scatter: in each of four rounds a
+// lane keeps half of its values and adds the partner's copy of that half
+// (partner lane ^ 16, ^ 8, ^ 4, ^ 2), then lanes l and l ^ 1 add their last
+// value.  Lane l ends with the warp sum of value brev4(l >> 1) (lanes l and
+// l ^ 1 hold the same bits): 16 double shuffles instead of 80 for 16 separate
+// butterflies, in a fixed order.
+__device__ __forceinline__ double warp_reduce_scatter16(double (&v)[16]) {
+  const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const int o = 16 >> r, c = 8 >> r;
+    const bool up = (lane & (uint32_t)o) != 0;
+#pragma unroll
+    for (int i = 0; i < c; ++i) {
+      const double send = up ? v[i] : v[i + c];
+      const double keep = up ? v[i + c] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+__device__ __forceinline__ uint32_t reduce_scatter16_index(uint32_t lane) {
+  return (((lane >> 4) & 1u) << 3) | (((lane >> 3) & 1u) << 2) | (((lane >> 2) & 1u) << 1) | ((lane >> 1) & 1u);
+}
+
 // One exercise date's regression across the job's blocks (round = the date's
 // position in the backward pass).  Every block has written its 15 moments to
 // partials[buf][lb]; thread 0 adds one to the job's arrival count, which the
@@ -1807,11 +1832,12 @@ __device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint
 #pragma unroll 4
     for (uint32_t blk = lane_grp; blk < nb; blk += n_grp) acc += __ldcg(a.partials + base_at + (size_t)blk * 16 + mom);
   }
-  fold[lane_grp * 16 + mom] = acc;
+  acc += __shfl_xor_sync(0xffffffffu, acc, 16);  // the warp's two lane groups
+  if ((threadIdx.x & 31u) < 16u) fold[(threadIdx.x >> 5) * 16 + mom] = acc;
   __syncthreads();
   if (threadIdx.x < (uint32_t)kLsmMom) {
     double t = 0.0;
-    for (uint32_t g = 0; g < n_grp; ++g) t += fold[g * 16 + threadIdx.x];
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) t += fold[w * 16 + threadIdx.x];
     s_mom[threadIdx.x] = t;
   }
   __syncthreads();
@@ -1962,13 +1988,16 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
       for (int r = 0; r < 4; ++r) m[10 + r] += (double)(b[r] * cont);
       m[14] += 1.0;
     }
-    // block reduction of the 15 moments: warp sums, then one thread per
-    // moment folds the warps in order (the order of block_reduce5)
+    // block reduction of the 15 moments: warp sums by reduce-scatter, then
+    // one thread per moment folds the warps in order
     const uint64_t part_at = ((uint64_t)buf * nb + lb) * 16;
+    {
+      double mv[16];
 #pragma unroll
-    for (int i = 0; i < kLsmMom; ++i) {
-      const double w = warp_sum(m[i]);
-      if ((threadIdx.x & 31) == 0) s_red15[threadIdx.x >> 5][i] = w;
+      for (int i = 0; i < 16; ++i) mv[i] = i < kLsmMom ? m[i] : 0.0;
+      const double w = warp_reduce_scatter16(mv);
+      const uint32_t lane = threadIdx.x & 31u;
+      if ((lane & 1u) == 0) s_red15[threadIdx.x >> 5][reduce_scatter16_index(lane)] = w;
     }
     __syncthreads();
     if (threadIdx.x < (uint32_t)kLsmMom) {

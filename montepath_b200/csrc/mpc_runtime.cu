@@ -1515,7 +1515,7 @@ const RateRow kRateMertonStep = {{1.05e11, 1.05e11, 1.97e11, 4.30e10}, {4.16e10,
 const RateRow kRateMertonTerminal = {{1.70e10, 1.70e10, 1.44e10, 7.09e9}, {1.83e10, 1.83e10, 1.30e10, 6.60e9}};
 const RateRow kRateBasket2 = {{5.46e9, 1.53e10, 1.28e10, 7.74e9}, {5.49e9, 1.58e10, 1.13e10, 6.77e9}};
 const double kRateBridge[2] = {1.41e11, 4.59e10};  // GBM stepwise through the bridge, fp32 / fp64
-const double kLsmFixedMs = 0.28, kLsmRate = 6.4e10; // 49 cross-block date rounds, then path-steps
+const double kLsmFixedMs = 0.24, kLsmRate = 6.4e10; // 49 cross-block date rounds, then path-steps
                                                       // (fit to 524,288 paths x 50 dates)
 const double kCallOverheadMs = 0.035;               // events, copies, one launch
 const double kFirstCallMs = 2.0;                    // tables and buffers of a new shape
