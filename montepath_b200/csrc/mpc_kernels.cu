@@ -2003,8 +2003,9 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
     if (threadIdx.x < (uint32_t)kLsmMom) {
       double t = 0.0;
       for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red15[w][threadIdx.x];
+      // published by thread 0's fence before its arrival in lsm_gather_solve:
+      // the block barrier orders these stores before that (cumulative) fence
       if (lsm_ok(a, part_at + threadIdx.x, a.partials_len, kLsmErrPartials)) a.partials[part_at + threadIdx.x] = t;
-      __threadfence();
     }
     if (si > 0) load_date(si - 1);  // next date's values, in flight during the wait
     // Every block waits (bounded) for all blocks' partials of this date, then
