@@ -40,6 +40,8 @@ __device__ __forceinline__ uint64_t xorshift_jump(const uint64_t* __restrict__ n
 }
 
 // Sequential MonteCarloRng positioned at an arbitrary normal index.
+__device__ __forceinline__ float neg2_log_fast(float u);
+
 struct XorshiftStream {
   uint64_t state;
   double cached;
@@ -80,14 +82,20 @@ struct XorshiftStream {
       has_cached = false;
       return (float)cached;
     }
-    float u1 = (float)next_open01();
-    float u2 = (float)next_open01();
-    float radius = sqrtf(-2.0f * logf(u1));
+    // FP32 path: the stream's uniforms with the short Box-Muller of the
+    // counter-hash normals (atanh series near 1 / hardware log2, approximate
+    // square root) and the hardware sine and cosine of 2 pi (u2 - 1/2) in
+    // [-pi, pi], where their documented error is 2^-21.4 absolute:
+    // sin / cos (2 pi u2) = -sin / -cos (2 pi (u2 - 1/2)).
+    const float u1 = (float)next_open01();
+    const float u2 = (float)next_open01();
+    float radius;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(radius) : "f"(neg2_log_fast(u1)));
     float s, c;
-    sincospif(2.0f * u2, &s, &c);
-    cached = (double)(radius * s);
+    __sincosf(6.28318548f * (u2 - 0.5f), &s, &c);
+    cached = (double)(radius * -s);
     has_cached = true;
-    return radius * c;
+    return radius * -c;
   }
   // Position the stream of `seed` so that the next normal is normal number
   // `normal_index` of the sequential stream.
