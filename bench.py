@@ -369,7 +369,9 @@ def run_ours(args) -> None:
             for key, i in (("heston", 0), ("merton", 1)):
                 line["prices"][key]["fp64_plain"] = plain_results[i].price
                 line["prices"][key]["minus_fp64_plain_in_se"] = (results[i].price - plain_results[i].price) / results[i].stderr
-        legs = [x for x in args.legs.split(",") if x and x != "none"]
+        # the configuration legs and the CPU baseline are single-GPU
+        # measurements: taken at N = 1 only
+        legs = [x for x in args.legs.split(",") if x and x != "none"] if world == 1 else []
         if "all" in legs:
             legs = ["config1", "config2", "config3", "config4", "config5"]
         if legs:
@@ -379,7 +381,7 @@ def run_ours(args) -> None:
                     line["configs"][leg] = leg_config4(backend, args.book_contracts)
                 else:
                     line["configs"][leg] = LEGS[leg](backend)
-        if not args.no_cpu:
+        if not args.no_cpu and world == 1:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     backend.close()
