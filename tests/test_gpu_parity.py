@@ -167,6 +167,25 @@ def test_fused_gbm_against_fp64_oracle(backend, sampling):
     assert abs(a.price - b.price) < 0.05 * b.stderr
 
 
+def test_heston_euler_bias_shrinks_to_semi_analytic(backend):
+    """The headline Heston request (1,048,576 paths, Sobol, FP32 path) against
+    the semi-analytic price: full-truncation Euler is biased by its time step
+    (the Feller condition fails at these parameters), so the gap falls as the
+    steps double, and the step-doubling estimate 2 P(2n) - P(n) lands within 3
+    of its standard-error bounds sqrt(5) SE(2n)."""
+
+    semi = O.heston_call(100, 100, 0.03, 0.04, 2.0, 0.04, 0.5, -0.7, 1.0)
+    prices = {}
+    for n in (256, 1024, 2048):
+        r = req("european_call", model="heston", n_paths=1 << 20, n_steps=n, seed=42, sampling="scrambled_sobol",
+                kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04)
+        prices[n] = backend.price(r)
+    gaps = [prices[n].price - semi for n in (256, 1024, 2048)]
+    assert gaps[0] > gaps[1] > gaps[2] > -3 * prices[2048].stderr, gaps
+    rich = 2 * prices[2048].price - prices[1024].price
+    assert abs(rich - semi) < 3 * math.sqrt(5.0) * prices[2048].stderr, (rich, semi)
+
+
 def test_fused_heston_merton_sobol_small(backend):
     for kw in (
         dict(model="heston", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04),
