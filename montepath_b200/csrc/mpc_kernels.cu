@@ -1962,6 +1962,11 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
     double m[kLsmMom];
 #pragma unroll
     for (int i = 0; i < kLsmMom; ++i) m[i] = 0.0;
+    // FP32 path: each thread first sums its own <= kLsmMaxP paths in FP32;
+    // FP64 takes over from the thread's sums (warp, block, cross-block)
+    float mf[kLsmMom];
+#pragma unroll
+    for (int i = 0; i < kLsmMom; ++i) mf[i] = 0.0f;
     Real sv[kLsmMaxP];
 #pragma unroll
     for (int j = 0; j < kLsmMaxP; ++j) sv[j] = sv_next[j];
@@ -1980,13 +1985,30 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
       Real b[4];
       laguerre4<Real>(s * inv_k, b);
       int idx = 0;
+      if constexpr (sizeof(Real) == 4) {
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < 4; ++r)
 #pragma unroll
-        for (int c = r; c < 4; ++c) m[idx++] += (double)(b[r] * b[c]);
+          for (int c = r; c < 4; ++c) {
+            mf[idx] = fmaf(b[r], b[c], mf[idx]);
+            ++idx;
+          }
 #pragma unroll
-      for (int r = 0; r < 4; ++r) m[10 + r] += (double)(b[r] * cont);
-      m[14] += 1.0;
+        for (int r = 0; r < 4; ++r) mf[10 + r] = fmaf(b[r], cont, mf[10 + r]);
+        mf[14] += 1.0f;
+      } else {
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = r; c < 4; ++c) m[idx++] += (double)(b[r] * b[c]);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) m[10 + r] += (double)(b[r] * cont);
+        m[14] += 1.0;
+      }
+    }
+    if constexpr (sizeof(Real) == 4) {
+#pragma unroll
+      for (int i = 0; i < kLsmMom; ++i) m[i] = (double)mf[i];
     }
     // block reduction of the 15 moments: warp sums by reduce-scatter, then
     // one thread per moment folds the warps in order
