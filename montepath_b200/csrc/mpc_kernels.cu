@@ -693,28 +693,35 @@ __device__ __forceinline__ void unit_merton(const DevReq& q, Src& src, double& p
   if constexpr (kQuadSource<Src>) {
     // four steps per three quads: step k of the chunk uses dimensions
     // d0 + 3k (z), d0 + 3k + 1 (Poisson uniform), d0 + 3k + 2 (jump normal)
-    const float lam_p0_f = q.lam_p0_f;
-    auto step = [&](const float z, const float u, auto&& jump_normal) {
+    // xu: the scrambled 32-bit Poisson sample; its top 23 bits against the
+    // integer thresholds give the jump count of sample_poisson exactly (the
+    // FP64 inversion only from four jumps on)
+    const uint32_t pois_m0 = q.pois_m[0];
+    auto step = [&](const float z, const uint32_t xu, auto&& jump_normal) {
       ls += drift + vol * z;
-      if (u > lam_p0_f) {
-        const uint32_t jumps = poisson_tail((double)u, q.lam_dt, q.lam_p0);
-        if (jumps > 0) ls += (Real)jumps * jm + jv * sq_root<Real>((Real)jumps) * jump_normal();
+      const uint32_t mu = xu >> 9;
+      if (mu >= pois_m0) {
+        uint32_t jumps = 1u + (mu >= q.pois_m[1] ? 1u : 0u) + (mu >= q.pois_m[2] ? 1u : 0u) + (mu >= q.pois_m[3] ? 1u : 0u);
+        if (jumps == 4u) jumps = poisson_tail((double)sobol_unit_f32_bits(xu), q.lam_dt, q.lam_p0);
+        ls += (Real)jumps * jm + jv * sq_root<Real>((Real)jumps) * jump_normal();
       }
     };
     for (; s0 + 4 <= n; s0 += 4) {
       const uint32_t d0 = 3 * s0;
       src.at_step(d0, 12);
       src.quad_load(d0);
-      const float z0 = src.template take_n<0>(d0), u0 = src.template take_u<1>(d0);
+      const float z0 = src.template take_n<0>(d0);
+      const uint32_t u0 = src.template take<1>(d0);
       step(z0, u0, [&] { return src.template take_n<2>(d0); });
       const float z1 = src.template take_n<3>(d0);
       src.quad_load(d0 + 4);
-      const float u1 = src.template take_u<0>(d0 + 4);
+      const uint32_t u1 = src.template take<0>(d0 + 4);
       step(z1, u1, [&] { return src.template take_n<1>(d0 + 4); });
-      const float z2 = src.template take_n<2>(d0 + 4), u2 = src.template take_u<3>(d0 + 4);
+      const float z2 = src.template take_n<2>(d0 + 4);
+      const uint32_t u2 = src.template take<3>(d0 + 4);
       src.quad_load(d0 + 8);
       step(z2, u2, [&] { return src.template take_n<0>(d0 + 8); });
-      step(src.template take_n<1>(d0 + 8), src.template take_u<2>(d0 + 8),
+      step(src.template take_n<1>(d0 + 8), src.template take<2>(d0 + 8),
            [&] { return src.template take_n<3>(d0 + 8); });
     }
   }

@@ -481,6 +481,17 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
     q.lam_p0 = std::exp(-q.lam_dt);
     q.lam_p0_f = float(q.lam_p0);
     if (double(q.lam_p0_f) > q.lam_p0) q.lam_p0_f = std::nextafter(q.lam_p0_f, 0.0f);
+    {  // the cumulative sums of sample_poisson in its own order of operations
+      double prob = q.lam_p0, cum = q.lam_p0;
+      for (int k = 0; k < 4; ++k) {
+        if (k > 0) {
+          prob *= q.lam_dt / double(k);
+          cum += prob;
+        }
+        const double c = cum * 8388608.0 - 0.5;  // exact: u > cum  <=>  m > c
+        q.pois_m[k] = c < 0.0 ? 0u : (c >= 8388607.0 ? 8388608u : uint32_t(std::floor(c)) + 1u);
+      }
+    }
     q.jump_mean = r.jump_mean;
     q.jump_vol = r.jump_volatility;
     q.normals_per_unit = 3ull * q.n_steps;

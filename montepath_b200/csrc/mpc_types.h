@@ -78,6 +78,11 @@ struct alignas(16) DevReq {
   double lam_p0;   // exp(-lam_dt): no jump while u <= lam_p0
   float lam_p0_f;  // largest float <= lam_p0 (exact FP32 test of the same event)
   uint32_t _pad_m;
+  // FP32 Sobol steps: with the Poisson uniform u = (m + 1/2) 2^-23 (m the
+  // top 23 bits of the scrambled sample), m >= pois_m[k] exactly when u
+  // exceeds the (k+1)-term cumulative sum of sample_poisson (cpu.rs:932-953),
+  // i.e. when the jump count is at least k + 1, k = 0..3
+  uint32_t pois_m[4];
   // Basket: lower Cholesky factor and per-asset step constants
   double chol[64], b_drift[8], b_vol[8], spots[8], weights[8];
   // MLMC level
