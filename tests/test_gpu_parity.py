@@ -186,6 +186,20 @@ def test_heston_euler_bias_shrinks_to_semi_analytic(backend):
     assert abs(rich - semi) < 3 * math.sqrt(5.0) * prices[2048].stderr, (rich, semi)
 
 
+def test_merton_fp32_jump_counts_match_oracle(backend):
+    """FP32 Sobol Merton steps count jumps with integer thresholds on the
+    uniform's 23-bit index.  At lambda dt = 0.625 steps with 1, 2, 3 and 4+
+    jumps are common (4+ take the FP64 inversion); a count that differed from
+    the oracle's sample_poisson would move a path's log-price by a whole jump
+    mean (-0.1), far outside the FP32 tolerance, so every path must match."""
+
+    r = req("european_call", model="merton", method="stepwise", n_paths=4096, n_steps=32, seed=13,
+            sampling="scrambled_sobol", jump_intensity=20.0, jump_mean=-0.1, jump_volatility=0.15)
+    _, ref_paths = O.price_paths(r)
+    got_paths = backend.price_paths(r)
+    assert np.allclose(got_paths, ref_paths, rtol=1e-3, atol=2e-3), np.max(np.abs(got_paths - ref_paths))
+
+
 def test_fused_heston_merton_sobol_small(backend):
     for kw in (
         dict(model="heston", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04),
