@@ -142,7 +142,11 @@ typedef struct mpc_request {
   uint64_t paths_per_level[MPC_MAX_LEVELS];
   double target_stderr;
   uint64_t pilot_paths_per_level, min_step_updates, max_step_updates;
-  /* Launch hints (0 = let the autotuner choose). */
+  /* Launch hints (0 = let the autotuner choose).  block_size: 0 or 256 (the
+   * kernels run 256-thread blocks; other values return MPC_E_UNSUPPORTED);
+   * paths_per_thread: 1..64 units per thread per tile, i.e. tiles of
+   * 256 * paths_per_thread paths (the tile partition fixes the order of the
+   * sums, so a hint changes results at rounding level only). */
   uint32_t block_size, paths_per_thread;
   uint64_t _reserved[4];
 } mpc_request_t;

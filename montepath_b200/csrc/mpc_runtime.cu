@@ -160,6 +160,10 @@ int validate(const mpc_request_t& r, std::string* msg) {
   if (r.precision != MPC_PRECISION_FP64_PLAIN && r.precision != MPC_PRECISION_FP32_PATH)
     return invalid(msg, "unknown precision");
   if (r.method < 0 || r.method > MPC_METHOD_STEPWISE) return invalid(msg, "unknown method");
+  // launch hints: the kernels are built for 256-thread blocks
+  if (r.block_size != 0 && r.block_size != 256)
+    return unsupported(msg, "block_size: the kernels run 256-thread blocks (0 or 256)");
+  if (r.paths_per_thread > 64) return invalid(msg, "paths_per_thread must be 0 (autotuner) to 64");
   for (double x : {r.s0, r.k, r.r, r.sigma, r.t})
     if (!finite(x)) return invalid(msg, "market parameters must be finite");
   if (r.workload == MPC_WORKLOAD_ASIAN_MLMC) {
@@ -414,6 +418,7 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
   DevReq& q = p->q;
   std::memset(&q, 0, sizeof(q));
   p->sampler = sampler_of(r.sampling);
+  p->ppt_hint = r.paths_per_thread;
   p->plain = r.precision == MPC_PRECISION_FP64_PLAIN;
   p->lsm = is_lsm(r.workload);
   p->mlmc = r.workload == MPC_WORKLOAD_ASIAN_MLMC;
@@ -539,6 +544,12 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
 }
 
 Shape choose_shape(mpc_context* ctx, const Prepared& p) {
+  if (p.ppt_hint) {  // the caller's paths-per-thread hint, not cached
+    Shape s;
+    s.block = 256;
+    s.ppt = p.ppt_hint;
+    return s;
+  }
   // Autotuner: paths-per-thread per (family, sampler, step bucket, size
   // bucket), picked so that a request spreads over at least four waves of
   // resident blocks; cached per context.

@@ -36,6 +36,7 @@ struct Prepared {
   bool plain = false;     // FP64 plain pipeline
   bool lsm = false;
   bool mlmc = false;
+  uint32_t ppt_hint = 0;  // request's paths_per_thread (0: autotuner)
   double cv_expectation = 0.0;
   std::vector<uint32_t> halton_primes;
   std::vector<double> halton_shifts;

@@ -96,6 +96,8 @@ def validate(r):
          abi.E_INVALID_CONFIG),
         ("arithmetic_asian_mlmc", dict(refinement_factor=1), abi.E_INVALID_CONFIG),
         ("arithmetic_asian_mlmc", dict(levels=0), abi.E_INVALID_CONFIG),
+        ("european_call", dict(block_size=128), abi.E_UNSUPPORTED),
+        ("european_call", dict(paths_per_thread=65), abi.E_INVALID_CONFIG),
     ],
 )
 def test_validation_codes(workload, kw, code):
@@ -109,6 +111,7 @@ def test_valid_requests_pass():
               "american_put", "bermudan_put", "arithmetic_asian_mlmc"):
         assert validate(make_request(w))[0] == abi.OK, w
     assert validate(make_request("european_call", model="merton", sampling="counter_hash"))[0] == abi.OK
+    assert validate(make_request("european_call", block_size=256, paths_per_thread=4))[0] == abi.OK
 
 
 def test_unknown_enum_rejected():

@@ -200,6 +200,22 @@ def test_merton_fp32_jump_counts_match_oracle(backend):
     assert np.allclose(got_paths, ref_paths, rtol=1e-3, atol=2e-3), np.max(np.abs(got_paths - ref_paths))
 
 
+def test_launch_hint_paths_per_thread(backend):
+    """A paths_per_thread hint replaces the autotuner's choice (mpc_prepare
+    reports it) and changes only the tile partition, so the price moves at
+    rounding level."""
+
+    base = req("european_call", model="heston", n_paths=1 << 18, n_steps=64, seed=8, sampling="scrambled_sobol")
+    hinted = req("european_call", model="heston", n_paths=1 << 18, n_steps=64, seed=8, sampling="scrambled_sobol",
+                 paths_per_thread=4, block_size=256)
+    art = backend.prepare(hinted)
+    assert art.paths_per_thread == 4 and art.block_size == 256
+    assert art.tiles == (1 << 18) // (256 * 4)
+    a, b = backend.price(base), backend.price(hinted)
+    assert abs(a.price - b.price) <= 1e-12 * abs(a.price)
+    assert abs(a.stderr - b.stderr) <= 1e-9 * a.stderr
+
+
 def test_fused_heston_merton_sobol_small(backend):
     for kw in (
         dict(model="heston", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04),
