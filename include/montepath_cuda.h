@@ -266,9 +266,11 @@ typedef struct mpc_device_info {
 
 typedef struct mpc_options {
   int32_t device;           /* CUDA device ordinal */
-  int32_t deterministic;    /* 1 = fixed tile order reductions (default) */
+  int32_t deterministic;    /* reductions always run in fixed tile order, so results
+                               are deterministic for 0 and 1 alike */
   uint64_t hbm_budget_bytes; /* 0 = 64 GiB */
-  uint32_t default_block_size;
+  uint32_t default_block_size; /* 0 or 256 (the kernels run 256-thread blocks;
+                                  other values: MPC_E_UNSUPPORTED) */
   uint32_t _pad0;
 } mpc_options_t;
 

@@ -1823,6 +1823,8 @@ int mpc_estimate_bytes(const mpc_request_t* req, uint64_t* bytes) {
 int mpc_create(const mpc_options_t* options, mpc_context_t** out) {
   if (!out) return MPC_E_INVALID_CONFIG;
   *out = nullptr;
+  // the kernels run 256-thread blocks
+  if (options && options->default_block_size != 0 && options->default_block_size != 256) return MPC_E_UNSUPPORTED;
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return MPC_E_NO_DEVICE;
   mpc_context* ctx = new mpc_context();

@@ -143,6 +143,14 @@ def test_create_without_device_reports_no_device():
     assert lib().mpc_create(None, ctypes.byref(handle)) == abi.E_NO_DEVICE
 
 
+def test_create_rejects_block_size_other_than_256():
+    # checked before any device call, so it holds with or without a GPU
+    handle = ctypes.c_void_p()
+    opts = abi.Options(device=0, deterministic=1, hbm_budget_bytes=0, default_block_size=128)
+    assert lib().mpc_create(ctypes.byref(opts), ctypes.byref(handle)) == abi.E_UNSUPPORTED
+    assert not handle.value
+
+
 def test_request_aliases():
     r = make_request("european_call", {"spot": 90, "strike": 95, "rate": 0.01, "volatility": 0.3, "maturity": 2,
                                        "paths": 1000, "steps": 12, "technique": "antithetic",
