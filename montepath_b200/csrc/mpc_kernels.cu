@@ -634,7 +634,25 @@ __device__ __forceinline__ void unit_heston(const DevReq& q, Src& src, double& p
   const bool anti = q.anti != 0;
   Real ls0 = (Real)q.log_s0, ls1 = ls0, v0 = (Real)q.v0, v1 = v0;
   const uint32_t n = q.n_steps;
+  // FP32 path: the same update with the step constants folded on the host
+  // (rate dt, dt / 2, kappa dt, kappa theta dt, xi sqrt(dt)) and FMAs; the
+  // variance is floored after every step and starts >= 0 (validated), so it
+  // needs no floor before use.  The FP64 path keeps the reference's form.
+  const float c_rdt = (float)(q.rate * q.dt), c_hdt = (float)(0.5 * q.dt), c_kdt = (float)(q.kappa * q.dt),
+              c_ktdt = (float)(q.kappa * q.theta * q.dt), c_xsq = (float)(q.xi * q.sqrt_dt);
+  auto step_f32 = [&](float& ls, float& v, const float zv, const float zi) {
+    const float sv = sqrt_approx(v);
+    const float zp = fmaf(rho, zv, rho_perp * zi);
+    ls += fmaf(sv * sqdt, zp, fmaf(-c_hdt, v, c_rdt));
+    const float vn = fmaf(c_xsq * sv, zv, v + fmaf(-c_kdt, v, c_ktdt));
+    v = vn > 0.0f ? vn : 0.0f;
+  };
   auto step = [&](const Real zv, const Real zi) {
+    if constexpr (sizeof(Real) == 4) {
+      step_f32(ls0, v0, zv, zi);
+      if (anti) step_f32(ls1, v1, -zv, -zi);
+      return;
+    }
     {
       Real vp = v0 > (Real)0 ? v0 : (Real)0;
       Real sv = sq_root<Real>(vp);
