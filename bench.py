@@ -53,7 +53,7 @@ SFU_PER_STEP = {"heston": 2 * 1 + 1, "merton": 1}
 # (smsp__inst_executed.sum of the quarter-size ncu capture in profiles/): the
 # kernels are issue-bound, so this gives the fraction of the SMs' issue slots
 # (4 warp instructions per cycle per SM) the measured rate uses.
-WARP_INSTR_PER_32_STEPS = {"heston": 109.5, "merton": 99.7}
+WARP_INSTR_PER_32_STEPS = {"heston": 106.0, "merton": 99.7}
 
 
 def requests(precision: str):
