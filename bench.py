@@ -204,6 +204,63 @@ def cpu_baseline(seconds_target: float = 12.0) -> dict:
     }
 
 
+# what the GPU legs hand to the CPU leg (requests and GPU prices to check)
+_CPU_LEG_INPUTS: dict = {}
+
+
+def cpu_leg(line: dict) -> None:
+    """The CPU leg (rank 0, N = 1; skipped by --no-cpu): the oracle -- the FP64
+    C++ restatement of the reference's CPU path -- timed on a bounded sample
+    of the workload (`cpu_baseline`), and its reference values for the prices
+    this line reports, with the GPU prices' errors against them: the closed
+    forms (Heston semi-analytic, Merton series, Black-Scholes), CRR for the
+    American put, and FP64 prices on the same samples.  All of the bench's
+    use of the oracle happens here, as the checker and as the timed CPU path."""
+
+    from oracle import oracle as O
+
+    line["cpu_baseline"] = cpu_baseline()
+    semi = O.heston_call(100, 100, 0.03, 0.04, 2.0, 0.04, 0.5, -0.7, 1.0)
+    series = O.merton_series(100, 100, 0.03, 0.2, 0.5, -0.1, 0.15, 1.0, exact=True)
+    h, m = line["prices"]["heston"], line["prices"]["merton"]
+    # the closed forms are continuous-time; the gap to them includes the
+    # 256-step scheme's discretisation bias (see config2)
+    h["semi_analytic"], h["minus_semi_in_se"] = semi, (h["price"] - semi) / h["stderr"]
+    m["series"], m["minus_series_in_se"] = series, (m["price"] - series) / m["stderr"]
+    configs = line.get("configs", {})
+    if "config1" in configs and "config1" in _CPU_LEG_INPUTS:
+        c1, r64 = configs["config1"], _CPU_LEG_INPUTS["config1"]
+        t0 = time.perf_counter()
+        ref = O.price(r64)
+        t_cpu = time.perf_counter() - t0
+        bs = 9.413403383853016
+        c1["fp64_plain"]["err_vs_black_scholes_se"] = (c1["fp64_plain"]["price"] - bs) / c1["fp64_plain"]["stderr"]
+        c1["fp64_plain"]["abs_diff_vs_oracle"] = abs(c1["fp64_plain"]["price"] - ref.price)
+        c1["cpu_oracle_1_thread"] = {"price": ref.price, "seconds": t_cpu, "path_steps_per_sec": 20000 * 64 / t_cpu}
+    if "config2" in configs:
+        c2 = configs["config2"]
+        c2["semi_analytic"] = semi
+        for row in c2["steps"].values():
+            row["minus_semi_in_se"] = (row["price"] - semi) / row["stderr"]
+        rich = c2["richardson_1024_2048"]
+        rich["minus_semi_in_se"] = (rich["price"] - semi) / rich["stderr_bound"]
+    if "config3" in configs:
+        for key, row in configs["config3"].items():
+            row["crr_2048"] = O.crr_put(float(key.split("_")[1]), 100.0, 0.06, 0.2, 1.0, 2048)
+    if "config4" in configs and "config4" in _CPU_LEG_INPUTS:
+        diffs_se, worst_abs = [], 0.0
+        for req, gpu_price in _CPU_LEG_INPUTS["config4"]:
+            ref = O.price(req)
+            d = abs(gpu_price - ref.price)
+            worst_abs = max(worst_abs, d)
+            if ref.stderr > 0:
+                diffs_se.append(d / ref.stderr)
+        configs["config4"]["vs_fp64_oracle"] = {
+            "contracts": len(_CPU_LEG_INPUTS["config4"]), "max_abs_diff": worst_abs,
+            "max_diff_in_se": max(diffs_se) if diffs_se else None,
+            "within_3se": sum(1 for x in diffs_se if x <= 3.0), "with_nonzero_stderr": len(diffs_se)}
+
+
 def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -313,10 +370,6 @@ def run_ours(args) -> None:
     if fr_sfu is not None and fr_fp32 is not None and fr_sfu > fr_fp32:
         bound, achieved, peak, unit, frac = "sfu", sfu / 1e12, sfu_peak, "Tops/s", fr_sfu
 
-    from oracle import oracle as O
-
-    heston_ref = O.heston_call(100, 100, 0.03, 0.04, 2.0, 0.04, 0.5, -0.7, 1.0)
-    merton_ref = O.merton_series(100, 100, 0.03, 0.2, 0.5, -0.1, 0.15, 1.0, exact=True)
     if rank == 0:
         line = {
             "metric": "path-steps/s",
@@ -355,12 +408,8 @@ def run_ours(args) -> None:
                 "hbm_peak_gbs": load_peaks().get("hbm_gbs"),
             },
             "prices": {
-                # the closed forms are continuous-time; the gap to them includes the
-                # 256-step scheme's discretisation bias (see the config2 leg)
-                "heston": {"price": results[0].price, "stderr": results[0].stderr, "semi_analytic": heston_ref,
-                           "minus_semi_in_se": (results[0].price - heston_ref) / results[0].stderr},
-                "merton": {"price": results[1].price, "stderr": results[1].stderr, "series": merton_ref,
-                           "minus_series_in_se": (results[1].price - merton_ref) / results[1].stderr},
+                "heston": {"price": results[0].price, "stderr": results[0].stderr},
+                "merton": {"price": results[1].price, "stderr": results[1].stderr},
             },
         }
         if plain_value is not None:
@@ -382,7 +431,7 @@ def run_ours(args) -> None:
                 else:
                     line["configs"][leg] = LEGS[leg](backend)
         if not args.no_cpu and world == 1:
-            line["cpu_baseline"] = cpu_baseline()
+            cpu_leg(line)
         print(json.dumps(line), flush=True)
     backend.close()
     if pg is not None:
@@ -399,7 +448,6 @@ def leg_config1(backend) -> dict:
     reference's MonteCarloRng stream replayed), FP64 one request per launch."""
 
     from montepath_b200.requests import make_request
-    from oracle import oracle as O
 
     cfg = dict(method="stepwise", n_paths=20000, n_steps=64, seed=42, n_threads=1)
     r64 = make_request("european_call", dict(cfg, precision="fp64_plain"))
@@ -409,16 +457,11 @@ def leg_config1(backend) -> dict:
         backend.price(r32)
     a, t64 = _timed(backend, lambda: backend.price(r64))
     b, t32 = _timed(backend, lambda: backend.price(r32))
-    t0 = time.perf_counter()
-    c = O.price(r64)
-    t_cpu = time.perf_counter() - t0
-    bs = 9.413403383853016
     ps = 20000 * 64
+    _CPU_LEG_INPUTS["config1"] = r64
     return {
-        "fp64_plain": {"price": a.price, "stderr": a.stderr, "ms": t64, "path_steps_per_sec": ps / (t64 * 1e-3),
-                       "err_vs_black_scholes_se": (a.price - bs) / a.stderr, "abs_diff_vs_oracle": abs(a.price - c.price)},
+        "fp64_plain": {"price": a.price, "stderr": a.stderr, "ms": t64, "path_steps_per_sec": ps / (t64 * 1e-3)},
         "fp32_path": {"price": b.price, "stderr": b.stderr, "ms": t32, "path_steps_per_sec": ps / (t32 * 1e-3)},
-        "cpu_oracle_1_thread": {"price": c.price, "seconds": t_cpu, "path_steps_per_sec": ps / t_cpu},
     }
 
 
@@ -433,20 +476,14 @@ def leg_config2(backend) -> dict:
     estimates' variances (they share the Sobol points, so it is smaller)."""
 
     from montepath_b200.requests import make_request
-    from oracle import oracle as O
 
-    semi = O.heston_call(100, 100, 0.03, 0.04, 2.0, 0.04, 0.5, -0.7, 1.0)
     rows = {}
     for n in (256, 512, 1024, 2048):
         r = make_request("european_call", dict(HESTON, n_steps=n, precision="fp32_path"))
-        res = backend.price(r)
-        rows[n] = res
-    out = {"semi_analytic": semi, "steps": {}}
-    for n, res in rows.items():
-        out["steps"][str(n)] = {"price": res.price, "stderr": res.stderr, "minus_semi_in_se": (res.price - semi) / res.stderr}
-    rich = 2.0 * rows[2048].price - rows[1024].price
-    se_bound = math.sqrt(5.0) * rows[2048].stderr
-    out["richardson_1024_2048"] = {"price": rich, "stderr_bound": se_bound, "minus_semi_in_se": (rich - semi) / se_bound}
+        rows[n] = backend.price(r)
+    out = {"steps": {str(n): {"price": res.price, "stderr": res.stderr} for n, res in rows.items()}}
+    out["richardson_1024_2048"] = {"price": 2.0 * rows[2048].price - rows[1024].price,
+                                   "stderr_bound": math.sqrt(5.0) * rows[2048].stderr}
     return out
 
 
@@ -454,11 +491,10 @@ def leg_config3(backend) -> dict:
     """American put by Longstaff-Schwartz, 524,288 paths x 50 dates, S0 in {90, 100, 110}."""
 
     from montepath_b200.requests import make_request
-    from oracle import oracle as O
 
     out = {}
     for s0 in (90.0, 100.0, 110.0):
-        row = {"crr_2048": O.crr_put(s0, 100.0, 0.06, 0.2, 1.0, 2048)}
+        row = {}
         for precision in ("fp32_path", "fp64_plain"):
             r = make_request("american_put", dict(s0=s0, k=100.0, r=0.06, sigma=0.2, t=1.0, n_paths=524288,
                                                   n_steps=50, basis_degree=3, seed=42, precision=precision))
@@ -485,18 +521,10 @@ def leg_config4(backend, contracts: int = 4096) -> dict:
     backend.price_batch(book)
     res, ms = _timed(backend, lambda: backend.price_batch(book))
     _, launches = backend.last_timing()
-    # the batched FP32 prices against the FP64 CPU oracle on the same samples,
-    # for the contracts small enough (<= 2e6 path-steps) to price on the CPU here
-    from oracle import oracle as O
-
+    # the contracts small enough (<= 2e6 path-steps) for the CPU leg to price
+    # with the oracle on the same samples
     small = [i for i, r in enumerate(book) if r.n_paths * r.n_steps <= 2_000_000][:64]
-    diffs_se, worst_abs = [], 0.0
-    for i in small:
-        ref = O.price(book[i])
-        d = abs(res[i].price - ref.price)
-        worst_abs = max(worst_abs, d)
-        if ref.stderr > 0:
-            diffs_se.append(d / ref.stderr)
+    _CPU_LEG_INPUTS["config4"] = [(book[i], res[i].price) for i in small]
     sample = book[::63]
     plain_ms = 0.0
     for r in sample:
@@ -514,9 +542,6 @@ def leg_config4(backend, contracts: int = 4096) -> dict:
                                "estimated_ms_full_book": total / plain_rate * 1e3},
         "speedup_batched_vs_plain": (total / (ms * 1e-3)) / plain_rate,
         "price_checksum": sum(x.price for x in res),
-        "vs_fp64_oracle": {"contracts": len(small), "max_abs_diff": worst_abs,
-                           "max_diff_in_se": max(diffs_se) if diffs_se else None,
-                           "within_3se": sum(1 for x in diffs_se if x <= 3.0), "with_nonzero_stderr": len(diffs_se)},
     }
 
 

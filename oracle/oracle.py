@@ -1,9 +1,9 @@
 """ctypes wrapper of the FP64 CPU oracle (oracle/mp_oracle.cpp).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
-and by bench.py (the CPU-baseline leg and the accuracy checks of its legs),
-to check results and to time the CPU path.  The product (``montepath_b200``)
-never imports it.
+and by bench.py's CPU leg (``cpu_baseline`` / ``cpu_leg``, and the reference
+arm), to check results and to time the CPU path.  The product
+(``montepath_b200``) never imports it.
 """
 
 from __future__ import annotations
