@@ -216,6 +216,41 @@ def test_launch_hint_paths_per_thread(backend):
     assert abs(a.stderr - b.stderr) <= 1e-9 * a.stderr
 
 
+EDGE_MODELS = [
+    ("european_call", dict(method="stepwise")),
+    ("arithmetic_asian_call", {}),
+    ("european_call", dict(model="heston", method="stepwise", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7)),
+    ("european_call", dict(model="merton", method="stepwise", jump_intensity=0.5, jump_mean=-0.1,
+                           jump_volatility=0.15)),
+]
+
+
+@pytest.mark.parametrize("workload,kw", EDGE_MODELS)
+@pytest.mark.parametrize("sampling", ["scrambled_sobol", "counter_hash"])
+@pytest.mark.parametrize("n_paths,n_steps", [(1, 1), (3, 3), (257, 5), (300, 7)])
+def test_edge_sizes_match_oracle(backend, workload, kw, sampling, n_paths, n_steps):
+    """Single paths, tile tails (257, 300 paths) and step counts that end in a
+    partial quad or Merton chunk (1, 3, 5, 7 steps): FP64 plain per path to
+    1e-10 (2e-5 with counter-hash normals, FP32 values from two libms), fused
+    FP32 per path within the FP32 tolerance, against the oracle."""
+
+    base = dict(kw, n_paths=n_paths, n_steps=n_steps, seed=21, sampling=sampling)
+    r64 = req(workload, precision="fp64_plain", **base)
+    _, ref = O.price_paths(r64)
+    got64 = backend.price_paths(r64)
+    tol = 2e-5 if sampling == "counter_hash" else 1e-10
+    assert np.allclose(got64, ref, rtol=tol, atol=tol)
+    r32 = req(workload, **base)
+    got32 = backend.price_paths(r32)
+    assert np.allclose(got32, ref, rtol=1e-3, atol=2e-3), np.max(np.abs(got32 - ref))
+    a = backend.price(r32)
+    assert math.isfinite(a.price) and a.n_samples == n_paths
+
+
+def test_empty_batch(backend):
+    assert backend.price_batch([]) == []
+
+
 def test_fused_heston_merton_sobol_small(backend):
     for kw in (
         dict(model="heston", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04),
