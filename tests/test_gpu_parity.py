@@ -247,6 +247,34 @@ def test_edge_sizes_match_oracle(backend, workload, kw, sampling, n_paths, n_ste
     assert math.isfinite(a.price) and a.n_samples == n_paths
 
 
+@pytest.mark.parametrize("n_paths,n_steps", [(1, 2), (5, 3), (513, 2), (513, 3)])
+def test_lsm_edge_sizes_match_oracle(backend, n_paths, n_steps):
+    """American put with one path (no regression can run), a handful of
+    paths and the fewest dates, FP64 against the oracle."""
+
+    r = req("american_put", n_paths=n_paths, n_steps=n_steps, seed=17, r=0.06, basis_degree=3,
+            precision="fp64_plain")
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) <= 1e-9 * max(abs(b.price), 1e-12)
+    assert a.early_exercise_count == b.early_exercise_count
+    assert a.regression_steps == b.regression_steps
+
+
+@pytest.mark.parametrize("n_paths", [1, 5, 257])
+def test_antithetic_odd_paths_match_oracle(backend, n_paths):
+    """Antithetic pairs with an odd path count (the reference prices
+    (n + 1) / 2 pairs), FP64 plain per pair against the oracle."""
+
+    r = req("european_call", method="stepwise", n_paths=n_paths, n_steps=9, seed=4, technique="antithetic",
+            precision="fp64_plain")
+    _, ref = O.price_paths(r)
+    got = backend.price_paths(r)
+    assert len(got) == (n_paths + 1) // 2
+    assert np.allclose(got, ref, rtol=1e-10, atol=1e-10)
+    a, b = backend.price(r), O.price(r)
+    assert abs(a.price - b.price) <= 1e-10 * max(abs(b.price), 1e-12)
+
+
 def test_empty_batch(backend):
     assert backend.price_batch([]) == []
 
