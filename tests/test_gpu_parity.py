@@ -300,6 +300,25 @@ def test_fused_basket_five_assets(backend):
     assert np.allclose(got, ref_paths, rtol=2e-4, atol=1e-3)
 
 
+@pytest.mark.parametrize("d", [1, 3, 4, 6, 7, 8])
+@pytest.mark.parametrize("sampling", ["scrambled_sobol", "counter_hash"])
+def test_basket_every_asset_count(backend, d, sampling):
+    """The basket unit is compiled per asset count: every count other than
+    the 2 and 5 above, stepwise with a partial last quad of dimensions, FP64
+    plain per path and fused FP32 per path against the oracle."""
+
+    spots = [100.0 - 3 * i for i in range(d)]
+    sigmas = [0.15 + 0.02 * i for i in range(d)]
+    r64 = req("basket_call", method="stepwise", n_steps=7, n_paths=1000, seed=31, sampling=sampling, spots=spots,
+              sigmas=sigmas, weights=[1.0 / d] * d, corr=0.3, k=95, precision="fp64_plain")
+    _, ref = O.price_paths(r64)
+    tol = 2e-5 if sampling == "counter_hash" else 1e-10
+    assert np.allclose(backend.price_paths(r64), ref, rtol=tol, atol=tol)
+    r32 = req("basket_call", method="stepwise", n_steps=7, n_paths=1000, seed=31, sampling=sampling, spots=spots,
+              sigmas=sigmas, weights=[1.0 / d] * d, corr=0.3, k=95)
+    assert np.allclose(backend.price_paths(r32), ref, rtol=1e-3, atol=2e-3)
+
+
 # --------------------------------------------------------------------- LSM --
 def test_lsm_fp64_plain_matches_oracle(backend):
     r = req("american_put", n_paths=8192, n_steps=50, seed=5, r=0.06, basis_degree=3, precision="fp64_plain")
