@@ -275,6 +275,43 @@ def test_antithetic_odd_paths_match_oracle(backend, n_paths):
     assert abs(a.price - b.price) <= 1e-10 * max(abs(b.price), 1e-12)
 
 
+def test_server_cancel_queued_request(backend):
+    """mpc_cancel: a request still queued (the only slot is held by a larger
+    one) is cancelled and its wait reports MPC_E_CANCELLED; a finished or
+    unknown ticket is refused."""
+
+    from montepath_b200.backend import BackendError
+
+    big = req("european_call", model="heston", n_paths=1 << 22, n_steps=256, seed=1, sampling="scrambled_sobol")
+    small = req("european_call", method="stepwise", n_paths=10000, n_steps=16, seed=2)
+    with backend.server(max_slots=1) as srv:
+        t1 = srv.submit(big)
+        t2 = srv.submit(small)
+        assert srv.cancel(t2) == abi.OK
+        with pytest.raises(BackendError) as err:
+            srv.wait(t2, 10_000)
+        assert err.value.status == abi.E_CANCELLED
+        assert srv.wait(t1, 60_000).status == abi.OK
+        assert srv.cancel(t1) == abi.E_BUSY
+        assert srv.cancel(t2 + 1000) == abi.E_NOT_FOUND
+        assert srv.stats().cancelled == 1
+
+
+def test_device_info_and_error_message(backend):
+    import ctypes
+
+    lib = abi.load_library()
+    info = abi.DeviceInfo()
+    assert lib.mpc_device_info(0, ctypes.byref(info)) == abi.OK
+    assert info.sm_count > 0 and info.cc_major >= 10 and info.total_memory_bytes > 0 and info.name
+    assert lib.mpc_device_info(10_000, ctypes.byref(info)) != abi.OK
+    from montepath_b200.backend import BackendError
+
+    with pytest.raises(BackendError) as err:
+        backend.price(req("european_call", n_paths=0))
+    assert err.value.status == abi.E_INVALID_CONFIG and "n_paths" in str(err.value)
+
+
 def test_empty_batch(backend):
     assert backend.price_batch([]) == []
 
