@@ -287,11 +287,14 @@ def test_server_cancel_queued_request(backend):
     with backend.server(max_slots=1) as srv:
         t1 = srv.submit(big)
         t2 = srv.submit(small)
+        assert srv.poll(t2) is None  # queued: mpc_poll answers MPC_E_BUSY
         assert srv.cancel(t2) == abi.OK
         with pytest.raises(BackendError) as err:
             srv.wait(t2, 10_000)
         assert err.value.status == abi.E_CANCELLED
-        assert srv.wait(t1, 60_000).status == abi.OK
+        done = srv.wait(t1, 60_000)
+        assert done.status == abi.OK
+        assert srv.poll(t1).price == done.price  # finished: mpc_poll returns the result
         assert srv.cancel(t1) == abi.E_BUSY
         assert srv.cancel(t2 + 1000) == abi.E_NOT_FOUND
         assert srv.stats().cancelled == 1
