@@ -745,10 +745,29 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
     cudaError_t e = cudaMemcpyAsync(d_reqs, hp, desc_bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_tiles, ht, tile_bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_counter, 0, groups * sizeof(uint32_t), ctx->stream);
-    for (size_t g = 0; g < groups && e == cudaSuccess; ++g)
+    if (e == cudaSuccess && groups > 1) e = cudaEventRecord(ctx->ev_fork, ctx->stream);
+    bool used[mpc_context::kSideStreams] = {};
+    for (size_t g = 0; g < groups && e == cudaSuccess; ++g) {
+      cudaStream_t st = ctx->stream;
+      if (g > 0) {
+        const int k = int((g - 1) % mpc_context::kSideStreams);
+        st = ctx->side[k];
+        if (!used[k]) {
+          used[k] = true;
+          e = cudaStreamWaitEvent(st, ctx->ev_fork, 0);
+          if (e != cudaSuccess) break;
+        }
+      }
       e = launch_fused(static_cast<DevReq*>(d_reqs), static_cast<Tile*>(d_tiles) + group_first[g], group_count[g],
                        static_cast<uint32_t*>(d_counter) + g, gl[g].family, gl[g].sampler, ctx->tabs, int(grids[g]),
-                       256, ctx->stream);
+                       256, st);
+    }
+    for (int k = 0; k < mpc_context::kSideStreams; ++k) {  // join every forked stream, also after an error
+      if (!used[k]) continue;
+      const cudaError_t ej = cudaEventRecord(ctx->ev_join[k], ctx->side[k]);
+      const cudaError_t ew = ej == cudaSuccess ? cudaStreamWaitEvent(ctx->stream, ctx->ev_join[k], 0) : ej;
+      if (e == cudaSuccess) e = ew;
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(hm, d_mom, mom_bytes, cudaMemcpyDeviceToHost, ctx->stream);
     return e;
   };
@@ -1844,6 +1863,12 @@ int mpc_create(const mpc_options_t* options, mpc_context_t** out) {
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device);
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess)
     return bail(e, "cudaStreamCreate");
+  for (int i = 0; i < mpc_context::kSideStreams; ++i) {
+    if ((e = cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking)) != cudaSuccess)
+      return bail(e, "cudaStreamCreate");
+    cudaEventCreateWithFlags(&ctx->ev_join[i], cudaEventDisableTiming);
+  }
+  cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
   cudaEventCreate(&ctx->ev_start);
   cudaEventCreate(&ctx->ev_stop);
   std::vector<uint32_t> sob;
@@ -1872,6 +1897,14 @@ int mpc_destroy(mpc_context_t* ctx) {
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  for (int i = 0; i < mpc_context::kSideStreams; ++i) {
+    if (ctx->side[i]) {
+      cudaStreamSynchronize(ctx->side[i]);
+      cudaStreamDestroy(ctx->side[i]);
+    }
+    if (ctx->ev_join[i]) cudaEventDestroy(ctx->ev_join[i]);
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return MPC_OK;

@@ -59,6 +59,13 @@ struct mpc_context {
   int sm_count = 148;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  // Concurrent group launches of a batch: group 0 runs on `stream`, group g
+  // on side[(g - 1) % kSideStreams], forked after the tile counters are reset
+  // and joined before the moments are copied out, so one family's blocks
+  // start on the SMs another family's tail leaves idle.
+  static constexpr int kSideStreams = 3;
+  cudaStream_t side[kSideStreams] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kSideStreams] = {};
   mpc::DeviceTables tabs{};
   void* d_sobol = nullptr;
   void* d_jump = nullptr;
