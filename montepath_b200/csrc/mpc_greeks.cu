@@ -4,9 +4,11 @@
 // european_call_greeks_cpu and siblings 4036-4356, bump recipe 4938-5008,
 // single-pass estimators 4670-4869) on the device:
 //  - bump-and-revalue: the base request plus an up and a down bump per Greek,
-//    all with the request's seed (common random numbers), priced by one
-//    mpc_price_batch call -- on the FP32 path that is one persistent launch
-//    for all 9 (13 for a basket) scenarios;
+//    all with the request's seed (common random numbers).  FP32 requests of
+//    the standard technique with xorshift, Sobol or counter-hash samples
+//    price all 9 legs (13 for a basket) in one scenario launch that draws
+//    each normal once for every leg; the others price their legs with one
+//    mpc_price_batch call;
 //  - pathwise / likelihood ratio: one kernel pass over the pseudorandom
 //    terminal shocks of the request's seed, sums in FP64.
 
@@ -133,9 +135,30 @@ void mean_stderr(double sum, double sq, uint64_t count, double* mean, double* se
 // kernel runs, a sampler whose normals depend only on (point, dimension).
 bool scenario_eligible(const Prepared& p, const mpc_request_t& r, size_t legs) {
   if (r.precision != MPC_PRECISION_FP32_PATH || r.technique != MPC_TECHNIQUE_STANDARD) return false;
-  if (legs > size_t(kMaxScen) || p.q.bridge) return false;
-  if (p.family != FAM_GBM_STEP && p.family != FAM_GBM_TERMINAL && p.family != FAM_HESTON) return false;
+  if (p.q.bridge) return false;
+  if (p.family == FAM_BASKET) {
+    if (legs > size_t(kBasketScen)) return false;
+  } else {
+    if (legs > size_t(kMaxScen)) return false;
+    if (p.family != FAM_GBM_STEP && p.family != FAM_GBM_TERMINAL && p.family != FAM_HESTON) return false;
+  }
   return p.sampler == SMP_XORSHIFT || p.sampler == SMP_SOBOL || p.sampler == SMP_COUNTER;
+}
+
+// Per-leg constants of the basket scenario kernel; legs past the last are
+// copies of the base leg (computed, never reported).
+BasketScen basket_legs(const std::vector<Prepared>& preps) {
+  BasketScen b{};
+  for (int s = 0; s < kBasketScen; ++s) {
+    const DevReq& q = preps[s < int(preps.size()) ? s : 0].q;
+    for (uint32_t a = 0; a < q.n_assets; ++a) {
+      b.log_drift[s][a] = float(q.b_drift[a] * double(q.n_steps));
+      b.step_vol[s][a] = float(q.b_vol[a]);
+      b.wspot[s][a] = float(q.weights[a] * q.spots[a]);
+    }
+    b.discount[s] = float(q.discount);
+  }
+  return b;
 }
 
 // Prices every leg (same seed, same dimensions) in one scenario launch.
@@ -148,8 +171,10 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
   }
   const Prepared& base = preps[0];
   const int n_scen = int(legs.size());
+  const bool basket = base.family == FAM_BASKET;
+  const int slots = basket ? kBasketScen : kMaxScen;  // legs per tile partial
   float scen[kScenFields * kMaxScen];
-  for (int s = 0; s < kMaxScen; ++s) {
+  for (int s = 0; s < kMaxScen && !basket; ++s) {
     const DevReq& q = preps[s < n_scen ? s : 0].q;
     float f[kScenFields];
     if (base.family == FAM_HESTON) {
@@ -174,7 +199,7 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
   // device layout: descriptor | leg parameters | partials | moments | counters (done, tile counter)
   const size_t o_scen = 256 * ((sizeof(DevReq) + 255) / 256);
   const size_t o_part = o_scen + 256;
-  const size_t o_mom = o_part + ((n_tiles * kMaxScen * 2 * sizeof(double) + 255) / 256) * 256;
+  const size_t o_mom = o_part + ((n_tiles * slots * 2 * sizeof(double) + 255) / 256) * 256;
   const size_t o_cnt = o_mom + 256;
   void* d = nullptr;
   int st = scratch(ctx, "scenarios", o_cnt + 256, &d);
@@ -186,22 +211,27 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
   q.tiles_done = reinterpret_cast<uint32_t*>(base_ptr + o_cnt);
   q.per_unit = nullptr;
   uint32_t* counter = q.tiles_done + 1;
-  double host_mom[kMaxScen * 2];
+  double host_mom[kBasketScen * 2];
+  static_assert(kBasketScen * 2 * sizeof(double) <= 256 && kBasketScen >= kMaxScen, "moments area");
   auto fin = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? MPC_OK : cuda_fail(ctx, e, what); };
   if ((st = fin(cudaMemsetAsync(q.tiles_done, 0, 2 * sizeof(uint32_t), ctx->stream), "memset counters"))) return st;
   if ((st = fin(cudaMemcpyAsync(base_ptr, &q, sizeof(q), cudaMemcpyHostToDevice, ctx->stream), "descriptor"))) return st;
-  if ((st = fin(cudaMemcpyAsync(base_ptr + o_scen, scen, sizeof(scen), cudaMemcpyHostToDevice, ctx->stream),
-                "leg parameters")))
+  if (!basket && (st = fin(cudaMemcpyAsync(base_ptr + o_scen, scen, sizeof(scen), cudaMemcpyHostToDevice, ctx->stream),
+                           "leg parameters")))
     return st;
-  const int occ = std::max(1, scenario_max_blocks_per_sm(base.family, base.sampler));
+  const int occ = std::max(1, basket ? basket_scenario_max_blocks_per_sm(base.sampler)
+                                     : scenario_max_blocks_per_sm(base.family, base.sampler));
   const int grid = int(std::min<uint64_t>(n_tiles, uint64_t(ctx->sm_count) * occ));
   if ((st = fin(cudaEventRecord(ctx->ev_start, ctx->stream), "event"))) return st;
-  if ((st = fin(launch_scenarios(reinterpret_cast<const DevReq*>(base_ptr), q.n_tiles, counter, base.family,
-                                 base.sampler, ctx->tabs, grid, ctx->stream),
-                "scenario kernel")))
-    return st;
+  const DevReq* d_req = reinterpret_cast<const DevReq*>(base_ptr);
+  const cudaError_t launched =
+      basket ? launch_basket_scenarios(d_req, q.n_tiles, counter, base.sampler, basket_legs(preps), ctx->tabs, grid,
+                                       ctx->stream)
+             : launch_scenarios(d_req, q.n_tiles, counter, base.family, base.sampler, ctx->tabs, grid, ctx->stream);
+  if ((st = fin(launched, "scenario kernel"))) return st;
   if ((st = fin(cudaEventRecord(ctx->ev_stop, ctx->stream), "event"))) return st;
-  if ((st = fin(cudaMemcpyAsync(host_mom, q.moments, sizeof(host_mom), cudaMemcpyDeviceToHost, ctx->stream),
+  if ((st = fin(cudaMemcpyAsync(host_mom, q.moments, size_t(slots) * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                                ctx->stream),
                 "moments")))
     return st;
   if ((st = fin(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize"))) return st;

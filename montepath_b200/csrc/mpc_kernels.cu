@@ -1520,6 +1520,216 @@ cudaError_t launch_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_
   }
 }
 
+// ------------------------------------------- basket scenario (bump) kernel ---
+// Bump legs of a d-asset basket with common random numbers.  A path draws
+// its n_steps x D normals once and keeps only the per-asset sums Z_a; the
+// correlated sums are W = L Z (L the Cholesky factor), and leg s prices
+//   basket_s = sum_a wspot[s][a] exp(log_drift[s][a] + step_vol[s][a] W_a)
+// (basket_terminal_payoff, cpu.rs:7616-7635, with the stepwise log return
+// sum_steps (drift_dt + vol_dt zc) regrouped as T drift + vol_dt W).  The
+// moment reduction is that of scenario_kernel: per-warp FP64 slots, tile
+// partials in warp order, the last tile sums the partials in tile order.
+template <int D, class Src>
+__device__ __forceinline__ void scen_basket_d(const DevReq& q, Src& src, const BasketScen& legs,
+                                              float pay[kBasketScen]) {
+  float zs[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) zs[a] = 0.0f;
+  const uint32_t n = q.n_steps;
+  uint32_t dim = 0;
+  for (uint32_t st = 0; st < n; ++st) {
+    src.at_step(dim, D);
+#pragma unroll
+    for (int a = 0; a < D; ++a) zs[a] += normal<float>(src, dim + a);
+    dim += D;
+  }
+  float w[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int b = 0; b <= a; ++b) acc += (float)q.chol[a * D + b] * zs[b];
+    w[a] = acc;
+  }
+  const float kk = (float)q.k;
+#pragma unroll
+  for (int s = 0; s < kBasketScen; ++s) {
+    float basket = 0.0f;
+#pragma unroll
+    for (int a = 0; a < D; ++a) basket += legs.wspot[s][a] * __expf(legs.log_drift[s][a] + legs.step_vol[s][a] * w[a]);
+    pay[s] = (basket - kk > 0.0f ? basket - kk : 0.0f) * legs.discount[s];
+  }
+}
+
+template <class Src>
+__device__ __forceinline__ void scen_basket(const DevReq& q, Src& src, const BasketScen& legs,
+                                            float pay[kBasketScen]) {
+  switch (q.n_assets) {
+    case 1:
+      scen_basket_d<1>(q, src, legs, pay);
+      break;
+    case 2:
+      scen_basket_d<2>(q, src, legs, pay);
+      break;
+    case 3:
+      scen_basket_d<3>(q, src, legs, pay);
+      break;
+    case 4:
+      scen_basket_d<4>(q, src, legs, pay);
+      break;
+    case 5:
+      scen_basket_d<5>(q, src, legs, pay);
+      break;
+    case 6:
+      scen_basket_d<6>(q, src, legs, pay);
+      break;
+    case 7:
+      scen_basket_d<7>(q, src, legs, pay);
+      break;
+    default:
+      scen_basket_d<8>(q, src, legs, pay);
+      break;
+  }
+}
+
+// One basket request (reqs[0]) split into n_tiles tiles of q.tile_units units.
+template <int SMP>
+__global__ void __launch_bounds__(kFusedBlock, 2) basket_scenario_kernel(const DevReq* __restrict__ reqs,
+                                                                        uint32_t n_tiles,
+                                                                        uint32_t* __restrict__ counter,
+                                                                        SrcCtx ctx, const BasketScen legs) {
+  extern __shared__ __align__(16) uint32_t sobol_window[];
+  if constexpr (SMP == SMP_SOBOL) {
+    float4* seg = reinterpret_cast<float4*>(sobol_window + kSobolWindowWords);
+    const float4* src = reinterpret_cast<const float4*>(ctx.sobol + MPC_ICDF_OFFSET);
+    for (uint32_t i = threadIdx.x; i < MPC_ICDF_SEGMENTS; i += blockDim.x) seg[i] = src[i];
+    ctx.win = sobol_window;
+    ctx.icdf = seg;
+  } else {
+    ctx.win = nullptr;
+    ctx.icdf = nullptr;
+  }
+  __shared__ DevReq sq;
+  __shared__ double slots[kWarps][kBasketScen][2];
+  __shared__ uint32_t s_tile;
+  __shared__ int s_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= n_tiles) break;
+    {
+      const uint4* src = reinterpret_cast<const uint4*>(reqs);
+      uint4* dst = reinterpret_cast<uint4*>(&sq);
+      for (uint32_t i = threadIdx.x; i < sizeof(DevReq) / sizeof(uint4); i += blockDim.x) dst[i] = src[i];
+    }
+    for (uint32_t i = threadIdx.x; i < kWarps * kBasketScen * 2; i += blockDim.x) (&slots[0][0][0])[i] = 0.0;
+    __syncthreads();
+    const uint64_t first = (uint64_t)t * sq.tile_units;
+    const uint64_t last = min(first + (uint64_t)sq.tile_units, sq.n_units);
+    const uint32_t iters = (uint32_t)((last - first + blockDim.x - 1) / blockDim.x);
+    for (uint32_t it = 0; it < iters; ++it) {
+      uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
+      const bool valid = u < last;
+      if (!valid) u = first;  // keeps block-synchronous sources in lockstep; discarded below
+      typename FusedUnitSource<FAM_BASKET, SMP>::type src;  // the samples fused_unit<FAM_BASKET, SMP> draws
+      src.template begin<false>(sq, ctx, u);
+      float pay[kBasketScen];
+      scen_basket(sq, src, legs, pay);
+#pragma unroll
+      for (int s = 0; s < kBasketScen; ++s) {
+        const double p = valid ? (double)pay[s] : 0.0;
+        const double a = warp_sum(p), b = warp_sum(p * p);
+        if (lane == 0) {
+          slots[warp][s][0] += a;
+          slots[warp][s][1] += b;
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x < (uint32_t)(2 * kBasketScen)) {
+      const int s = threadIdx.x >> 1, k = threadIdx.x & 1;
+      double sum = 0.0;
+      for (int w = 0; w < kWarps; ++w) sum += slots[w][s][k];
+      sq.partials[((size_t)t * kBasketScen + s) * 2 + k] = sum;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = (atomicAdd(sq.tiles_done, 1u) == n_tiles - 1) ? 1 : 0;
+    __syncthreads();
+    if (s_last) {
+      __threadfence();
+      if (threadIdx.x < (uint32_t)(2 * kBasketScen)) {
+        const int s = threadIdx.x >> 1, k = threadIdx.x & 1;
+        double sum = 0.0;
+        for (uint32_t tt = 0; tt < n_tiles; ++tt)
+          sum += __ldcg(sq.partials + ((size_t)tt * kBasketScen + s) * 2 + k);
+        sq.moments[s * 2 + k] = sum;
+      }
+      if (threadIdx.x == 0) *sq.tiles_done = 0u;
+    }
+    __syncthreads();
+  }
+}
+
+// The Sobol instance's window and inverse-normal table (46,592 bytes) plus
+// the static descriptor and 13-leg slots pass the 48 KB default, so the
+// dynamic size is raised once per device (the attribute is per device).
+template <int SMP>
+static cudaError_t basket_scen_attr() {
+  static std::atomic<bool> done[64];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64 && done[dev].load()) return cudaSuccess;
+  e = cudaFuncSetAttribute(basket_scenario_kernel<SMP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)fused_dynamic_smem<SMP>());
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(true);
+  return e;
+}
+
+template <int SMP>
+static cudaError_t launch_basket_scen_s(const DevReq* d_req, uint32_t n_tiles, uint32_t* counter, const SrcCtx& ctx,
+                                        const BasketScen& legs, int grid, cudaStream_t stream) {
+  const cudaError_t e = basket_scen_attr<SMP>();
+  if (e != cudaSuccess) return e;
+  basket_scenario_kernel<SMP><<<grid, kFusedBlock, fused_dynamic_smem<SMP>(), stream>>>(d_req, n_tiles, counter, ctx,
+                                                                                        legs);
+  count_launch();
+  return cudaGetLastError();
+}
+
+template <int SMP>
+static int basket_scen_occ() {
+  int n = 0;
+  if (basket_scen_attr<SMP>() != cudaSuccess) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, basket_scenario_kernel<SMP>, kFusedBlock, fused_dynamic_smem<SMP>());
+  return n;
+}
+
+int basket_scenario_max_blocks_per_sm(int sampler) {
+  if (sampler == SMP_XORSHIFT) return basket_scen_occ<SMP_XORSHIFT>();
+  if (sampler == SMP_SOBOL) return basket_scen_occ<SMP_SOBOL>();
+  if (sampler == SMP_COUNTER) return basket_scen_occ<SMP_COUNTER>();
+  return 0;
+}
+
+cudaError_t launch_basket_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_counter, int sampler,
+                                    const BasketScen& legs, const DeviceTables& tabs, int grid, cudaStream_t stream) {
+  SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
+  switch (sampler) {
+    case SMP_XORSHIFT:
+      return launch_basket_scen_s<SMP_XORSHIFT>(d_req, n_tiles, d_counter, ctx, legs, grid, stream);
+    case SMP_SOBOL:
+      return launch_basket_scen_s<SMP_SOBOL>(d_req, n_tiles, d_counter, ctx, legs, grid, stream);
+    case SMP_COUNTER:
+      return launch_basket_scen_s<SMP_COUNTER>(d_req, n_tiles, d_counter, ctx, legs, grid, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
 // ------------------------------------------------------ FP64 plain path ---
 __device__ __forceinline__ bool is_uniform_dim(const DevReq& q, uint32_t d) {
   return (q.family == FAM_MERTON_STEP || q.family == FAM_MERTON_TERMINAL) && (d % 3u) == 1u;

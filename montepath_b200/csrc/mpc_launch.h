@@ -92,6 +92,13 @@ cudaError_t launch_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_
                              const DeviceTables& tabs, int grid, cudaStream_t stream);
 int scenario_max_blocks_per_sm(int family, int sampler);
 
+// Basket bump legs sharing every normal: one basket request d_req
+// (xorshift, Sobol or counter-hash samples); q.partials must hold
+// [n_tiles][kBasketScen][2] doubles and q.moments [kBasketScen][2].
+cudaError_t launch_basket_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_counter, int sampler,
+                                    const BasketScen& legs, const DeviceTables& tabs, int grid, cudaStream_t stream);
+int basket_scenario_max_blocks_per_sm(int sampler);
+
 // Single-pass Greek estimators of the terminal-GBM European call
 // (pathwise: delta, vega, rho, theta; likelihood ratio: delta, vega, rho)
 // over the pseudorandom terminal shocks of one MonteCarloRng stream.

@@ -30,6 +30,20 @@ constexpr uint32_t kBridgeMaxSteps = 65536;
 constexpr int kMaxScen = 9;
 constexpr int kScenFields = 6;
 
+// Basket bump legs (base, then up and down for two spots, two volatilities,
+// the rate and the maturity).  The basket payoff reads only terminal values,
+// and each leg's log return of asset a is affine in the same correlated
+// normal sum, x_a = (r - sigma_a^2 / 2) T + sigma_a sqrt(dt) W_a, so the
+// legs share W and differ only in these per-leg constants (float, read from
+// the kernel's parameter bank).
+constexpr int kBasketScen = 13;
+struct BasketScen {
+  float log_drift[kBasketScen][8];  // (r - sigma_a^2 / 2) T
+  float step_vol[kBasketScen][8];   // sigma_a sqrt(dt)
+  float wspot[kBasketScen][8];      // weight_a * spot_a
+  float discount[kBasketScen];      // exp(-r T)
+};
+
 // Kernel families: the model-specific loop a tile runs.
 enum Family : int32_t {
   FAM_GBM_STEP = 0,

@@ -548,6 +548,48 @@ def test_scenario_bump_legs_equal_separate_pricing(backend, workload, kw):
     assert abs(delta.bumped_down_price - backend.price(down).price) <= 1e-7 * abs(delta.bumped_down_price)
 
 
+_BASKET5 = {"spots": [100.0, 95.0, 105.0, 90.0, 110.0], "sigmas": [0.2, 0.25, 0.3, 0.35, 0.4], "corr": 0.3}
+
+
+@pytest.mark.parametrize("kw", [
+    {},
+    {"method": "stepwise", "n_steps": 16, "sampling": "scrambled_sobol", **_BASKET5},
+    {"method": "stepwise", "n_steps": 7, "sampling": "counter_hash", "spots": [100.0, 90.0, 110.0]},
+    {"method": "stepwise", "n_steps": 3, "sampling": "pseudorandom", **_BASKET5, "k": 80.0},
+])
+def test_basket_scenario_legs_equal_separate_pricing(backend, kw):
+    """The 13 FP32 basket legs share each path's normal sums in one launch and
+    price like the same legs priced one by one.  The scenario kernel regroups
+    each asset's log return as T drift + sigma sqrt(dt) (L sum z) instead of
+    summing the steps, so FP32 rounding differs per path: leg prices agree to
+    2e-5 relative; the Greeks agree with the FP64-plain Greeks of the same
+    normals to 0.5 of their standard error."""
+
+    r = req("basket_call", n_paths=30000, seed=23, **kw)
+    rep = backend.greeks(r, "bump_and_revalue")
+    base = backend.price(r)
+    assert abs(rep.base_price - base.price) <= 2e-5 * abs(base.price)
+    assert abs(rep.base_stderr - base.stderr) <= 2e-4 * base.stderr
+    fields = {abi.GREEK_DELTA: ("spots", 0), abi.GREEK_DELTA2: ("spots", 1), abi.GREEK_VEGA: ("sigmas", 0),
+              abi.GREEK_VEGA2: ("sigmas", 1), abi.GREEK_RHO: ("r", None), abi.GREEK_THETA: ("t", None)}
+    est = _estimates(rep)
+    assert set(est) == set(fields)
+    for greek, (name, idx) in fields.items():
+        e = est[greek]
+        for sign, want in ((1.0, e.bumped_up_price), (-1.0, e.bumped_down_price)):
+            leg = abi.Request.from_buffer_copy(r)
+            if idx is None:
+                setattr(leg, name, getattr(r, name) + sign * e.bump_size)
+            else:
+                getattr(leg, name)[idx] = getattr(r, name)[idx] + sign * e.bump_size
+            got = backend.price(leg).price
+            assert abs(want - got) <= 2e-5 * abs(got), (greek, sign, want, got)
+    r64 = req("basket_call", n_paths=30000, seed=23, precision="fp64_plain", **kw)
+    ref = _estimates(backend.greeks(r64, "bump_and_revalue"))
+    for greek, e in ref.items():
+        assert abs(est[greek].value - e.value) < 0.5 * e.stderr, (greek, est[greek].value, e.value, e.stderr)
+
+
 def test_greeks_unsupported_cases(backend):
     from montepath_b200.backend import BackendError
 
