@@ -81,3 +81,37 @@ def replay(backend: CudaBackend, stream: Sequence[tuple[float, str, abi.Request]
         "mlmc_step_cap_hit": sum(1 for k, _, r in results if k == "asian_mlmc" and r.max_step_updates_hit),
         "mlmc_stderr_p50": pct(sorted(r.stderr for k, _, r in results if k == "asian_mlmc"), 0.5),
     }
+
+
+def main(argv: Sequence[str] | None = None) -> None:
+    """``python -m montepath_b200.serving``: replays a seeded Poisson stream
+    (default: 2,000 requests/s for 60 s, 64 GB budget) through the
+    continuous-batching server and prints the summary as one JSON line."""
+
+    import argparse
+    import json
+
+    from . import workloads
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--seconds", type=float, default=60.0, help="arrival window of the stream")
+    ap.add_argument("--rate", type=float, default=2000.0, help="mean arrivals per second")
+    ap.add_argument("--seed", type=int, default=42)
+    ap.add_argument("--budget-gb", type=float, default=64.0, help="HBM budget of the server")
+    ap.add_argument("--plain", action="store_true", help="plain FIFO FP64 server, one request per launch")
+    ap.add_argument("--out", default="", help="also write the summary to this file")
+    args = ap.parse_args(argv)
+    stream = workloads.serving_stream(args.seed, rate=args.rate, duration_s=args.seconds,
+                                      precision="fp64_plain" if args.plain else "fp32_path")
+    with CudaBackend(0) as backend:
+        summary = replay(backend, stream, plain=args.plain, hbm_budget_bytes=int(args.budget_gb * (1 << 30)))
+    summary.update({"rate": args.rate, "seed": args.seed, "budget_gb": args.budget_gb})
+    line = json.dumps(summary)
+    print(line)
+    if args.out:
+        with open(args.out, "w") as f:
+            f.write(line + "\n")
+
+
+if __name__ == "__main__":
+    main()
