@@ -4,11 +4,11 @@
 // european_call_greeks_cpu and siblings 4036-4356, bump recipe 4938-5008,
 // single-pass estimators 4670-4869) on the device:
 //  - bump-and-revalue: the base request plus an up and a down bump per Greek,
-//    all with the request's seed (common random numbers).  FP32 requests of
-//    the standard technique with xorshift, Sobol or counter-hash samples
-//    price all 9 legs (13 for a basket) in one scenario launch that draws
-//    each normal once for every leg; the others price their legs with one
-//    mpc_price_batch call;
+//    all with the request's seed (common random numbers).  FP32 requests
+//    with xorshift, Sobol or counter-hash samples (any technique; a basket
+//    with the standard one) price all 9 legs (13 for a basket) in one
+//    scenario launch that draws each normal once for every leg; the others
+//    price their legs with one mpc_price_batch call;
 //  - pathwise / likelihood ratio: one kernel pass over the pseudorandom
 //    terminal shocks of the request's seed, sums in FP64.
 
@@ -131,13 +131,14 @@ void mean_stderr(double sum, double sq, uint64_t count, double* mean, double* se
 }
 
 // Whether the legs of a bump report can share their normals in one
-// scenario launch: FP32 path, standard technique, a family the scenario
-// kernel runs, a sampler whose normals depend only on (point, dimension).
+// scenario launch: FP32 path, a family the scenario kernel runs (any
+// technique; a basket with the standard one), a sampler whose normals depend
+// only on (point, dimension).
 bool scenario_eligible(const Prepared& p, const mpc_request_t& r, size_t legs) {
-  if (r.precision != MPC_PRECISION_FP32_PATH || r.technique != MPC_TECHNIQUE_STANDARD) return false;
+  if (r.precision != MPC_PRECISION_FP32_PATH) return false;
   if (p.q.bridge) return false;
   if (p.family == FAM_BASKET) {
-    if (legs > size_t(kBasketScen)) return false;
+    if (legs > size_t(kBasketScen) || r.technique != MPC_TECHNIQUE_STANDARD) return false;
   } else {
     if (legs > size_t(kMaxScen)) return false;
     if (p.family != FAM_GBM_STEP && p.family != FAM_GBM_TERMINAL && p.family != FAM_HESTON) return false;
@@ -173,6 +174,8 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
   const int n_scen = int(legs.size());
   const bool basket = base.family == FAM_BASKET;
   const int slots = basket ? kBasketScen : kMaxScen;  // legs per tile partial
+  const int technique = legs[0].technique;
+  const int nm = basket ? 2 : scenario_moments(technique);  // moments per leg
   float scen[kScenFields * kMaxScen];
   for (int s = 0; s < kMaxScen && !basket; ++s) {
     const DevReq& q = preps[s < n_scen ? s : 0].q;
@@ -199,8 +202,8 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
   // device layout: descriptor | leg parameters | partials | moments | counters (done, tile counter)
   const size_t o_scen = 256 * ((sizeof(DevReq) + 255) / 256);
   const size_t o_part = o_scen + 256;
-  const size_t o_mom = o_part + ((n_tiles * slots * 2 * sizeof(double) + 255) / 256) * 256;
-  const size_t o_cnt = o_mom + 256;
+  const size_t o_mom = o_part + ((n_tiles * slots * nm * sizeof(double) + 255) / 256) * 256;
+  const size_t o_cnt = o_mom + ((size_t(slots) * nm * sizeof(double) + 255) / 256) * 256;
   void* d = nullptr;
   int st = scratch(ctx, "scenarios", o_cnt + 256, &d);
   if (st != MPC_OK) return st;
@@ -211,8 +214,8 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
   q.tiles_done = reinterpret_cast<uint32_t*>(base_ptr + o_cnt);
   q.per_unit = nullptr;
   uint32_t* counter = q.tiles_done + 1;
-  double host_mom[kBasketScen * 2];
-  static_assert(kBasketScen * 2 * sizeof(double) <= 256 && kBasketScen >= kMaxScen, "moments area");
+  double host_mom[kBasketScen * 5];
+  static_assert(kBasketScen >= kMaxScen, "moments buffer");
   auto fin = [&](cudaError_t e, const char* what) { return e == cudaSuccess ? MPC_OK : cuda_fail(ctx, e, what); };
   if ((st = fin(cudaMemsetAsync(q.tiles_done, 0, 2 * sizeof(uint32_t), ctx->stream), "memset counters"))) return st;
   if ((st = fin(cudaMemcpyAsync(base_ptr, &q, sizeof(q), cudaMemcpyHostToDevice, ctx->stream), "descriptor"))) return st;
@@ -220,17 +223,18 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
                            "leg parameters")))
     return st;
   const int occ = std::max(1, basket ? basket_scenario_max_blocks_per_sm(base.sampler)
-                                     : scenario_max_blocks_per_sm(base.family, base.sampler));
+                                     : scenario_max_blocks_per_sm(base.family, base.sampler, technique));
   const int grid = int(std::min<uint64_t>(n_tiles, uint64_t(ctx->sm_count) * occ));
   if ((st = fin(cudaEventRecord(ctx->ev_start, ctx->stream), "event"))) return st;
   const DevReq* d_req = reinterpret_cast<const DevReq*>(base_ptr);
   const cudaError_t launched =
       basket ? launch_basket_scenarios(d_req, q.n_tiles, counter, base.sampler, basket_legs(preps), ctx->tabs, grid,
                                        ctx->stream)
-             : launch_scenarios(d_req, q.n_tiles, counter, base.family, base.sampler, ctx->tabs, grid, ctx->stream);
+             : launch_scenarios(d_req, q.n_tiles, counter, base.family, base.sampler, technique, ctx->tabs, grid,
+                                ctx->stream);
   if ((st = fin(launched, "scenario kernel"))) return st;
   if ((st = fin(cudaEventRecord(ctx->ev_stop, ctx->stream), "event"))) return st;
-  if ((st = fin(cudaMemcpyAsync(host_mom, q.moments, size_t(slots) * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+  if ((st = fin(cudaMemcpyAsync(host_mom, q.moments, size_t(slots) * nm * sizeof(double), cudaMemcpyDeviceToHost,
                                 ctx->stream),
                 "moments")))
     return st;
@@ -239,13 +243,12 @@ int run_scenario_legs(mpc_context* ctx, const std::vector<mpc_request_t>& legs, 
   cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
   ctx->last_ms = ms;
   res.assign(legs.size(), mpc_result_t{});
-  const double n = double(q.n_units);
-  for (int s = 0; s < n_scen; ++s) {  // summarize_payoffs (cpu.rs:7641-7652)
-    const double mean = host_mom[2 * s] / n;
-    const double var = std::max(host_mom[2 * s + 1] / n - mean * mean, 0.0);
-    res[s].price = mean;
-    res[s].stderr = std::sqrt(var) / std::sqrt(n);
-    res[s].n_samples = q.n_units;
+  for (int s = 0; s < n_scen; ++s) {
+    // the fused path's moments layout (count, sum p, sum p^2, sum c, sum c^2,
+    // sum p c), summarised by the request's own estimator (cpu.rs:7641-7771)
+    double m[MPC_MOMENTS] = {double(q.n_units), 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < nm; ++k) m[1 + k] = host_mom[s * nm + k];
+    summarize_moments(preps[s], m, &res[s]);
     res[s].path_steps = preps[s].path_steps;
     res[s].runtime_ms = ms;
     res[s].status = MPC_OK;

@@ -18,6 +18,9 @@
 // and exercise decisions are applied in registers.
 
 #include <atomic>
+#include <mutex>
+#include <set>
+#include <utility>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -1251,6 +1254,23 @@ int fused_max_blocks_per_sm(int family, int sampler, int block) {
   }
 }
 
+// Raises a kernel's dynamic shared memory limit to `bytes` once per device
+// (the attribute is per device).  Kernels whose Sobol window and
+// inverse-normal table (46,592 bytes) plus their static shared memory pass
+// the 48 KB default need it before their first launch and occupancy query.
+static cudaError_t allow_dynamic_smem(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count({fn, dev})) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done.insert({fn, dev});
+  return e;
+}
+
 // ------------------------------------------------ scenario (bump) kernel ---
 // Bump-and-revalue Greeks with common random numbers: every leg of the
 // recipe (base, then up and down per Greek) has the same seed, so every leg
@@ -1259,15 +1279,24 @@ int fused_max_blocks_per_sm(int family, int sampler, int block) {
 // the same arithmetic as the single-request unit of its family.  Per unit the
 // legs' payoffs are warp-summed (FP64 sum and sum of squares) into per-warp
 // shared slots; per tile the slots are summed in warp order into tile
-// partials [tile][leg][2], and the last tile sums those in tile order.
+// partials [tile][leg][NM], and the last tile sums those in tile order.
+// TECH follows the request's technique: antithetic legs also run the mirrored
+// path (-z) and record the pair average, as unit_* does; control-variate legs
+// also record the discounted terminal price c with sum c, sum c^2 and sum p c
+// (NM = 5 moments per leg instead of 2).
 // Scenario parameters, struct of arrays [field][kMaxScen] (float):
 //   GBM:    log_s0, s0, drift_dt, vol_dt, discount, knocked-out-at-start (0/1)
 //   Heston: log_s0, v0, rate, dt, sqrt_dt, discount
-template <int W, class Src>
+constexpr int kScenStd = MPC_TECHNIQUE_STANDARD, kScenAnti = MPC_TECHNIQUE_ANTITHETIC,
+              kScenCv = MPC_TECHNIQUE_CONTROL_VARIATE;
+
+template <int W, int TECH, class Src>
 __device__ __forceinline__ void scen_gbm_step(const DevReq& q, Src& src, const float* __restrict__ sp, int n_scen,
-                                              float pay[kMaxScen]) {
+                                              float pay[kMaxScen], float pay2[kMaxScen], float ctl[kMaxScen]) {
+  constexpr bool ANTI = TECH == kScenAnti;
   float ls[kMaxScen], acc[kMaxScen], drift[kMaxScen], vol[kMaxScen];
-  bool ko[kMaxScen];
+  float ls2[kMaxScen], acc2[kMaxScen];  // mirrored paths (antithetic)
+  bool ko[kMaxScen], ko2[kMaxScen];
 #pragma unroll
   for (int s = 0; s < kMaxScen; ++s) {
     ls[s] = __ldg(sp + 0 * kMaxScen + s);
@@ -1275,6 +1304,11 @@ __device__ __forceinline__ void scen_gbm_step(const DevReq& q, Src& src, const f
     drift[s] = __ldg(sp + 2 * kMaxScen + s);
     vol[s] = __ldg(sp + 3 * kMaxScen + s);
     ko[s] = __ldg(sp + 5 * kMaxScen + s) != 0.0f;
+    if constexpr (ANTI) {
+      ls2[s] = ls[s];
+      acc2[s] = acc[s];
+      ko2[s] = ko[s];
+    }
   }
   const float lbar = (float)q.log_barrier;
   const uint32_t n = q.n_steps;
@@ -1289,42 +1323,64 @@ __device__ __forceinline__ void scen_gbm_step(const DevReq& q, Src& src, const f
       else if constexpr (W == W_LOOKBACK) acc[s] = acc[s] > __expf(ls[s]) ? acc[s] : __expf(ls[s]);
       else if constexpr (W == W_DAO) ko[s] |= ls[s] <= lbar;
       else if constexpr (W == W_UAO) ko[s] |= ls[s] >= lbar;
+      if constexpr (ANTI) {
+        ls2[s] += drift[s] - vol[s] * z;
+        if constexpr (W == W_ASIAN) acc2[s] += __expf(ls2[s]);
+        else if constexpr (W == W_LOOKBACK) acc2[s] = acc2[s] > __expf(ls2[s]) ? acc2[s] : __expf(ls2[s]);
+        else if constexpr (W == W_DAO) ko2[s] |= ls2[s] <= lbar;
+        else if constexpr (W == W_UAO) ko2[s] |= ls2[s] >= lbar;
+      }
     }
   }
   const float kk = (float)q.k, inv_n = (float)(1.0 / (double)n);
+  auto payoff = [&](float l, float a, bool out, float disc) {
+    float v;
+    if constexpr (W == W_ASIAN) v = a * inv_n - kk;
+    else if constexpr (W == W_LOOKBACK) v = a - kk;
+    else {
+      v = __expf(l) - kk;
+      if (out) v = 0.0f;
+    }
+    return (v > 0.0f ? v : 0.0f) * disc;
+  };
 #pragma unroll
   for (int s = 0; s < kMaxScen; ++s) {
-    float v;
-    if constexpr (W == W_ASIAN) v = acc[s] * inv_n - kk;
-    else if constexpr (W == W_LOOKBACK) v = acc[s] - kk;
-    else {
-      v = __expf(ls[s]) - kk;
-      if (ko[s]) v = 0.0f;
-    }
-    pay[s] = (v > 0.0f ? v : 0.0f) * __ldg(sp + 4 * kMaxScen + s);
+    const float disc = __ldg(sp + 4 * kMaxScen + s);
+    pay[s] = payoff(ls[s], acc[s], ko[s], disc);
+    if constexpr (ANTI) pay2[s] = payoff(ls2[s], acc2[s], ko2[s], disc);
+    if constexpr (TECH == kScenCv) ctl[s] = disc * __expf(ls[s]);
   }
 }
 
-template <class Src>
+template <int TECH, class Src>
 __device__ __forceinline__ void scen_gbm_terminal(const DevReq& q, Src& src, const float* __restrict__ sp, int n_scen,
-                                                  float pay[kMaxScen]) {
+                                                  float pay[kMaxScen], float pay2[kMaxScen], float ctl[kMaxScen]) {
   src.at_step(0, 1);
   const float z = normal<float>(src, 0);
   const float kk = (float)q.k;
 #pragma unroll
   for (int s = 0; s < kMaxScen; ++s) {
-    const float st = __ldg(sp + 1 * kMaxScen + s) * __expf(__ldg(sp + 2 * kMaxScen + s) + __ldg(sp + 3 * kMaxScen + s) * z);
-    pay[s] = (st - kk > 0.0f ? st - kk : 0.0f) * __ldg(sp + 4 * kMaxScen + s);
+    const float s0 = __ldg(sp + 1 * kMaxScen + s), drift = __ldg(sp + 2 * kMaxScen + s),
+                vol = __ldg(sp + 3 * kMaxScen + s), disc = __ldg(sp + 4 * kMaxScen + s);
+    const float st = s0 * __expf(drift + vol * z);
+    pay[s] = (st - kk > 0.0f ? st - kk : 0.0f) * disc;
+    if constexpr (TECH == kScenAnti) {
+      const float sb = s0 * __expf(drift + vol * (-z));
+      pay2[s] = (sb - kk > 0.0f ? sb - kk : 0.0f) * disc;
+    }
+    if constexpr (TECH == kScenCv) ctl[s] = disc * st;
   }
   (void)n_scen;
 }
 
-template <class Src>
+template <int TECH, class Src>
 __device__ __forceinline__ void scen_heston(const DevReq& q, Src& src, const float* __restrict__ sp, int n_scen,
-                                            float pay[kMaxScen]) {
+                                            float pay[kMaxScen], float pay2[kMaxScen], float ctl[kMaxScen]) {
+  constexpr bool ANTI = TECH == kScenAnti;
   const float kappa = (float)q.kappa, theta = (float)q.theta, xi = (float)q.xi, rho = (float)q.rho,
               rho_perp = (float)q.rho_perp;
   float ls[kMaxScen], v[kMaxScen], rate[kMaxScen], dt[kMaxScen], sqdt[kMaxScen];
+  float ls2[kMaxScen], v2[kMaxScen];  // mirrored paths (antithetic)
 #pragma unroll
   for (int s = 0; s < kMaxScen; ++s) {
     ls[s] = __ldg(sp + 0 * kMaxScen + s);
@@ -1332,7 +1388,18 @@ __device__ __forceinline__ void scen_heston(const DevReq& q, Src& src, const flo
     rate[s] = __ldg(sp + 2 * kMaxScen + s);
     dt[s] = __ldg(sp + 3 * kMaxScen + s);
     sqdt[s] = __ldg(sp + 4 * kMaxScen + s);
+    if constexpr (ANTI) {
+      ls2[s] = ls[s];
+      v2[s] = v[s];
+    }
   }
+  auto step = [&](float& l, float& var, int s, float zp, float zv) {
+    const float vp = var > 0.0f ? var : 0.0f;
+    const float sv = sqrt_approx(vp);
+    l += (rate[s] - 0.5f * vp) * dt[s] + sv * sqdt[s] * zp;
+    var = var + kappa * (theta - vp) * dt[s] + xi * sv * sqdt[s] * zv;
+    var = var > 0.0f ? var : 0.0f;
+  };
   const uint32_t n = q.n_steps;
   for (uint32_t st = 0; st < n; ++st) {
     src.at_step(2 * st, 2);
@@ -1342,53 +1409,58 @@ __device__ __forceinline__ void scen_heston(const DevReq& q, Src& src, const flo
 #pragma unroll
     for (int s = 0; s < kMaxScen; ++s) {
       if (s >= n_scen) break;
-      const float vp = v[s] > 0.0f ? v[s] : 0.0f;
-      const float sv = sqrt_approx(vp);
-      ls[s] += (rate[s] - 0.5f * vp) * dt[s] + sv * sqdt[s] * zp;
-      v[s] = v[s] + kappa * (theta - vp) * dt[s] + xi * sv * sqdt[s] * zv;
-      v[s] = v[s] > 0.0f ? v[s] : 0.0f;
+      step(ls[s], v[s], s, zp, zv);
+      if constexpr (ANTI) step(ls2[s], v2[s], s, rho * (-zv) + rho_perp * (-zi), -zv);
     }
   }
   const float kk = (float)q.k;
 #pragma unroll
   for (int s = 0; s < kMaxScen; ++s) {
+    const float disc = __ldg(sp + 5 * kMaxScen + s);
     const float stv = __expf(ls[s]);
-    pay[s] = (stv - kk > 0.0f ? stv - kk : 0.0f) * __ldg(sp + 5 * kMaxScen + s);
+    pay[s] = (stv - kk > 0.0f ? stv - kk : 0.0f) * disc;
+    if constexpr (ANTI) {
+      const float sb = __expf(ls2[s]);
+      pay2[s] = (sb - kk > 0.0f ? sb - kk : 0.0f) * disc;
+    }
+    if constexpr (TECH == kScenCv) ctl[s] = stv * disc;
   }
 }
 
-template <int FAM, class Src>
-__device__ __forceinline__ void scen_unit(const DevReq& q, Src& src, int n_scen, float pay[kMaxScen]) {
+template <int FAM, int TECH, class Src>
+__device__ __forceinline__ void scen_unit(const DevReq& q, Src& src, int n_scen, float pay[kMaxScen],
+                                          float pay2[kMaxScen], float ctl[kMaxScen]) {
   const float* sp = q.scen;
   if constexpr (FAM == FAM_HESTON) {
-    scen_heston(q, src, sp, n_scen, pay);
+    scen_heston<TECH>(q, src, sp, n_scen, pay, pay2, ctl);
   } else if constexpr (FAM == FAM_GBM_TERMINAL) {
-    scen_gbm_terminal(q, src, sp, n_scen, pay);
+    scen_gbm_terminal<TECH>(q, src, sp, n_scen, pay, pay2, ctl);
   } else {
     switch (q.workload) {
       case W_ASIAN:
-        scen_gbm_step<W_ASIAN>(q, src, sp, n_scen, pay);
+        scen_gbm_step<W_ASIAN, TECH>(q, src, sp, n_scen, pay, pay2, ctl);
         break;
       case W_DAO:
-        scen_gbm_step<W_DAO>(q, src, sp, n_scen, pay);
+        scen_gbm_step<W_DAO, TECH>(q, src, sp, n_scen, pay, pay2, ctl);
         break;
       case W_UAO:
-        scen_gbm_step<W_UAO>(q, src, sp, n_scen, pay);
+        scen_gbm_step<W_UAO, TECH>(q, src, sp, n_scen, pay, pay2, ctl);
         break;
       case W_LOOKBACK:
-        scen_gbm_step<W_LOOKBACK>(q, src, sp, n_scen, pay);
+        scen_gbm_step<W_LOOKBACK, TECH>(q, src, sp, n_scen, pay, pay2, ctl);
         break;
       default:
-        scen_gbm_step<W_EURO>(q, src, sp, n_scen, pay);
+        scen_gbm_step<W_EURO, TECH>(q, src, sp, n_scen, pay, pay2, ctl);
         break;
     }
   }
 }
 
 // One request (reqs[0]) split into n_tiles tiles of q.tile_units units.
-template <int FAM, int SMP>
+template <int FAM, int SMP, int TECH>
 __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* __restrict__ reqs, uint32_t n_tiles,
                                                                  uint32_t* __restrict__ counter, SrcCtx ctx) {
+  constexpr int NM = TECH == kScenCv ? 5 : 2;  // moments per leg
   extern __shared__ __align__(16) uint32_t sobol_window[];
   if constexpr (SMP == SMP_SOBOL) {
     float4* seg = reinterpret_cast<float4*>(sobol_window + kSobolWindowWords);
@@ -1401,7 +1473,7 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
     ctx.icdf = nullptr;
   }
   __shared__ DevReq sq;
-  __shared__ double slots[kWarps][kMaxScen][2];
+  __shared__ double slots[kWarps][kMaxScen][NM];
   __shared__ uint32_t s_tile;
   __shared__ int s_last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1415,7 +1487,7 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
       uint4* dst = reinterpret_cast<uint4*>(&sq);
       for (uint32_t i = threadIdx.x; i < sizeof(DevReq) / sizeof(uint4); i += blockDim.x) dst[i] = src[i];
     }
-    for (uint32_t i = threadIdx.x; i < kWarps * kMaxScen * 2; i += blockDim.x) (&slots[0][0][0])[i] = 0.0;
+    for (uint32_t i = threadIdx.x; i < kWarps * kMaxScen * NM; i += blockDim.x) (&slots[0][0][0])[i] = 0.0;
     __syncthreads();
     const int n_scen = (int)sq.n_scen;
     const uint64_t first = (uint64_t)t * sq.tile_units;
@@ -1427,13 +1499,24 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
       if (!valid) u = first;  // keeps block-synchronous sources in lockstep; discarded below
       typename FusedUnitSource<FAM, SMP>::type src;  // the samples fused_unit<FAM, SMP> draws
       src.template begin<false>(sq, ctx, u);
-      float pay[kMaxScen];
-      scen_unit<FAM>(sq, src, n_scen, pay);
+      float pay[kMaxScen], pay2[kMaxScen], ctl[kMaxScen];
+      scen_unit<FAM, TECH>(sq, src, n_scen, pay, pay2, ctl);
 #pragma unroll
       for (int s = 0; s < kMaxScen; ++s) {
         if (s >= n_scen) break;
-        const double p = valid ? (double)pay[s] : 0.0;
+        double p = (double)pay[s];
+        if constexpr (TECH == kScenAnti) p = 0.5 * ((double)pay[s] + (double)pay2[s]);
+        if (!valid) p = 0.0;
         const double a = warp_sum(p), b = warp_sum(p * p);
+        if constexpr (TECH == kScenCv) {
+          const double c = valid ? (double)ctl[s] : 0.0;
+          const double cs = warp_sum(c), cc = warp_sum(c * c), pc = warp_sum(p * c);
+          if (lane == 0) {
+            slots[warp][s][2] += cs;
+            slots[warp][s][3] += cc;
+            slots[warp][s][4] += pc;
+          }
+        }
         if (lane == 0) {
           slots[warp][s][0] += a;
           slots[warp][s][1] += b;
@@ -1441,11 +1524,11 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
       }
     }
     __syncthreads();
-    if (threadIdx.x < (uint32_t)(2 * n_scen)) {
-      const int s = threadIdx.x >> 1, k = threadIdx.x & 1;
+    if (threadIdx.x < (uint32_t)(NM * n_scen)) {
+      const int s = threadIdx.x / NM, k = threadIdx.x % NM;
       double sum = 0.0;
       for (int w = 0; w < kWarps; ++w) sum += slots[w][s][k];
-      sq.partials[((size_t)t * kMaxScen + s) * 2 + k] = sum;
+      sq.partials[((size_t)t * kMaxScen + s) * NM + k] = sum;
     }
     __threadfence();
     __syncthreads();
@@ -1453,11 +1536,11 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
     __syncthreads();
     if (s_last) {
       __threadfence();
-      if (threadIdx.x < (uint32_t)(2 * n_scen)) {
-        const int s = threadIdx.x >> 1, k = threadIdx.x & 1;
+      if (threadIdx.x < (uint32_t)(NM * n_scen)) {
+        const int s = threadIdx.x / NM, k = threadIdx.x % NM;
         double sum = 0.0;
-        for (uint32_t tt = 0; tt < n_tiles; ++tt) sum += __ldcg(sq.partials + ((size_t)tt * kMaxScen + s) * 2 + k);
-        sq.moments[s * 2 + k] = sum;
+        for (uint32_t tt = 0; tt < n_tiles; ++tt) sum += __ldcg(sq.partials + ((size_t)tt * kMaxScen + s) * NM + k);
+        sq.moments[s * NM + k] = sum;
       }
       if (threadIdx.x == 0) *sq.tiles_done = 0u;
     }
@@ -1465,56 +1548,83 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
   }
 }
 
-template <int SMP>
-static cudaError_t launch_scen_s(int family, const DevReq* d_req, uint32_t n_tiles, uint32_t* counter,
-                                 const SrcCtx& ctx, int grid, cudaStream_t stream) {
-  const size_t smem = fused_dynamic_smem<SMP>();
+using ScenarioKernel = void (*)(const DevReq*, uint32_t, uint32_t*, SrcCtx);
+template <int SMP, int TECH>
+static ScenarioKernel scenario_kernel_of(int family) {
   switch (family) {
     case FAM_GBM_STEP:
-      scenario_kernel<FAM_GBM_STEP, SMP><<<grid, kFusedBlock, smem, stream>>>(d_req, n_tiles, counter, ctx);
-      break;
+      return scenario_kernel<FAM_GBM_STEP, SMP, TECH>;
     case FAM_GBM_TERMINAL:
-      scenario_kernel<FAM_GBM_TERMINAL, SMP><<<grid, kFusedBlock, smem, stream>>>(d_req, n_tiles, counter, ctx);
-      break;
+      return scenario_kernel<FAM_GBM_TERMINAL, SMP, TECH>;
     case FAM_HESTON:
-      scenario_kernel<FAM_HESTON, SMP><<<grid, kFusedBlock, smem, stream>>>(d_req, n_tiles, counter, ctx);
-      break;
+      return scenario_kernel<FAM_HESTON, SMP, TECH>;
     default:
-      return cudaErrorInvalidValue;
+      return nullptr;
   }
+}
+
+template <int SMP, int TECH>
+static cudaError_t launch_scen_t(int family, const DevReq* d_req, uint32_t n_tiles, uint32_t* counter,
+                                 const SrcCtx& ctx, int grid, cudaStream_t stream) {
+  const size_t smem = fused_dynamic_smem<SMP>();
+  const ScenarioKernel kernel = scenario_kernel_of<SMP, TECH>(family);
+  if (!kernel) return cudaErrorInvalidValue;
+  const cudaError_t e = allow_dynamic_smem((const void*)kernel, smem);
+  if (e != cudaSuccess) return e;
+  kernel<<<grid, kFusedBlock, smem, stream>>>(d_req, n_tiles, counter, ctx);
   count_launch();
   return cudaGetLastError();
 }
 
 template <int SMP>
-static int scen_occ_s(int family) {
+static cudaError_t launch_scen_s(int family, int technique, const DevReq* d_req, uint32_t n_tiles,
+                                 uint32_t* counter, const SrcCtx& ctx, int grid, cudaStream_t stream) {
+  switch (technique) {
+    case kScenStd:
+      return launch_scen_t<SMP, kScenStd>(family, d_req, n_tiles, counter, ctx, grid, stream);
+    case kScenAnti:
+      return launch_scen_t<SMP, kScenAnti>(family, d_req, n_tiles, counter, ctx, grid, stream);
+    case kScenCv:
+      return launch_scen_t<SMP, kScenCv>(family, d_req, n_tiles, counter, ctx, grid, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <int SMP, int TECH>
+static int scen_occ_t(int family) {
   int n = 0;
   const size_t smem = fused_dynamic_smem<SMP>();
-  if (family == FAM_GBM_STEP)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scenario_kernel<FAM_GBM_STEP, SMP>, kFusedBlock, smem);
-  else if (family == FAM_GBM_TERMINAL)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scenario_kernel<FAM_GBM_TERMINAL, SMP>, kFusedBlock, smem);
-  else if (family == FAM_HESTON)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, scenario_kernel<FAM_HESTON, SMP>, kFusedBlock, smem);
+  const ScenarioKernel kernel = scenario_kernel_of<SMP, TECH>(family);
+  if (!kernel || allow_dynamic_smem((const void*)kernel, smem) != cudaSuccess) return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kFusedBlock, smem);
   return n;
 }
-int scenario_max_blocks_per_sm(int family, int sampler) {
-  if (sampler == SMP_XORSHIFT) return scen_occ_s<SMP_XORSHIFT>(family);
-  if (sampler == SMP_SOBOL) return scen_occ_s<SMP_SOBOL>(family);
-  if (sampler == SMP_COUNTER) return scen_occ_s<SMP_COUNTER>(family);
+
+template <int SMP>
+static int scen_occ_s(int family, int technique) {
+  if (technique == kScenAnti) return scen_occ_t<SMP, kScenAnti>(family);
+  if (technique == kScenCv) return scen_occ_t<SMP, kScenCv>(family);
+  return scen_occ_t<SMP, kScenStd>(family);
+}
+
+int scenario_max_blocks_per_sm(int family, int sampler, int technique) {
+  if (sampler == SMP_XORSHIFT) return scen_occ_s<SMP_XORSHIFT>(family, technique);
+  if (sampler == SMP_SOBOL) return scen_occ_s<SMP_SOBOL>(family, technique);
+  if (sampler == SMP_COUNTER) return scen_occ_s<SMP_COUNTER>(family, technique);
   return 0;
 }
 
 cudaError_t launch_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_counter, int family, int sampler,
-                             const DeviceTables& tabs, int grid, cudaStream_t stream) {
+                             int technique, const DeviceTables& tabs, int grid, cudaStream_t stream) {
   SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
   switch (sampler) {
     case SMP_XORSHIFT:
-      return launch_scen_s<SMP_XORSHIFT>(family, d_req, n_tiles, d_counter, ctx, grid, stream);
+      return launch_scen_s<SMP_XORSHIFT>(family, technique, d_req, n_tiles, d_counter, ctx, grid, stream);
     case SMP_SOBOL:
-      return launch_scen_s<SMP_SOBOL>(family, d_req, n_tiles, d_counter, ctx, grid, stream);
+      return launch_scen_s<SMP_SOBOL>(family, technique, d_req, n_tiles, d_counter, ctx, grid, stream);
     case SMP_COUNTER:
-      return launch_scen_s<SMP_COUNTER>(family, d_req, n_tiles, d_counter, ctx, grid, stream);
+      return launch_scen_s<SMP_COUNTER>(family, technique, d_req, n_tiles, d_counter, ctx, grid, stream);
     default:
       return cudaErrorInvalidValue;
   }
@@ -1673,26 +1783,10 @@ __global__ void __launch_bounds__(kFusedBlock, 2) basket_scenario_kernel(const D
   }
 }
 
-// The Sobol instance's window and inverse-normal table (46,592 bytes) plus
-// the static descriptor and 13-leg slots pass the 48 KB default, so the
-// dynamic size is raised once per device (the attribute is per device).
-template <int SMP>
-static cudaError_t basket_scen_attr() {
-  static std::atomic<bool> done[64];
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev >= 0 && dev < 64 && done[dev].load()) return cudaSuccess;
-  e = cudaFuncSetAttribute(basket_scenario_kernel<SMP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)fused_dynamic_smem<SMP>());
-  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev].store(true);
-  return e;
-}
-
 template <int SMP>
 static cudaError_t launch_basket_scen_s(const DevReq* d_req, uint32_t n_tiles, uint32_t* counter, const SrcCtx& ctx,
                                         const BasketScen& legs, int grid, cudaStream_t stream) {
-  const cudaError_t e = basket_scen_attr<SMP>();
+  const cudaError_t e = allow_dynamic_smem((const void*)basket_scenario_kernel<SMP>, fused_dynamic_smem<SMP>());
   if (e != cudaSuccess) return e;
   basket_scenario_kernel<SMP><<<grid, kFusedBlock, fused_dynamic_smem<SMP>(), stream>>>(d_req, n_tiles, counter, ctx,
                                                                                         legs);
@@ -1703,7 +1797,8 @@ static cudaError_t launch_basket_scen_s(const DevReq* d_req, uint32_t n_tiles, u
 template <int SMP>
 static int basket_scen_occ() {
   int n = 0;
-  if (basket_scen_attr<SMP>() != cudaSuccess) return 0;
+  if (allow_dynamic_smem((const void*)basket_scenario_kernel<SMP>, fused_dynamic_smem<SMP>()) != cudaSuccess)
+    return 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, basket_scenario_kernel<SMP>, kFusedBlock, fused_dynamic_smem<SMP>());
   return n;
 }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/montepath_cuda.h"
 #include "mpc_types.h"
 
 namespace mpc {
@@ -85,12 +86,15 @@ constexpr uint32_t kLsmThreads = 512;
 constexpr size_t kLsmCounterBytes = 64;
 
 // Bump-and-revalue legs sharing every normal: one request d_req (GBM step,
-// GBM terminal or Heston; xorshift, Sobol or counter-hash samples) whose
-// q.scen holds the legs' parameters; q.partials must hold
-// [n_tiles][kMaxScen][2] doubles and q.moments [kMaxScen][2].
+// GBM terminal or Heston; xorshift, Sobol or counter-hash samples; any
+// technique) whose q.scen holds the legs' parameters; with NM =
+// scenario_moments(technique), q.partials must hold [n_tiles][kMaxScen][NM]
+// doubles and q.moments [kMaxScen][NM]: sum p, sum p^2 (pair averages for
+// antithetic requests), then for control variates sum c, sum c^2, sum p c.
+constexpr int scenario_moments(int technique) { return technique == MPC_TECHNIQUE_CONTROL_VARIATE ? 5 : 2; }
 cudaError_t launch_scenarios(const DevReq* d_req, uint32_t n_tiles, uint32_t* d_counter, int family, int sampler,
-                             const DeviceTables& tabs, int grid, cudaStream_t stream);
-int scenario_max_blocks_per_sm(int family, int sampler);
+                             int technique, const DeviceTables& tabs, int grid, cudaStream_t stream);
+int scenario_max_blocks_per_sm(int family, int sampler, int technique);
 
 // Basket bump legs sharing every normal: one basket request d_req
 // (xorshift, Sobol or counter-hash samples); q.partials must hold

@@ -548,6 +548,48 @@ def test_scenario_bump_legs_equal_separate_pricing(backend, workload, kw):
     assert abs(delta.bumped_down_price - backend.price(down).price) <= 1e-7 * abs(delta.bumped_down_price)
 
 
+@pytest.mark.parametrize("workload,kw", [
+    ("european_call", {"technique": "antithetic"}),
+    ("european_call", {"technique": "control_variate", "sampling": "counter_hash"}),
+    ("european_call", {"method": "stepwise", "n_steps": 32, "sampling": "scrambled_sobol", "technique": "antithetic"}),
+    ("arithmetic_asian_call", {"n_steps": 24, "technique": "control_variate", "sampling": "scrambled_sobol"}),
+    ("up_and_out_call", {"n_steps": 24, "barrier": 130.0, "technique": "antithetic", "sampling": "counter_hash"}),
+    ("down_and_out_call", {"n_steps": 24, "barrier": 85.0, "technique": "control_variate"}),
+    ("lookback_call", {"n_steps": 16, "technique": "antithetic"}),
+    ("european_call", {"model": "heston", "n_steps": 16, "technique": "antithetic", "sampling": "scrambled_sobol"}),
+    ("european_call", {"model": "heston", "n_steps": 16, "technique": "control_variate", "sampling": "counter_hash"}),
+])
+def test_scenario_technique_legs_equal_separate_pricing(backend, workload, kw):
+    """Antithetic and control-variate bump legs share each normal in one
+    scenario launch: each leg's antithetic pair average, or its payoff and
+    discounted terminal control, are the single-request unit's FP32
+    expressions, summarised by the request's own estimator.  Every leg (base,
+    up and down per Greek) prices within 1e-6 of the same leg priced alone
+    (FMA contraction and summation order), standard errors within 1e-5."""
+
+    r = req(workload, n_paths=20001, seed=37, **kw)
+    rep = backend.greeks(r, "bump_and_revalue")
+    base = backend.price(r)
+    assert abs(rep.base_price - base.price) <= 1e-6 * abs(base.price)
+    assert abs(rep.base_stderr - base.stderr) <= 1e-5 * base.stderr
+    est = _estimates(rep)
+    for greek, e in est.items():
+        for sign, want in ((1.0, e.bumped_up_price), (-1.0, e.bumped_down_price)):
+            leg = abi.Request.from_buffer_copy(r)
+            if greek == abi.GREEK_DELTA:
+                leg.s0 = r.s0 + sign * e.bump_size
+            elif greek == abi.GREEK_VEGA and kw.get("model") == "heston":
+                leg.v0 = (math.sqrt(r.v0) + sign * e.bump_size) ** 2
+            elif greek == abi.GREEK_VEGA:
+                leg.sigma = r.sigma + sign * e.bump_size
+            elif greek == abi.GREEK_RHO:
+                leg.r = r.r + sign * e.bump_size
+            else:
+                leg.t = r.t + sign * e.bump_size
+            got = backend.price(leg).price
+            assert abs(want - got) <= 1e-6 * abs(got) + 1e-12, (greek, sign, want, got)
+
+
 _BASKET5 = {"spots": [100.0, 95.0, 105.0, 90.0, 110.0], "sigmas": [0.2, 0.25, 0.3, 0.35, 0.4], "corr": 0.3}
 
 
