@@ -334,6 +334,18 @@ int mpc_estimate_bytes(const mpc_request_t* req, uint64_t* bytes);
 /* NvidiaCudaBackend::estimate_cost (cuda.rs:121-152) from the measured cost
  * model (host only).  sm_count 0 = 148. */
 int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out);
+/* The same estimate from rates measured on this context's device by
+ * mpc_calibrate_cost (confidence "calibrated"); before any calibration, the
+ * built-in rates scaled by the device's SM count. */
+int mpc_estimate_cost_ctx(mpc_context_t* ctx, const mpc_request_t* req, mpc_cost_t* out);
+/* Measures this device's rates for the cost model: one request of 1,048,576
+ * paths x 64 steps (1 step for terminal workloads) per model row, sampler
+ * column (pseudorandom, counter hash, scrambled Sobol, Halton) and
+ * precision, priced twice, the second call's device time kept.  Replaces the
+ * single-B200 table that cuda.rs:121-152's estimate would otherwise read;
+ * `seconds` (optional) receives the wall time it took (under a second on a
+ * B200). */
+int mpc_calibrate_cost(mpc_context_t* ctx, double* seconds);
 
 /* ----- context ---------------------------------------------------------- */
 int mpc_create(const mpc_options_t* options, mpc_context_t** out);

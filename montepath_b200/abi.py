@@ -355,6 +355,8 @@ FUNCTIONS = [
     ("mpc_supports", c_int, [POINTER(Request), POINTER(Support)]),
     ("mpc_estimate_bytes", c_int, [POINTER(Request), POINTER(c_uint64)]),
     ("mpc_estimate_cost", c_int, [POINTER(Request), c_int, POINTER(Cost)]),
+    ("mpc_estimate_cost_ctx", c_int, [c_void_p, POINTER(Request), POINTER(Cost)]),
+    ("mpc_calibrate_cost", c_int, [c_void_p, POINTER(c_double)]),
     ("mpc_create", c_int, [POINTER(Options), POINTER(c_void_p)]),
     ("mpc_destroy", c_int, [c_void_p]),
     ("mpc_last_error_message", c_char_p, [c_void_p]),

@@ -137,6 +137,18 @@ class CudaBackend:
         self._check(self.lib.mpc_measure_peaks(self.handle, byref(fp32), byref(sfu)))
         return fp32.value, sfu.value
 
+    def calibrate_cost(self) -> float:
+        """Measures this device's cost-model rates (mpc_calibrate_cost); returns the seconds it took."""
+        seconds = c_double()
+        self._check(self.lib.mpc_calibrate_cost(self.handle, byref(seconds)))
+        return seconds.value
+
+    def estimate_cost(self, req: abi.Request) -> abi.Cost:
+        """Cost estimate from this context's rates (mpc_estimate_cost_ctx)."""
+        cost = abi.Cost()
+        self._check(self.lib.mpc_estimate_cost_ctx(self.handle, byref(req), byref(cost)))
+        return cost
+
     def server(self, hbm_budget_bytes: int = 0, max_slots: int = 0, wave_tiles: int = 0, plain: bool = False) -> "Server":
         return Server(self, hbm_budget_bytes, max_slots, wave_tiles, plain)
 

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1548,18 +1549,36 @@ namespace {
 struct RateRow {
   double fp32[4], fp64[4];
 };
-const RateRow kRateGbmStep = {{2.24e11, 3.25e11, 3.85e11, 9.05e10}, {1.31e11, 1.35e11, 5.96e10, 5.38e10}};
-const RateRow kRateAsian = {{2.12e11, 2.93e11, 3.50e11, 8.84e10}, {1.12e11, 1.16e11, 5.59e10, 5.02e10}};
-const RateRow kRateGbmTerminal = {{6.68e9, 1.83e10, 1.53e10, 1.11e10}, {7.38e9, 2.45e10, 1.98e10, 1.12e10}};
-const RateRow kRateHeston = {{1.45e11, 1.93e11, 2.23e11, 5.37e10}, {7.09e10, 6.85e10, 3.02e10, 3.14e10}};
-const RateRow kRateMertonStep = {{1.05e11, 1.05e11, 1.97e11, 4.30e10}, {4.16e10, 4.16e10, 2.65e10, 2.63e10}};
-const RateRow kRateMertonTerminal = {{1.70e10, 1.70e10, 1.44e10, 7.09e9}, {1.83e10, 1.83e10, 1.30e10, 6.60e9}};
-const RateRow kRateBasket2 = {{5.46e9, 1.53e10, 1.28e10, 7.74e9}, {5.49e9, 1.58e10, 1.13e10, 6.77e9}};
-const double kRateBridge[2] = {1.41e11, 4.59e10};  // GBM stepwise through the bridge, fp32 / fp64
+// Rows of the rate table; the bridge row has one rate per precision (all
+// columns alike).
+enum CostRow : int {
+  ROW_GBM_STEP,
+  ROW_ASIAN,
+  ROW_GBM_TERMINAL,
+  ROW_HESTON,
+  ROW_MERTON_STEP,
+  ROW_MERTON_TERMINAL,
+  ROW_BASKET2,
+  ROW_BRIDGE,
+  ROW_COUNT
+};
+const RateRow kRates[ROW_COUNT] = {
+    {{2.24e11, 3.25e11, 3.85e11, 9.05e10}, {1.31e11, 1.35e11, 5.96e10, 5.38e10}},  // GBM stepwise
+    {{2.12e11, 2.93e11, 3.50e11, 8.84e10}, {1.12e11, 1.16e11, 5.59e10, 5.02e10}},  // arithmetic Asian
+    {{6.68e9, 1.83e10, 1.53e10, 1.11e10}, {7.38e9, 2.45e10, 1.98e10, 1.12e10}},    // GBM terminal
+    {{1.45e11, 1.93e11, 2.23e11, 5.37e10}, {7.09e10, 6.85e10, 3.02e10, 3.14e10}},  // Heston
+    {{1.05e11, 1.05e11, 1.97e11, 4.30e10}, {4.16e10, 4.16e10, 2.65e10, 2.63e10}},  // Merton stepwise
+    {{1.70e10, 1.70e10, 1.44e10, 7.09e9}, {1.83e10, 1.83e10, 1.30e10, 6.60e9}},    // Merton terminal
+    {{5.46e9, 1.53e10, 1.28e10, 7.74e9}, {5.49e9, 1.58e10, 1.13e10, 6.77e9}},      // 2-asset basket
+    {{1.41e11, 1.41e11, 1.41e11, 1.41e11}, {4.59e10, 4.59e10, 4.59e10, 4.59e10}},  // GBM stepwise, bridge
+};
 const double kLsmFixedMs = 0.24, kLsmRate = 6.4e10; // 49 cross-block date rounds, then path-steps
                                                       // (fit to 524,288 paths x 50 dates)
 const double kCallOverheadMs = 0.035;               // events, copies, one launch
 const double kFirstCallMs = 2.0;                    // tables and buffers of a new shape
+const int kCostColumns = 4;
+const int kCalibrationSampling[kCostColumns] = {MPC_SAMPLING_PSEUDORANDOM, MPC_SAMPLING_COUNTER_HASH,
+                                                MPC_SAMPLING_SCRAMBLED_SOBOL, MPC_SAMPLING_RANDOMIZED_HALTON};
 
 int rate_column(int sampling) {
   switch (sampling) {
@@ -1574,9 +1593,23 @@ int rate_column(int sampling) {
       return 3;
   }
 }
-}  // namespace
 
-int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out) {
+// Units per second of (row, precision, column): the context's calibrated
+// rate when it has one, else the built-in B200 rate scaled by SM count.
+struct RateSource {
+  const std::vector<double>* calibrated;  // [row][2][kCostColumns] or null
+  double scale;
+  double at(int row, bool fp64, int col) const {
+    if (calibrated && !calibrated->empty()) {
+      const double v = (*calibrated)[(size_t(row) * 2 + (fp64 ? 1 : 0)) * kCostColumns + col];
+      if (v > 0.0) return v;
+    }
+    return (fp64 ? kRates[row].fp64[col] : kRates[row].fp32[col]) * scale;
+  }
+  bool measured_here() const { return calibrated && !calibrated->empty(); }
+};
+
+int estimate_cost_with(const mpc_request_t* req, const RateSource& rates, mpc_cost_t* out) {
   if (!req || !out) return MPC_E_INVALID_CONFIG;
   std::memset(out, 0, sizeof(*out));
   std::string msg;
@@ -1585,12 +1618,11 @@ int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out) {
   const mpc_request_t& r = *req;
   const bool fp64 = r.precision == MPC_PRECISION_FP64_PLAIN;
   const int col = rate_column(r.sampling);
-  const double scale = double(sm_count > 0 ? sm_count : 148) / 148.0;
-  auto pick = [&](const RateRow& row) { return (fp64 ? row.fp64[col] : row.fp32[col]) * scale; };
+  auto pick = [&](int row) { return rates.at(row, fp64, col); };
   double units = double(r.n_paths) * double(r.n_steps), rate = 0.0, fixed_ms = 0.0;
-  const char* confidence = "measured";
+  const char* confidence = rates.measured_here() ? "calibrated" : "measured";
   if (is_lsm(r.workload)) {
-    rate = kLsmRate * scale;
+    rate = kLsmRate * rates.scale;
     fixed_ms = kLsmFixedMs * double(std::max<uint32_t>(r.n_steps, 2) - 1) / 49.0;
     if (r.workload == MPC_WORKLOAD_BERMUDAN_PUT) fixed_ms *= double(std::max<uint32_t>(r.n_exercise, 1)) / 49.0;
     confidence = "derived";
@@ -1602,29 +1634,29 @@ int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out) {
       updates += double(r.paths_per_level[l]) * double(fine) * (l ? 1.5 : 1.0);
     if (r.target_stderr > 0.0) updates = double(r.max_step_updates);
     units = updates;
-    rate = pick(kRateAsian);
+    rate = pick(ROW_ASIAN);
     fixed_ms = 2.0 * kCallOverheadMs * double(std::max<uint32_t>(r.levels, 1));
     confidence = "derived";
   } else if (r.workload == MPC_WORKLOAD_BASKET_CALL) {
     units = double(r.n_paths) * double(std::max<uint32_t>(r.n_steps, 1)) * double(std::max<uint32_t>(r.n_assets, 2)) / 2.0;
-    rate = pick(kRateBasket2);
+    rate = pick(ROW_BASKET2);
     if (r.n_assets > 2 || r.n_steps > 1) confidence = "derived";
   } else if (r.model == MPC_MODEL_HESTON) {
-    rate = pick(kRateHeston);
+    rate = pick(ROW_HESTON);
   } else if (r.model == MPC_MODEL_MERTON) {
     if (r.method == MPC_METHOD_STEPWISE) {
-      rate = pick(kRateMertonStep);
+      rate = pick(ROW_MERTON_STEP);
     } else {
       units = double(r.n_paths);
-      rate = pick(kRateMertonTerminal);
+      rate = pick(ROW_MERTON_TERMINAL);
     }
   } else if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.method != MPC_METHOD_STEPWISE) {
     units = double(r.n_paths);
-    rate = pick(kRateGbmTerminal);
+    rate = pick(ROW_GBM_TERMINAL);
   } else if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE) {
-    rate = kRateBridge[fp64 ? 1 : 0] * scale;
+    rate = pick(ROW_BRIDGE);
   } else {
-    rate = pick(r.workload == MPC_WORKLOAD_ARITHMETIC_ASIAN_CALL ? kRateAsian : kRateGbmStep);
+    rate = pick(r.workload == MPC_WORKLOAD_ARITHMETIC_ASIAN_CALL ? ROW_ASIAN : ROW_GBM_STEP);
   }
   if (r.technique == MPC_TECHNIQUE_ANTITHETIC) rate *= 1.6;  // one draw drives two paths
   uint64_t bytes = 0;
@@ -1636,6 +1668,92 @@ int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out) {
   out->path_steps_per_sec = rate;
   out->path_steps = uint64_t(units);
   std::snprintf(out->confidence, sizeof(out->confidence), "%s", confidence);
+  return MPC_OK;
+}
+
+// The request a calibration cell times: 1,048,576 paths x 64 steps (one
+// step for the terminal rows), the standard technique.
+mpc_request_t calibration_request(int row, bool fp64, int col) {
+  mpc_request_t r;
+  int workload = MPC_WORKLOAD_EUROPEAN_CALL;
+  if (row == ROW_ASIAN) workload = MPC_WORKLOAD_ARITHMETIC_ASIAN_CALL;
+  if (row == ROW_BASKET2) workload = MPC_WORKLOAD_BASKET_CALL;
+  mpc_request_defaults(&r, workload);
+  r.n_paths = 1u << 20;
+  r.n_steps = 64;
+  r.seed = 1;
+  r.technique = MPC_TECHNIQUE_STANDARD;
+  r.precision = fp64 ? MPC_PRECISION_FP64_PLAIN : MPC_PRECISION_FP32_PATH;
+  r.sampling = row == ROW_BRIDGE ? MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE : kCalibrationSampling[col];
+  switch (row) {
+    case ROW_GBM_STEP:
+    case ROW_BRIDGE:
+      r.method = MPC_METHOD_STEPWISE;
+      break;
+    case ROW_GBM_TERMINAL:
+      r.method = MPC_METHOD_TERMINAL;
+      break;
+    case ROW_HESTON:
+      r.model = MPC_MODEL_HESTON;
+      r.method = MPC_METHOD_STEPWISE;
+      break;
+    case ROW_MERTON_STEP:
+      r.model = MPC_MODEL_MERTON;
+      r.method = MPC_METHOD_STEPWISE;
+      break;
+    case ROW_MERTON_TERMINAL:
+      r.model = MPC_MODEL_MERTON;
+      r.method = MPC_METHOD_TERMINAL;
+      break;
+    case ROW_BASKET2:
+      r.method = MPC_METHOD_TERMINAL;
+      break;
+    default:
+      break;
+  }
+  return r;
+}
+}  // namespace
+
+int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out) {
+  const RateSource rates{nullptr, double(sm_count > 0 ? sm_count : 148) / 148.0};
+  return estimate_cost_with(req, rates, out);
+}
+
+int mpc_estimate_cost_ctx(mpc_context_t* ctx, const mpc_request_t* req, mpc_cost_t* out) {
+  if (!ctx) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  const RateSource rates{&ctx->cost_rates, double(ctx->sm_count) / 148.0};
+  return estimate_cost_with(req, rates, out);
+}
+
+int mpc_calibrate_cost(mpc_context_t* ctx, double* seconds) {
+  if (!ctx) return MPC_E_INVALID_CONFIG;
+  std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<double> rates(size_t(ROW_COUNT) * 2 * kCostColumns, 0.0);
+  const RateSource builtin{nullptr, double(ctx->sm_count) / 148.0};
+  for (int row = 0; row < ROW_COUNT; ++row) {
+    for (int p = 0; p < 2; ++p) {
+      for (int col = 0; col < kCostColumns; ++col) {
+        double* cell = &rates[(size_t(row) * 2 + p) * kCostColumns + col];
+        if (row == ROW_BRIDGE && col > 0) {  // one bridge rate per precision
+          *cell = rates[(size_t(row) * 2 + p) * kCostColumns];
+          continue;
+        }
+        const mpc_request_t r = calibration_request(row, p == 1, col);
+        mpc_cost_t units;
+        if (estimate_cost_with(&r, builtin, &units) != MPC_OK) continue;
+        mpc_result_t res;
+        // first call: tables and buffers of the shape; second: steady state
+        if (mpc_price(ctx, &r, &res) != MPC_OK || mpc_price(ctx, &r, &res) != MPC_OK) continue;
+        if (ctx->last_ms > 0.0) *cell = double(units.path_steps) / (ctx->last_ms * 1e-3);
+      }
+    }
+  }
+  ctx->cost_rates = rates;
+  ctx->last_error.clear();
+  if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return MPC_OK;
 }
 

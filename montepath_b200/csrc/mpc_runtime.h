@@ -90,6 +90,9 @@ struct mpc_context {
   std::vector<uint64_t> last_batch_key;  // key of the previous fused batch
   uint64_t graph_kernels = 0;           // kernels in graph_exec
   uint64_t graph_replays = 0;
+  // Cost-model rates measured on this device by mpc_calibrate_cost, units
+  // per second as [row][fp32, fp64][sampler column]; empty until then.
+  std::vector<double> cost_rates;
 };
 
 namespace mpc {

@@ -267,6 +267,16 @@ def test_mc_bench_rows_have_the_harness_shape(monkeypatch):
         assert row["throughput_per_sec"] > 0 and row["metric_value"] > 0
 
 
+def test_calibrated_cost_entry_points_reject_null_context():
+    import ctypes
+
+    lib = abi.load_library()
+    r = make_request("european_call", {"n_paths": 1000})
+    cost = abi.Cost()
+    assert lib.mpc_estimate_cost_ctx(None, ctypes.byref(r), ctypes.byref(cost)) == abi.E_INVALID_CONFIG
+    assert lib.mpc_calibrate_cost(None, None) == abi.E_INVALID_CONFIG
+
+
 def test_cost_model_and_planner_priority():
     """mpc_estimate_cost (host only) and the planner order it feeds."""
 

@@ -787,6 +787,34 @@ def test_cost_model_predicts_device_time(backend, workload, kw):
     assert 0.5 < cost.estimated_runtime_ms / measured < 2.0, (cost.estimated_runtime_ms, measured)
 
 
+def test_cost_model_calibrated_on_this_device(backend):
+    """mpc_calibrate_cost measures the rate table on the device in use; the
+    calibrated estimates then predict the device time of requests of other
+    sizes and shapes within 1.6x (the built-in table: 2x)."""
+
+    seconds = backend.calibrate_cost()
+    assert 0.0 < seconds < 60.0
+    cases = [
+        ("european_call", dict(model="heston", method="stepwise", n_steps=128, sampling="scrambled_sobol")),
+        ("european_call", dict(model="merton", method="stepwise", n_steps=96, sampling="scrambled_sobol")),
+        ("arithmetic_asian_call", dict(n_steps=96, sampling="counter_hash")),
+        ("european_call", dict(method="stepwise", n_steps=64, precision="fp64_plain", sampling="scrambled_sobol")),
+        ("down_and_out_call", dict(n_steps=80, barrier=80.0, sampling="pseudorandom")),
+        ("european_call", dict(n_paths=1 << 21)),
+    ]
+    for workload, kw in cases:
+        kw = dict(kw)
+        r = req(workload, n_paths=kw.pop("n_paths", 1 << 19), seed=3, **kw)
+        cost = backend.estimate_cost(r)
+        assert cost.confidence.decode() == "calibrated"
+        times = []
+        for _ in range(3):
+            backend.price(r)
+            times.append(backend.last_timing()[0])
+        measured = min(times)
+        assert 1 / 1.6 < cost.estimated_runtime_ms / measured < 1.6, (workload, kw, cost.estimated_runtime_ms, measured)
+
+
 # ---------------------------------------------------------- harness rows --
 def test_mc_bench_compact_rows(backend):
     """mc_cuda_* rows (BenchmarkResult shape) from the real device, compact suite."""
