@@ -343,8 +343,9 @@ int mpc_estimate_cost_ctx(mpc_context_t* ctx, const mpc_request_t* req, mpc_cost
  * column (pseudorandom, counter hash, scrambled Sobol, Halton) and
  * precision, priced twice, the second call's device time kept.  Replaces the
  * single-B200 table that cuda.rs:121-152's estimate would otherwise read;
- * `seconds` (optional) receives the wall time it took (under a second on a
- * B200). */
+ * combinations the backend does not run, or past the context's byte budget,
+ * keep the built-in rate.  `seconds` (optional) receives the wall time it
+ * took.  Returns MPC_E_CUDA if a pricing call fails on the device. */
 int mpc_calibrate_cost(mpc_context_t* ctx, double* seconds);
 
 /* ----- context ---------------------------------------------------------- */

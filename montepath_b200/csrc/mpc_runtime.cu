@@ -1745,14 +1745,20 @@ int mpc_calibrate_cost(mpc_context_t* ctx, double* seconds) {
         mpc_cost_t units;
         if (estimate_cost_with(&r, builtin, &units) != MPC_OK) continue;
         mpc_result_t res;
-        // first call: tables and buffers of the shape; second: steady state
-        if (mpc_price(ctx, &r, &res) != MPC_OK || mpc_price(ctx, &r, &res) != MPC_OK) continue;
+        // first call: tables and buffers of the shape; second: steady state.
+        // A combination the backend does not run, or one past the context's
+        // byte budget, keeps the built-in rate; a CUDA failure ends the
+        // calibration with its status.
+        int st = mpc_price(ctx, &r, &res);
+        if (st == MPC_OK) st = mpc_price(ctx, &r, &res);
+        if (st == MPC_E_CUDA || st == MPC_E_NO_DEVICE) return st;
+        if (st != MPC_OK) continue;
         if (ctx->last_ms > 0.0) *cell = double(units.path_steps) / (ctx->last_ms * 1e-3);
       }
     }
   }
   ctx->cost_rates = rates;
-  ctx->last_error.clear();
+  ctx->last_error.clear();  // messages of the skipped combinations
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return MPC_OK;
 }
