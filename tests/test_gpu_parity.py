@@ -332,6 +332,29 @@ def test_fused_heston_merton_sobol_small(backend):
         assert abs(a.price - b.price) < 0.1 * b.stderr, kw["model"]
 
 
+def test_headline_full_size_fp32_against_fp64_plain(backend):
+    """The headline pair at full size (1,048,576 paths x 256 steps, scrambled
+    Sobol, seeds 42 / 43): the fused FP32 path reads the same Sobol points as
+    the FP64 plain path, so its estimator sits within 0.05 standard errors of
+    the FP64 one, with the standard error within 0.5%; the Merton price also
+    lies within 3 standard errors of the series price (the stepwise scheme is
+    exact in distribution)."""
+
+    heston = dict(model="heston", kappa=2.0, theta=0.04, vol_of_vol=0.5, rho=-0.7, v0=0.04, seed=42)
+    merton = dict(model="merton", method="stepwise", jump_intensity=0.5, jump_mean=-0.1, jump_volatility=0.15,
+                  seed=43)
+    for kw in (heston, merton):
+        r32 = req("european_call", n_paths=1 << 20, n_steps=256, sampling="scrambled_sobol", **kw)
+        r64 = req("european_call", n_paths=1 << 20, n_steps=256, sampling="scrambled_sobol",
+                  precision="fp64_plain", **kw)
+        a, b = backend.price(r32), backend.price(r64)
+        assert a.path_steps == b.path_steps == (1 << 20) * 256
+        assert abs(a.price - b.price) < 0.05 * b.stderr, (kw["model"], a.price, b.price, b.stderr)
+        assert abs(a.stderr - b.stderr) < 5e-3 * b.stderr
+    series = O.merton_series(100.0, 100.0, 0.03, 0.2, 0.5, -0.1, 0.15, 1.0, exact=True)
+    assert abs(a.price - series) < 3 * a.stderr, (a.price, series, a.stderr)
+
+
 def test_fused_basket_five_assets(backend):
     r = req("basket_call", method="stepwise", n_steps=20, n_paths=8000, seed=4, sampling="counter_hash",
             spots=[100, 95, 105, 98, 102], sigmas=[0.2, 0.25, 0.3, 0.15, 0.22], weights=[0.2] * 5, corr=0.3, k=100)
@@ -686,6 +709,24 @@ def test_batch_equals_individual(backend):
     batch = backend.price_batch(reqs)
     for a, b in zip(alone, batch):
         assert a.price == b.price and a.stderr == b.stderr
+
+
+def test_full_book_batch_equals_individual(backend):
+    """The full 4,096-contract heterogeneous book (seed 42; European, Asian,
+    up-and-out and 5-asset basket; 1e3-1e6 paths, 16-365 steps) in one batch:
+    every result of 32 contracts spread over the book, 8 of each kind, equals
+    that contract priced alone bit for bit (tile partials are per request and
+    summed in tile order), and every price is finite with a positive count."""
+
+    from montepath_b200 import workloads
+
+    book = workloads.book(42)
+    batch = backend.price_batch(book)
+    assert len(batch) == 4096
+    assert all(math.isfinite(b.price) and b.price >= 0.0 and b.n_samples > 0 for b in batch)
+    for i in list(range(0, 4096, 128)):
+        alone = backend.price(book[i])
+        assert alone.price == batch[i].price and alone.stderr == batch[i].stderr, i
 
 
 def test_repeated_batches_replay_a_graph(backend):
