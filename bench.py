@@ -224,12 +224,12 @@ def cpu_leg(line: dict) -> None:
     series = O.merton_series(100, 100, 0.03, 0.2, 0.5, -0.1, 0.15, 1.0, exact=True)
     h, m = line["prices"]["heston"], line["prices"]["merton"]
     # the closed forms are continuous-time; the gap to them includes the
-    # 256-step scheme's discretisation bias (see config2)
+    # 256-step scheme's discretisation bias (see the Heston/Merton leg)
     h["semi_analytic"], h["minus_semi_in_se"] = semi, (h["price"] - semi) / h["stderr"]
     m["series"], m["minus_series_in_se"] = series, (m["price"] - series) / m["stderr"]
-    configs = line.get("configs", {})
-    if "config1" in configs and "config1" in _CPU_LEG_INPUTS:
-        c1, r64 = configs["config1"], _CPU_LEG_INPUTS["config1"]
+    leg_out = line.get("legs", {})
+    if "gbm_european_20000x64" in leg_out and "gbm_european_20000x64" in _CPU_LEG_INPUTS:
+        c1, r64 = leg_out["gbm_european_20000x64"], _CPU_LEG_INPUTS["gbm_european_20000x64"]
         t0 = time.perf_counter()
         ref = O.price(r64)
         t_cpu = time.perf_counter() - t0
@@ -237,26 +237,26 @@ def cpu_leg(line: dict) -> None:
         c1["fp64_plain"]["err_vs_black_scholes_se"] = (c1["fp64_plain"]["price"] - bs) / c1["fp64_plain"]["stderr"]
         c1["fp64_plain"]["abs_diff_vs_oracle"] = abs(c1["fp64_plain"]["price"] - ref.price)
         c1["cpu_oracle_1_thread"] = {"price": ref.price, "seconds": t_cpu, "path_steps_per_sec": 20000 * 64 / t_cpu}
-    if "config2" in configs:
-        c2 = configs["config2"]
+    if "heston_merton_1048576x256" in leg_out:
+        c2 = leg_out["heston_merton_1048576x256"]
         c2["semi_analytic"] = semi
         for row in c2["steps"].values():
             row["minus_semi_in_se"] = (row["price"] - semi) / row["stderr"]
         rich = c2["richardson_1024_2048"]
         rich["minus_semi_in_se"] = (rich["price"] - semi) / rich["stderr_bound"]
-    if "config3" in configs:
-        for key, row in configs["config3"].items():
+    if "american_put_lsm_524288x50" in leg_out:
+        for key, row in leg_out["american_put_lsm_524288x50"].items():
             row["crr_2048"] = O.crr_put(float(key.split("_")[1]), 100.0, 0.06, 0.2, 1.0, 2048)
-    if "config4" in configs and "config4" in _CPU_LEG_INPUTS:
+    if "book_4096" in leg_out and "book_4096" in _CPU_LEG_INPUTS:
         diffs_se, worst_abs = [], 0.0
-        for req, gpu_price in _CPU_LEG_INPUTS["config4"]:
+        for req, gpu_price in _CPU_LEG_INPUTS["book_4096"]:
             ref = O.price(req)
             d = abs(gpu_price - ref.price)
             worst_abs = max(worst_abs, d)
             if ref.stderr > 0:
                 diffs_se.append(d / ref.stderr)
-        configs["config4"]["vs_fp64_oracle"] = {
-            "contracts": len(_CPU_LEG_INPUTS["config4"]), "max_abs_diff": worst_abs,
+        leg_out["book_4096"]["vs_fp64_oracle"] = {
+            "contracts": len(_CPU_LEG_INPUTS["book_4096"]), "max_abs_diff": worst_abs,
             "max_diff_in_se": max(diffs_se) if diffs_se else None,
             "within_3se": sum(1 for x in diffs_se if x <= 3.0), "with_nonzero_stderr": len(diffs_se)}
 
@@ -422,14 +422,14 @@ def run_ours(args) -> None:
         # measurements: taken at N = 1 only
         legs = [x for x in args.legs.split(",") if x and x != "none"] if world == 1 else []
         if "all" in legs:
-            legs = ["config1", "config2", "config3", "config4", "config5"]
+            legs = list(LEGS)
         if legs:
-            line["configs"] = {}
+            line["legs"] = {}
             for leg in legs:
-                if leg == "config4":
-                    line["configs"][leg] = leg_config4(backend, args.book_contracts)
+                if leg == "book_4096":
+                    line["legs"][leg] = leg_book(backend, args.book_contracts)
                 else:
-                    line["configs"][leg] = LEGS[leg](backend)
+                    line["legs"][leg] = LEGS[leg](backend)
         if not args.no_cpu and world == 1:
             cpu_leg(line)
         print(json.dumps(line), flush=True)
@@ -443,7 +443,7 @@ def _timed(backend, fn):
     return res, backend.last_timing()[0]
 
 
-def leg_config1(backend) -> dict:
+def leg_gbm_european_small(backend) -> dict:
     """Plain method, small: GBM European 20,000 x 64, seed 42, pseudorandom (the
     reference's MonteCarloRng stream replayed), FP64 one request per launch."""
 
@@ -458,14 +458,14 @@ def leg_config1(backend) -> dict:
     a, t64 = _timed(backend, lambda: backend.price(r64))
     b, t32 = _timed(backend, lambda: backend.price(r32))
     ps = 20000 * 64
-    _CPU_LEG_INPUTS["config1"] = r64
+    _CPU_LEG_INPUTS["gbm_european_20000x64"] = r64
     return {
         "fp64_plain": {"price": a.price, "stderr": a.stderr, "ms": t64, "path_steps_per_sec": ps / (t64 * 1e-3)},
         "fp32_path": {"price": b.price, "stderr": b.stderr, "ms": t32, "path_steps_per_sec": ps / (t32 * 1e-3)},
     }
 
 
-def leg_config2(backend) -> dict:
+def leg_heston_merton(backend) -> dict:
     """Accuracy of the headline Heston request against the semi-analytic
     price as the step count grows (1,048,576 paths, scrambled Sobol, FP32
     path): the full-truncation Euler scheme is biased by its time step (the
@@ -487,7 +487,7 @@ def leg_config2(backend) -> dict:
     return out
 
 
-def leg_config3(backend) -> dict:
+def leg_american_put_lsm(backend) -> dict:
     """American put by Longstaff-Schwartz, 524,288 paths x 50 dates, S0 in {90, 100, 110}."""
 
     from montepath_b200.requests import make_request
@@ -507,7 +507,7 @@ def leg_config3(backend) -> dict:
     return out
 
 
-def leg_config4(backend, contracts: int = 4096) -> dict:
+def leg_book(backend, contracts: int = 4096) -> dict:
     """4,096-contract heterogeneous book in one batched launch vs plain FP64
     per-request launches (timed on every 63rd contract, which cycles through
     the four contract kinds, and extrapolated by path-steps).  `contracts`
@@ -524,7 +524,7 @@ def leg_config4(backend, contracts: int = 4096) -> dict:
     # the contracts small enough (<= 2e6 path-steps) for the CPU leg to price
     # with the oracle on the same samples
     small = [i for i, r in enumerate(book) if r.n_paths * r.n_steps <= 2_000_000][:64]
-    _CPU_LEG_INPUTS["config4"] = [(book[i], res[i].price) for i in small]
+    _CPU_LEG_INPUTS["book_4096"] = [(book[i], res[i].price) for i in small]
     sample = book[::63]
     plain_ms = 0.0
     for r in sample:
@@ -545,7 +545,7 @@ def leg_config4(backend, contracts: int = 4096) -> dict:
     }
 
 
-def leg_config5(backend) -> dict:
+def leg_serving(backend) -> dict:
     """Poisson serving stream at 2,000 requests/s: continuous batching on a
     2 s slice of arrivals, plain FIFO FP64 on a 0.25 s slice."""
 
@@ -556,8 +556,8 @@ def leg_config5(backend) -> dict:
     return {"continuous_batching": fused, "plain_fifo": plain}
 
 
-LEGS = {"config1": leg_config1, "config2": leg_config2, "config3": leg_config3, "config4": leg_config4,
-        "config5": leg_config5}
+LEGS = {"gbm_european_20000x64": leg_gbm_european_small, "heston_merton_1048576x256": leg_heston_merton, "american_put_lsm_524288x50": leg_american_put_lsm, "book_4096": leg_book,
+        "serving_2000rps": leg_serving}
 
 
 def main() -> None:
@@ -569,9 +569,9 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain comparison of the headline")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling cases)")
-    ap.add_argument("--legs", default="all", help="comma list of config1,config2,config3,config4,config5, all or none")
+    ap.add_argument("--legs", default="all", help="comma list of gbm_european_20000x64, heston_merton_1048576x256, american_put_lsm_524288x50, book_4096, serving_2000rps; all or none")
     ap.add_argument("--book-contracts", type=int, default=4096,
-                    help="first contracts of the book in the config4 leg (profiling cases)")
+                    help="first contracts of the book in the book_4096 leg (profiling cases)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -73,7 +73,7 @@ def test_sobol_fp32_normals_same_uniforms(backend):
 
 
 # -------------------------------------------------------------- plain FP64 --
-def test_config1_plain_fp64_replays_reference_stream(backend):
+def test_gbm_european_small_plain_fp64_replays_reference_stream(backend):
     r = req("european_call", method="stepwise", n_paths=20000, n_steps=64, seed=42, n_threads=1,
             precision="fp64_plain")
     got = backend.price(r)

@@ -177,7 +177,7 @@ def test_european_stepwise_close_to_black_scholes():
     assert abs(res.price - O.bs_call(100, 100, 0.03, 0.2, 1.0)) < 5 * res.stderr
 
 
-def test_config1_statistically_matches_reference_python_pricer():
+def test_gbm_european_small_statistically_matches_reference_python_pricer():
     with open(os.path.join(GOLDEN, "python_reference_runs.json")) as f:
         runs = {r["workload"]: r for r in json.load(f)}
     ref = runs["european_call"]
