@@ -297,3 +297,13 @@ def test_cost_model_and_planner_priority():
                                        cuda_available=True)[0] == "nvidia_cuda"
     assert production.planner_priority("european_call", {"n_paths": 100}, cuda_available=True)[0] == "cpu_native"
     assert production.planner_priority("european_call", {"n_paths": 10**6}, cuda_available=False)[0] == "cpu_native"
+
+
+def test_serving_command_line_help():
+    """``python -m montepath_b200.serving`` parses its options without a GPU."""
+
+    from montepath_b200 import serving
+
+    with pytest.raises(SystemExit) as done:
+        serving.main(["--help"])
+    assert done.value.code == 0
