@@ -211,11 +211,12 @@ def test_mapping_abi_response_shape(monkeypatch):
 
 def test_reference_pricing_surface_accepts_module(monkeypatch):
     """montepath's own price_* helpers (python/montepath/pricing.py:711-780)
-    drive this module when the reference package is importable here."""
+    drive this module when a reference checkout is named by MONTEPATH_REFERENCE."""
 
-    ref_python = "/root/reference/python"
-    if not os.path.isdir(ref_python):
-        pytest.skip("reference package not present")
+    root = os.environ.get("MONTEPATH_REFERENCE", "")
+    ref_python = os.path.join(root, "python")
+    if not root or not os.path.isdir(ref_python):
+        pytest.skip("MONTEPATH_REFERENCE does not name a montepath checkout")
     import sys
 
     monkeypatch.syspath_prepend(ref_python)
