@@ -432,6 +432,11 @@ int mpc_measure_peaks(mpc_context_t* ctx, double* fp32_tflops, double* sfu_tops)
  *    antithetic pairs) per request; larger requests return MPC_E_OOM_BUDGET.
  *  - Samplers: pseudorandom, counter_hash, scrambled_sobol; path-payoff
  *    workloads only (not LSM, MLMC or FP64-plain requests: MPC_E_UNSUPPORTED).
+ *  - A paths_per_thread hint is honoured when it is a power of two up to 16
+ *    whose tiles (256 * hint paths) number at most 4,096; any other hint
+ *    returns MPC_E_UNSUPPORTED.  Without a hint the tile is the smallest
+ *    power-of-two multiple of 256 paths that fits 4,096 tiles.
+ *  - Serves device ordinals 0-63.
  *  - The first call on a device resolves the arrays' device addresses and
  *    uploads the lookup tables (set-up); make that first call before any
  *    stream capture.

@@ -55,8 +55,11 @@ struct DeviceState {
   int sm_count = 0;
 };
 
+// One slot per device ordinal in storage that never moves: a call in flight on
+// one device keeps a valid DeviceState* while another device is set up.
+constexpr int kNoAllocMaxDevices = 64;
 std::mutex g_mu;
-std::vector<DeviceState> g_devices;
+DeviceState g_devices[kNoAllocMaxDevices];
 
 void write_message(char* out, size_t len, const std::string& msg) {
   if (out && len) std::snprintf(out, len, "%s", msg.c_str());
@@ -65,8 +68,12 @@ void write_message(char* out, size_t len, const std::string& msg) {
 // Once per device, with that device current: resolves the device addresses
 // of the static arrays and uploads the lookup tables.
 int setup_device(int device, DeviceState** out, std::string* msg) {
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    *msg = "device ordinal " + std::to_string(device) + " is beyond the " + std::to_string(kNoAllocMaxDevices) +
+           " devices the no-allocation entry point serves";
+    return MPC_E_NO_DEVICE;
+  }
   std::lock_guard<std::mutex> lock(g_mu);
-  if (int(g_devices.size()) <= device) g_devices.resize(device + 1);
   DeviceState& st = g_devices[device];
   if (!st.ready) {
     void* scratch = nullptr;
@@ -136,9 +143,22 @@ extern "C" int mpc_price_fused_noalloc(const mpc_request_t* req, mpc_result_t* o
   DeviceState* ds = nullptr;
   if ((st = setup_device(device, &ds, &msg)) != MPC_OK) return reject(st, msg);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // tiles of 256 * ppt units, ppt the smallest power of two that fits the work list
+  // Tiles of 256 * ppt units: the request's paths_per_thread hint when it is a
+  // power of two whose work list fits the scratch, else (no hint) the smallest
+  // power of two that fits.
   uint32_t ppt = 1;
-  while ((p.q.n_units + 256ull * ppt - 1) / (256ull * ppt) > kNoAllocMaxTiles) ppt *= 2;
+  if (req->paths_per_thread != 0) {
+    ppt = req->paths_per_thread;
+    const bool pow2 = (ppt & (ppt - 1)) == 0;
+    if (!pow2 || ppt > kNoAllocMaxPpt ||
+        (p.q.n_units + 256ull * ppt - 1) / (256ull * ppt) > kNoAllocMaxTiles)
+      return reject(MPC_E_UNSUPPORTED, "paths_per_thread hint " + std::to_string(ppt) +
+                                           " is not a power of two up to " + std::to_string(kNoAllocMaxPpt) +
+                                           " whose tiles of 256 * hint paths fit the " +
+                                           std::to_string(kNoAllocMaxTiles) + "-tile scratch");
+  } else {
+    while ((p.q.n_units + 256ull * ppt - 1) / (256ull * ppt) > kNoAllocMaxTiles) ppt *= 2;
+  }
   mpc::DevReq q = p.q;
   q.tile_units = 256 * ppt;
   q.n_tiles = uint32_t((q.n_units + q.tile_units - 1) / q.tile_units);
