@@ -174,24 +174,30 @@ def load_traffic() -> dict:
     return {}
 
 
+def _cpu_pair(paths: int, threads: int) -> float:
+    """Prices the Heston and Merton requests at `paths` paths with the oracle on
+    `threads` host threads; returns the wall seconds."""
+
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    for cfg in (HESTON, MERTON):
+        O.price_threaded(O.make_request("european_call", dict(cfg, n_paths=paths, precision="fp64_plain")), threads)
+    return time.perf_counter() - t0
+
+
 def cpu_baseline(seconds_target: float = 12.0) -> dict:
     """The oracle (FP64 C++ restatement of the reference CPU path) on a
     bounded sample of the same workload, all host threads."""
 
-    from montepath_b200.requests import make_request
     from oracle import oracle as O
 
     O.lib()  # compile/load the oracle before timing
     threads = os.cpu_count() or 1
     paths = 2048
     while True:
-        total_steps = 0
-        t0 = time.perf_counter()
-        for cfg in (HESTON, MERTON):
-            req = make_request("european_call", dict(cfg, n_paths=paths, precision="fp64_plain"))
-            O.price_threaded(req, threads)
-            total_steps += paths * N_STEPS
-        dt = time.perf_counter() - t0
+        dt = _cpu_pair(paths, threads)
+        total_steps = 2 * paths * N_STEPS
         if dt * threads >= seconds_target or paths >= N_PATHS:
             break
         paths = min(N_PATHS, int(paths * max(2.0, seconds_target / max(dt * threads, 1e-3))))
@@ -262,19 +268,28 @@ def cpu_leg(line: dict) -> None:
 
 
 def run_reference(args) -> None:
+    """The reference arm: the reference's CPU path for this workload -- its C++
+    restatement (the oracle; the Rust crate does not build here) -- pricing
+    the full Heston + Merton pair, 1,048,576 paths x 256 steps each, in FP64 on
+    all host threads (the reference's chunk-per-thread scheme).  Warm-up steps
+    price 16,384-path samples; every timed step is the full workload.  Loads
+    nothing from the CUDA library."""
+
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle import oracle as O
+
+    O.lib()
+    threads = os.cpu_count() or 1
+    paths = args.paths or N_PATHS
     for _ in range(args.warmup):
-        cpu_baseline(seconds_target=2.0)
-    vals = []
-    t0 = time.perf_counter()
-    last = None
+        _cpu_pair(min(16_384, paths), threads)
+    wall = 0.0
     for _ in range(args.steps):
-        last = cpu_baseline(seconds_target=8.0)
-        vals.append(last["value"])
-    wall = time.perf_counter() - t0
-    value = sum(vals) / len(vals)
+        wall += _cpu_pair(paths, threads)
+    path_steps = 2 * paths * N_STEPS
+    value = path_steps * args.steps / wall
     line = {
         "impl": "reference",
         "metric": "path-steps/s",
@@ -289,9 +304,12 @@ def run_reference(args) -> None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded scrambled Sobol samples)",
-        "config": {"workload": WORKLOAD, "paths": N_PATHS, "steps_per_path": N_STEPS, "requests": 2,
-                   "note": "CPU restatement of the reference path on a bounded sample of the workload"},
-        "cpu_baseline": dict(last, value=value),
+        "config": {"workload": WORKLOAD, "paths": paths, "steps_per_path": N_STEPS, "requests": 2,
+                   "host_cores": threads,
+                   "note": "the reference CPU path (its C++ restatement) on the full workload every timed step"},
+        "cpu_baseline": {"value": value, "unit": "path-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"Heston + Merton Sobol {paths} paths x {N_STEPS} steps each (workload: {N_PATHS}), "
+                                   f"FP64, {args.steps} steps of {wall / max(args.steps, 1):.2f} s"},
         "e2e": {"value": value, "unit": "path-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

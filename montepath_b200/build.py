@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "lib")
 OBJ_DIR = os.path.join(OUT_DIR, "obj")
 LIBRARY = os.path.join(OUT_DIR, "libmontepath_cuda.so")
-SOURCES = ["mpc_kernels.cu", "mpc_runtime.cu", "mpc_server.cu", "mpc_peaks.cu", "mpc_noalloc.cu", "mpc_greeks.cu"]
+SOURCES = ["mpc_kernels.cu", "mpc_runtime.cu", "mpc_server.cu", "mpc_peaks.cu", "mpc_noalloc.cu", "mpc_greeks.cu", "mpc_merton.cu"]
 HEADERS = [
     "mpc_device.cuh",
     "mpc_launch.h",

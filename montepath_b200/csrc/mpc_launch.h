@@ -119,6 +119,32 @@ struct GreekArgs {
 cudaError_t launch_greeks_single_pass(const GreekArgs& a, uint32_t grid, const DeviceTables& tabs,
                                       cudaStream_t stream);
 
+// The reference's Merton estimator (terminal, pseudorandom): each chunk's
+// sequential MonteCarloRng stream is replayed and the variable number of
+// draws per path resolved by a parallel chain over 64-position segments
+// (mpc_merton.cu).  Per chunk, qpad stream positions (a multiple of
+// kMertonSegment, at least 3 per path plus one spare segment) and n_segs =
+// qpad / kMertonSegment - 1 segments.
+constexpr uint32_t kMertonSegment = 64;
+struct MertonStreamArgs {
+  uint64_t n_paths;             // all chunks
+  uint32_t n_chunks, cv;        // chunk count (1 = one stream); record controls
+  uint64_t chunk_base, chunk_rem;  // the reference's split of n_paths
+  uint64_t seed;                // request seed (chunk seeds derived from it)
+  uint64_t qpad, n_segs;
+  double mean, p0;              // lambda T and exp(-lambda T)
+  double log_s0, drift_t, vol_t, jump_mean, jump_vol, k, discount;
+  uint64_t* x;                  // [n_chunks][qpad] stream outputs
+  uint32_t* bits;               // [n_chunks][qpad / 32] jump bits
+  uint16_t* maps;               // [n_chunks][n_segs][9] segment maps
+  uint8_t* seg_state;           // [n_chunks][n_segs] entry state
+  unsigned long long* seg_before;  // [n_chunks][n_segs] paths before the segment
+  uint64_t* starts;             // [n_paths] path start states
+  double* payoff;               // [n_paths]
+  double* control;              // [n_paths] or null
+};
+cudaError_t launch_merton_stream(const MertonStreamArgs& a, const DeviceTables& tabs, cudaStream_t stream);
+
 // Device generators for the ABI's sampler entry points.
 cudaError_t launch_generate_normals(const DevReq& q, int sampler, int fp32, void* d_out, uint64_t n_points,
                                     uint32_t dims, const DeviceTables& tabs, cudaStream_t stream);

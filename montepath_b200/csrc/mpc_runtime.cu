@@ -250,10 +250,16 @@ int validate(const mpc_request_t& r, std::string* msg) {
     if (!(r.jump_intensity >= 0.0)) return invalid(msg, "jump_intensity must be >= 0");
     if (!(r.jump_volatility >= 0.0)) return invalid(msg, "jump_volatility must be >= 0");
     if (!finite(r.jump_mean)) return invalid(msg, "jump_mean must be finite");
-    if (r.sampling == MPC_SAMPLING_PSEUDORANDOM)
+    if (r.sampling == MPC_SAMPLING_PSEUDORANDOM && r.method == MPC_METHOD_STEPWISE)
       return unsupported(msg,
-                         "Merton draws a variable number of normals per path from one sequential stream; "
-                         "use scrambled_sobol, randomized_halton, latin_hypercube or counter_hash on the GPU");
+                         "stepwise Merton draws a variable number of normals per step from one sequential "
+                         "stream; the pseudorandom stream replay covers the reference's terminal Merton "
+                         "(method auto/terminal); use scrambled_sobol, randomized_halton, latin_hypercube or "
+                         "counter_hash for stepwise Merton");
+    if (r.sampling == MPC_SAMPLING_PSEUDORANDOM && r.technique != MPC_TECHNIQUE_STANDARD)
+      return unsupported(msg, "the reference's pseudorandom Merton estimator is the standard technique");
+    if (r.sampling == MPC_SAMPLING_PSEUDORANDOM && r.n_paths > (1ull << 30))
+      return unsupported(msg, "pseudorandom Merton supports at most 2^30 paths per request");
     if (r.technique == MPC_TECHNIQUE_ANTITHETIC) return unsupported(msg, "Merton supports standard and control variate");
   }
   uint64_t dims_per_unit = r.n_steps;
@@ -267,6 +273,12 @@ int validate(const mpc_request_t& r, std::string* msg) {
   if (r.sampling == MPC_SAMPLING_LATIN_HYPERCUBE && dims_per_unit > 8192)
     return unsupported(msg, "Latin hypercube supports at most 8192 dimensions");
   return MPC_OK;
+}
+
+// The reference's own Merton: terminal, pseudorandom (mpc_merton.cu).
+static bool merton_stream_request(const mpc_request_t& r) {
+  return r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.model == MPC_MODEL_MERTON &&
+         r.sampling == MPC_SAMPLING_PSEUDORANDOM && r.method != MPC_METHOD_STEPWISE;
 }
 
 uint64_t estimate_bytes(const mpc_request_t& r) {
@@ -293,6 +305,12 @@ uint64_t estimate_bytes(const mpc_request_t& r) {
   if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.model == MPC_MODEL_GBM && r.method != MPC_METHOD_STEPWISE)
     dims = 1;
   uint64_t partials = (units / 256 + 1) * 64 + 1024;
+  if (merton_stream_request(r)) {
+    // stream outputs and jump bits (3 positions per path + spare segments),
+    // segment maps and states, path starts, payoffs
+    const uint64_t positions = 3 * r.n_paths + 64 * (2 + std::max<uint64_t>(r.n_threads, 1)) + 64;
+    return positions * 8 + positions / 32 * 4 + positions / 64 * (18 + 1 + 8) + r.n_paths * 16 + partials;
+  }
   if (r.precision == MPC_PRECISION_FP64_PLAIN) return units * dims * 8 + units * 16 + partials;
   return partials + 2048;
 }
@@ -894,6 +912,95 @@ static int run_plain(mpc_context* ctx, Prepared* p, mpc_result_t* out, double* p
   return MPC_OK;
 }
 
+// The reference's terminal pseudorandom Merton: each chunk's MonteCarloRng
+// stream replayed on the device (mpc_merton.cu), payoffs reduced like the
+// plain path.  Both precisions run this FP64 pipeline: its cost is the stream
+// replay, and it reproduces the reference's per-path payoffs.
+static int run_merton_stream(mpc_context* ctx, Prepared* p, mpc_result_t* out, double* per_unit_host,
+                             uint64_t per_unit_cap) {
+  DevReq& q = p->q;
+  const uint64_t n = q.n_paths;
+  MertonStreamArgs a{};
+  a.n_paths = n;
+  a.n_chunks = q.n_chunks <= 1 ? 1 : q.n_chunks;
+  a.chunk_base = q.chunk_base;
+  a.chunk_rem = q.chunk_rem;
+  a.seed = q.seed;
+  a.cv = q.cv;
+  const uint64_t max_chunk = a.n_chunks <= 1 ? n : q.chunk_base + (q.chunk_rem ? 1 : 0);
+  const uint64_t positions = 3 * max_chunk + 8;  // a path reads at most 3 positions past its start
+  a.n_segs = (positions + kMertonSegment - 1) / kMertonSegment;
+  a.qpad = (a.n_segs + 1) * kMertonSegment;  // one spare segment: the last one reads 2 bits past its end
+  a.mean = q.lam_dt;                         // lambda T (terminal: dt = T)
+  a.p0 = q.lam_p0;                           // exp(-lambda T), as sample_poisson computes it
+  a.log_s0 = q.log_s0;
+  a.drift_t = q.drift_dt;
+  a.vol_t = q.vol_dt;
+  a.jump_mean = q.jump_mean;
+  a.jump_vol = q.jump_vol;
+  a.k = q.k;
+  a.discount = q.discount;
+  const uint64_t chunks = a.n_chunks, segs = a.n_segs * chunks;
+  void *d_x, *d_bits, *d_maps, *d_state, *d_before, *d_starts = nullptr, *d_pay, *d_ctl = nullptr;
+  void *d_req, *d_part, *d_mom, *d_done;
+  int st;
+  if ((st = scratch(ctx, "merton_x", chunks * a.qpad * sizeof(uint64_t), &d_x))) return st;
+  if ((st = scratch(ctx, "merton_bits", chunks * a.qpad / 32 * sizeof(uint32_t), &d_bits))) return st;
+  if ((st = scratch(ctx, "merton_maps", segs * 9 * sizeof(uint16_t), &d_maps))) return st;
+  if ((st = scratch(ctx, "merton_state", segs, &d_state))) return st;
+  if ((st = scratch(ctx, "merton_before", segs * sizeof(uint64_t), &d_before))) return st;
+  if (a.mean != 0.0 && (st = scratch(ctx, "merton_starts", n * sizeof(uint64_t), &d_starts))) return st;
+  if ((st = scratch(ctx, "plain_pay", n * sizeof(double), &d_pay))) return st;
+  if (q.cv && (st = scratch(ctx, "plain_ctl", n * sizeof(double), &d_ctl))) return st;
+  a.x = static_cast<uint64_t*>(d_x);
+  a.bits = static_cast<uint32_t*>(d_bits);
+  a.maps = static_cast<uint16_t*>(d_maps);
+  a.seg_state = static_cast<uint8_t*>(d_state);
+  a.seg_before = static_cast<unsigned long long*>(d_before);
+  a.starts = static_cast<uint64_t*>(d_starts);
+  a.payoff = static_cast<double*>(d_pay);
+  a.control = static_cast<double*>(d_ctl);
+  q.tile_units = 2048;
+  q.n_tiles = uint32_t((n + q.tile_units - 1) / q.tile_units);
+  if ((st = scratch(ctx, "plain_req", sizeof(DevReq), &d_req))) return st;
+  if ((st = scratch(ctx, "plain_part", size_t(q.n_tiles) * MPC_MOMENTS * sizeof(double), &d_part))) return st;
+  if ((st = scratch(ctx, "plain_mom", MPC_MOMENTS * sizeof(double), &d_mom))) return st;
+  if ((st = scratch(ctx, "plain_done", 16, &d_done))) return st;
+  q.partials = static_cast<double*>(d_part);
+  q.moments = static_cast<double*>(d_mom);
+  q.tiles_done = static_cast<uint32_t*>(d_done);
+  q.per_unit = nullptr;
+  void* pin = nullptr;
+  if ((st = pinned_staging(ctx, sizeof(DevReq) + MPC_MOMENTS * sizeof(double), &pin))) return st;
+  std::memcpy(pin, &q, sizeof(DevReq));
+  double* hm = reinterpret_cast<double*>(static_cast<uint8_t*>(pin) + sizeof(DevReq));
+  uint64_t launches_before = kernel_launch_count();
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+  MPC_CUDA(ctx, cudaMemcpyAsync(d_req, pin, sizeof(DevReq), cudaMemcpyHostToDevice, ctx->stream));
+  MPC_CUDA(ctx, cudaMemsetAsync(d_done, 0, 16, ctx->stream));
+  cudaError_t e = launch_merton_stream(a, ctx->tabs, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "Merton stream replay");
+  e = launch_plain_reduce(static_cast<DevReq*>(d_req), a.payoff, a.control, n, q.n_tiles, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "Merton reduction");
+  MPC_CUDA(ctx, cudaMemcpyAsync(hm, d_mom, MPC_MOMENTS * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  MPC_CUDA(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+  MPC_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop);
+  ctx->last_ms = ms;
+  ctx->last_launches = kernel_launch_count() - launches_before;
+  ctx->last_h2d = sizeof(DevReq);
+  ctx->last_d2h = MPC_MOMENTS * sizeof(double);
+  summarize_moments(*p, hm, out);
+  out->path_steps = p->path_steps;
+  out->runtime_ms = ms;
+  if (per_unit_host) {
+    uint64_t count = std::min<uint64_t>(per_unit_cap, n);
+    MPC_CUDA(ctx, cudaMemcpy(per_unit_host, d_pay, count * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return MPC_OK;
+}
+
 // ------------------------------------------------------------------- LSM ---
 static double powi(double a, int b) {  // f64::powi as compiler-rt __powidf2
   bool recip = b < 0;
@@ -1411,7 +1518,9 @@ static int price_one(mpc_context* ctx, const mpc_request_t* req, mpc_result_t* o
       out->status = st;
       return fail(ctx, st, msg);
     }
-    if (p.plain) {
+    if (merton_stream_request(*req)) {
+      st = run_merton_stream(ctx, &p, out, per_unit, cap);
+    } else if (p.plain) {
       st = run_plain(ctx, &p, out, per_unit, cap);
     } else {
       std::vector<Prepared*> pp{&p};
@@ -2100,7 +2209,7 @@ int mpc_price_batch(mpc_context_t* ctx, const mpc_request_t* reqs, size_t n, mpc
     int st = validate(reqs[i], &msg);
     if (st == MPC_OK && reqs[i].workload != MPC_WORKLOAD_ASIAN_MLMC && !is_lsm(reqs[i].workload)) {
       st = prepare(ctx, reqs[i], &preps[i], &msg);
-      if (st == MPC_OK && !preps[i].plain) {
+      if (st == MPC_OK && !preps[i].plain && !merton_stream_request(reqs[i])) {
         fused.push_back(&preps[i]);
         fused_out.push_back(&out[i]);
         continue;
@@ -2124,7 +2233,7 @@ int mpc_price_batch(mpc_context_t* ctx, const mpc_request_t* reqs, size_t n, mpc
       mlmc_out.push_back(&out[i]);
       continue;
     }
-    // FP64-plain requests run one launch sequence each
+    // FP64-plain requests and the pseudorandom Merton replay run one launch sequence each
     st = price_one(ctx, &reqs[i], &out[i], nullptr, 0);
     total_ms += ctx->last_ms;
     if (st != MPC_OK && first_error == MPC_OK) first_error = st;

@@ -16,6 +16,7 @@ the GPU; a request the device path cannot run raises with its status code.
 
 from __future__ import annotations
 
+import math
 import threading
 from typing import Any, Mapping
 
@@ -178,19 +179,11 @@ def price_heston_european_call(config: Mapping[str, Any]) -> dict:
 
 
 def price_merton_jump_diffusion_call(config: Mapping[str, Any]) -> dict:
-    """The reference Merton config has no sampling field (cpu.rs:1470-1482) and
-    draws a variable number of normals per path from one stream, which a
-    parallel device cannot replay; pseudorandom requests use the stateless
-    counter-hash generator instead."""
+    """The reference Merton estimator (cpu.rs:3151-3189): terminal sampling from
+    the pseudorandom MonteCarloRng stream of each chunk, which the device
+    replays exactly (per-path payoffs equal the reference's)."""
 
-    cfg = dict(config or {})
-    extra = {"model": "merton"}
-    if cfg.get("sampling", "pseudorandom") in (None, "pseudorandom"):
-        extra["sampling"] = "counter_hash"
-    out = _price("european_call", "price_merton_jump_diffusion_call", cfg, extra)
-    if "sampling" in extra:
-        out["warnings"].append("pseudorandom Merton runs on the counter-hash generator (statistically equivalent)")
-    return out
+    return _price("european_call", "price_merton_jump_diffusion_call", config, {"model": "merton"})
 
 
 def arithmetic_asian_mlmc(config: Mapping[str, Any]) -> dict:
@@ -199,8 +192,47 @@ def arithmetic_asian_mlmc(config: Mapping[str, Any]) -> dict:
     return out
 
 
+def _standard_normal_cdf(x: float) -> float:
+    """standard_normal_cdf (cpu.rs:898-910): Abramowitz-Stegun 7.1.26 erf."""
+
+    sign = -1.0 if x < 0.0 else 1.0
+    z = abs(x) / math.sqrt(2.0)
+    t = 1.0 / (1.0 + 0.3275911 * z)
+    a1, a2, a3, a4, a5 = 0.254829592, -0.284496736, 1.421413741, -1.453152027, 1.061405429
+    poly = (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t
+    return 0.5 * (1.0 + sign * (1.0 - poly * math.exp(-z * z)))
+
+
+def black_scholes_european_call_price(s0: float, k: float, r: float, sigma: float, t: float) -> float:
+    """black_scholes_european_call_price (cpu.rs:839-860), the sweep's analytic column."""
+
+    if k == 0.0:
+        return s0
+    if t == 0.0:
+        return max(s0 - k, 0.0)
+    if sigma == 0.0:
+        return max(s0 - k * math.exp(-r * t), 0.0)
+    sqrt_t = math.sqrt(t)
+    d1 = (math.log(s0 / k) + (r + 0.5 * sigma * sigma) * t) / (sigma * sqrt_t)
+    d2 = d1 - sigma * sqrt_t
+    return s0 * _standard_normal_cdf(d1) - k * math.exp(-r * t) * _standard_normal_cdf(d2)
+
+
+# EuropeanCallSweepScenario fields (cpu.rs:5044-5082) and their mapping-ABI aliases
+_SWEEP_FIELDS = {
+    "s0": ("s0", "spot"), "k": ("k", "strike"), "r": ("r", "rate"), "sigma": ("sigma", "volatility"),
+    "t": ("t", "maturity"), "n_paths": ("n_paths", "paths"), "n_steps": ("n_steps", "steps"),
+    "sampling": ("sampling",), "technique": ("technique",),
+}
+
+
 def price_european_call_parameter_sweep(config: Mapping[str, Any]) -> dict:
-    """price_european_call_parameter_sweep_cpu (cpu.rs:3028-3096) as one batched launch."""
+    """price_european_call_parameter_sweep_cpu (cpu.rs:3028-3096) as one batched
+    launch: each scenario overrides the base config, takes seed
+    base + seed_stride * index unless it names its own (cpu.rs:5071-5074), and
+    its row carries the Black-Scholes price and the error in standard errors;
+    scenarios more than 4 standard errors away raise a warning, as the
+    reference's do."""
 
     cfg = dict(config or {})
     base = dict(cfg.get("base_config") or {})
@@ -209,14 +241,20 @@ def price_european_call_parameter_sweep(config: Mapping[str, Any]) -> dict:
             base[key] = cfg[key]
     stride = int(cfg.get("seed_stride", 10_000))
     method = cfg.get("method", "terminal_distribution")
-    scenarios = cfg.get("scenarios") or [{"scenario_id": "base"}]
+    scenarios = cfg.get("scenarios") or [
+        {"scenario_id": "atm_base"}, {"scenario_id": "down_10pct", "s0": 90.0}, {"scenario_id": "high_vol", "sigma": 0.35},
+    ]  # EuropeanCallParameterSweepConfig::default (cpu.rs:1378-1402)
     reqs, rows_cfg = [], []
     for index, sc in enumerate(scenarios):
         sc = dict(sc)
         scenario_cfg = dict(base)
-        for key in ("spot", "strike", "rate", "volatility", "maturity", "n_paths", "n_steps", "sampling", "technique"):
-            if sc.get(key) is not None:
-                scenario_cfg[key] = sc[key]
+        for field, keys in _SWEEP_FIELDS.items():
+            for key in keys:
+                if sc.get(key) is not None:
+                    for alias in keys:
+                        scenario_cfg.pop(alias, None)
+                    scenario_cfg[field] = sc[key]
+                    break
         seed = sc.get("seed")
         scenario_cfg["seed"] = int(seed) if seed is not None else (int(base.get("seed", 42)) + stride * index) % (1 << 64)
         scenario_cfg["method"] = sc.get("method") or method
@@ -226,14 +264,24 @@ def price_european_call_parameter_sweep(config: Mapping[str, Any]) -> dict:
         results = backend().price_batch(reqs)
     except BackendError as exc:
         raise ValueError(f"MC_BACKEND_CUDA_{exc.code.replace('MPC_E_', '')}: {exc}") from exc
-    rows = []
+    rows, warnings = [], []
     for index, ((sid, sc), req, res) in enumerate(zip(rows_cfg, reqs, results)):
-        rows.append({"scenario_index": index, "scenario_id": sid, "config": sc, "price": res.price, "stderr": res.stderr})
+        analytic = black_scholes_european_call_price(req.s0, req.k, req.r, req.sigma, req.t)
+        signed = res.price - analytic
+        err = abs(signed)
+        units = err / res.stderr if res.stderr > 0.0 else (0.0 if err == 0.0 else math.inf)
+        if units > 4.0:
+            warnings.append(f"scenario '{sid}' is {units:.3f} standard errors from Black-Scholes reference")
+        rows.append({"scenario_index": index, "scenario_id": sid, "method": sc["method"], "config": sc,
+                     "price": res.price, "stderr": res.stderr, "analytic_price": analytic,
+                     "signed_error_vs_black_scholes": signed, "abs_error_vs_black_scholes": err,
+                     "abs_error_stderr_units": units})
     return {
         "values": {"schema_version": "european-call-sweep.v1", "scenario_count": len(rows), "rows": rows,
-                   "total_paths": sum(r.n_paths for r in reqs)},
+                   "total_paths": sum(r.n_paths for r in reqs), "base_seed": int(base.get("seed", 42)),
+                   "seed_stride": stride},
         "manifest": _manifest("european_call_parameter_sweep", "price_european_call_parameter_sweep", cfg, reqs[0]),
-        "warnings": [],
+        "warnings": warnings,
     }
 
 

@@ -12,7 +12,7 @@ Rust ``Default`` values (``mpc_request_defaults``).
 from __future__ import annotations
 
 import ctypes
-from typing import Any, Mapping
+from typing import Any, Callable, Mapping
 
 from . import abi
 
@@ -45,13 +45,17 @@ def defaults(workload: int) -> abi.Request:
     return req
 
 
-def make_request(workload: str | int, config: Mapping[str, Any] | None = None, **overrides: Any) -> abi.Request:
-    """Request for `workload` (a name of ``abi.WORKLOADS`` or its code) from a config mapping."""
+def make_request(workload: str | int, config: Mapping[str, Any] | None = None, *,
+                 defaults: Callable[[int], abi.Request] | None = None, **overrides: Any) -> abi.Request:
+    """Request for `workload` (a name of ``abi.WORKLOADS`` or its code) from a config mapping.
+
+    `defaults(code)` supplies the starting request (the library's
+    ``mpc_request_defaults`` unless given)."""
 
     cfg: dict[str, Any] = dict(config or {})
     cfg.update(overrides)
     code = abi.WORKLOADS[workload] if isinstance(workload, str) else int(workload)
-    req = defaults(code)
+    req = (defaults or globals()["defaults"])(code)
 
     def f64(attr: str, *keys: str) -> None:
         value = _lookup(cfg, keys or (attr,))

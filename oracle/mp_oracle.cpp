@@ -1858,6 +1858,85 @@ void or_generate_uniforms(int sampling, uint64_t seed, uint64_t n_points, uint64
 }
 
 int or_price(const mpc_request_t* req, mpc_result_t* res) { return orc::price(*req, res, orc::Out{}); }
+
+// The reference configs' Default values (cpu.rs:1311-1327 EuropeanCallConfig,
+// 1448-1466 Heston, 1484-1500 Merton, 1517-1533 Asian, 1551-1568 MLMC,
+// 1620-1630 MLMC tolerance, 1660-1678 down-and-out, 1694-1710 lookback,
+// 1731-1751 basket, 1767-1781 American put, 1799-1815 Bermudan put), folded
+// into one request: the fields a workload's config does not have are the
+// values of the config that has them.  The up-and-out barrier (120) has no
+// reference config.  The oracle's own copy, so that a caller of the oracle
+// (the CPU reference arm of the benchmark) needs nothing from the CUDA library.
+int or_request_defaults(mpc_request_t* r, int workload) {
+  if (!r) return MPC_E_INVALID_CONFIG;
+  std::memset(r, 0, sizeof(*r));
+  r->workload = workload;
+  r->model = MPC_MODEL_GBM;
+  r->method = MPC_METHOD_AUTO;
+  r->technique = MPC_TECHNIQUE_STANDARD;
+  r->sampling = MPC_SAMPLING_PSEUDORANDOM;
+  r->precision = MPC_PRECISION_FP32_PATH;
+  r->n_paths = 100000;
+  r->n_steps = 252;
+  r->seed = 42;
+  r->s0 = 100.0;
+  r->k = 100.0;
+  r->r = 0.03;
+  r->sigma = 0.2;
+  r->t = 1.0;
+  r->v0 = 0.04;
+  r->kappa = 1.5;
+  r->theta = 0.04;
+  r->vol_of_vol = 0.3;
+  r->rho = -0.6;
+  r->jump_intensity = 0.4;
+  r->jump_mean = -0.08;
+  r->jump_volatility = 0.25;
+  r->n_assets = 2;
+  r->spots[0] = 100.0;
+  r->spots[1] = 95.0;
+  r->sigmas[0] = 0.2;
+  r->sigmas[1] = 0.25;
+  r->weights[0] = 0.5;
+  r->weights[1] = 0.5;
+  r->corr[0] = 1.0;
+  r->corr[1] = 0.35;
+  r->corr[2] = 0.35;
+  r->corr[3] = 1.0;
+  r->basis_degree = 2;
+  r->base_steps = 16;
+  r->levels = 4;
+  r->refinement_factor = 2;
+  r->scramble_replicates = 1;
+  const uint64_t ppl[4] = {50000, 25000, 12500, 6250};
+  for (int i = 0; i < 4; ++i) r->paths_per_level[i] = ppl[i];
+  r->pilot_paths_per_level = 2048;
+  r->min_step_updates = 100000;
+  r->max_step_updates = 10000000;
+  switch (workload) {
+    case MPC_WORKLOAD_DOWN_AND_OUT_CALL:
+      r->barrier = 80.0;
+      break;
+    case MPC_WORKLOAD_UP_AND_OUT_CALL:
+      r->barrier = 120.0;
+      break;
+    case MPC_WORKLOAD_AMERICAN_PUT:
+      r->n_steps = 64;
+      break;
+    case MPC_WORKLOAD_BERMUDAN_PUT:
+      r->n_steps = 64;
+      r->n_exercise = 4;
+      for (int i = 0; i < 4; ++i) r->exercise_steps[i] = 16u * uint32_t(i + 1);
+      break;
+    case MPC_WORKLOAD_BASKET_CALL:
+      r->method = MPC_METHOD_TERMINAL;
+      r->n_steps = 1;
+      break;
+    default:
+      break;
+  }
+  return (workload < 0 || workload > MPC_WORKLOAD_ASIAN_MLMC) ? MPC_E_INVALID_CONFIG : MPC_OK;
+}
 int or_greeks(const mpc_request_t* req, int estimator, mpc_greek_report_t* out) {
   return orc::greeks(*req, estimator, out);
 }

@@ -62,6 +62,7 @@ def lib() -> ctypes.CDLL:
         "or_generate_normals": (None, [c_int, c_uint64, c_uint64, c_uint64, POINTER(c_double)]),
         "or_generate_uniforms": (None, [c_int, c_uint64, c_uint64, c_uint64, POINTER(c_double)]),
         "or_price": (c_int, [POINTER(abi.Request), POINTER(abi.Result)]),
+        "or_request_defaults": (c_int, [POINTER(abi.Request), c_int]),
         "or_greeks": (c_int, [POINTER(abi.Request), c_int, POINTER(abi.GreekReport)]),
         "or_price_paths": (c_int, [POINTER(abi.Request), POINTER(abi.Result), POINTER(c_double), c_uint64]),
         "or_price_from_f32_normals": (
@@ -116,6 +117,24 @@ def generate_uniforms(sampling: int, seed: int, n_points: int, dims: int) -> np.
     out = np.zeros(n_points * dims, dtype=np.float64)
     lib().or_generate_uniforms(sampling, seed, n_points, dims, _ptr(out, c_double))
     return out.reshape(n_points, dims)
+
+
+def request_defaults(workload: int) -> abi.Request:
+    """The reference configs' Default values, from the oracle's own copy."""
+
+    req = abi.Request()
+    if lib().or_request_defaults(ctypes.byref(req), int(workload)) != 0:
+        raise ValueError(f"unknown workload {workload}")
+    return req
+
+
+def make_request(workload, config=None, **overrides) -> abi.Request:
+    """A request built from a config mapping like montepath_b200.requests.make_request,
+    with the oracle's defaults: loads nothing from the CUDA library."""
+
+    from montepath_b200.requests import make_request as _make
+
+    return _make(workload, config, defaults=request_defaults, **overrides)
 
 
 def price(req: abi.Request) -> abi.Result:

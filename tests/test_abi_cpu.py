@@ -81,7 +81,9 @@ def validate(r):
         ("european_call", dict(t=0.0), abi.E_INVALID_CONFIG),
         ("european_call", dict(model="heston", rho=1.5), abi.E_INVALID_CONFIG),
         ("european_call", dict(model="heston", vol_of_vol=-0.1), abi.E_INVALID_CONFIG),
-        ("european_call", dict(model="merton", sampling="pseudorandom"), abi.E_UNSUPPORTED),
+        ("european_call", dict(model="merton", method="stepwise", sampling="pseudorandom"), abi.E_UNSUPPORTED),
+        ("european_call", dict(model="merton", sampling="pseudorandom", technique="control_variate"),
+         abi.E_UNSUPPORTED),
         ("european_call", dict(model="merton", sampling="scrambled_sobol", technique="antithetic"), abi.E_UNSUPPORTED),
         ("european_call", dict(method="stepwise", n_steps=70_000, sampling="scrambled_sobol_brownian_bridge"),
          abi.E_UNSUPPORTED),
@@ -111,6 +113,7 @@ def test_valid_requests_pass():
               "american_put", "bermudan_put", "arithmetic_asian_mlmc"):
         assert validate(make_request(w))[0] == abi.OK, w
     assert validate(make_request("european_call", model="merton", sampling="counter_hash"))[0] == abi.OK
+    assert validate(make_request("european_call", model="merton", sampling="pseudorandom"))[0] == abi.OK
     assert validate(make_request("european_call", block_size=256, paths_per_thread=4))[0] == abi.OK
 
 
@@ -202,7 +205,9 @@ def test_mapping_abi_response_shape(monkeypatch):
     assert out["manifest"]["backend"] == "nvidia_cuda"
     assert out["manifest"]["config"] == cfg
     mer = native.price_merton_jump_diffusion_call(dict(cfg, jump_intensity=0.4, jump_mean=-0.08, jump_volatility=0.25))
-    assert any("counter-hash" in w for w in mer["warnings"])
+    ref = O.price(make_request("european_call", dict(model="merton", n_paths=2000, seed=42, jump_intensity=0.4,
+                                                     jump_mean=-0.08, jump_volatility=0.25)))
+    assert mer["price"] == ref.price  # the reference's own pseudorandom Merton, not a substitute stream
     lsm = native.price_american_put(dict(cfg, basis_degree=5, n_steps=16))
     assert lsm["values"]["regression_basis"] == "laguerre_lsm_degree_3"
     with pytest.raises(ValueError):

@@ -771,7 +771,7 @@ def test_invalid_config_returns_code(backend):
     with pytest.raises(BackendError) as err:
         backend.price(r)
     assert err.value.status == abi.E_INVALID_CONFIG
-    r = req("european_call", model="merton", sampling="pseudorandom")
+    r = req("european_call", model="merton", method="stepwise", sampling="pseudorandom")
     with pytest.raises(BackendError) as err:
         backend.price(r)
     assert err.value.status == abi.E_UNSUPPORTED
