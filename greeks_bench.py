@@ -1,18 +1,22 @@
 """Bump-and-revalue Greeks timing: each case's report (all legs in one
 scenario launch that draws every normal once) against the same legs priced
 as one ``mpc_price_batch``.  Device times from CUDA events, L2 flushed before
-each timed call, best of five.  ``python -m montepath_b200.greeks_bench``
-prints one JSON object."""
+each timed call, best of five.  ``python greeks_bench.py`` prints one JSON
+object."""
 
 from __future__ import annotations
 
 import argparse
 import json
 import math
+import os
+import sys
 
-from . import abi
-from .backend import CudaBackend
-from .requests import make_request
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+from montepath_b200 import abi  # noqa: E402
+from montepath_b200.backend import CudaBackend  # noqa: E402
+from montepath_b200.requests import make_request  # noqa: E402
 
 BASKET5 = {"spots": [100.0, 95.0, 105.0, 90.0, 110.0], "sigmas": [0.2, 0.25, 0.3, 0.35, 0.4], "corr": 0.3}
 CASES = {
