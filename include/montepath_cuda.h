@@ -299,7 +299,8 @@ typedef struct mpc_server_options {
   uint64_t hbm_budget_bytes; /* admission budget (0 = 64 GiB) */
   uint32_t max_slots;        /* live requests on the device at once (0 = 256) */
   uint32_t wave_tiles;       /* tiles per scheduling wave (0 = auto) */
-  uint32_t mode;             /* 0 = continuous batching, 1 = plain FIFO, one request per launch in FP64 */
+  uint32_t mode;             /* 0 = continuous batching in host-scheduled waves, 1 = plain FIFO, one request
+                                per launch in FP64, 2 = continuous batching in a resident device loop */
   uint32_t _pad0;
 } mpc_server_options_t;
 

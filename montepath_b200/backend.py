@@ -149,18 +149,27 @@ class CudaBackend:
         self._check(self.lib.mpc_estimate_cost_ctx(self.handle, byref(req), byref(cost)))
         return cost
 
-    def server(self, hbm_budget_bytes: int = 0, max_slots: int = 0, wave_tiles: int = 0, plain: bool = False) -> "Server":
-        return Server(self, hbm_budget_bytes, max_slots, wave_tiles, plain)
+    def server(self, hbm_budget_bytes: int = 0, max_slots: int = 0, wave_tiles: int = 0, plain: bool = False,
+               mode: str | None = None) -> "Server":
+        """mode: "device_loop" (resident device loop), "waves" (host-scheduled
+        waves) or "plain" (FIFO FP64, one request per launch); `plain=True`
+        selects "plain"; the default is "device_loop"."""
+        return Server(self, hbm_budget_bytes, max_slots, wave_tiles, mode or ("plain" if plain else "device_loop"))
+
+
+SERVER_MODES = {"waves": 0, "plain": 1, "device_loop": 2}
 
 
 class Server:
-    """Serving loop (``mpc_server_start``): continuous batching, or the plain FIFO baseline."""
+    """Serving loop (``mpc_server_start``): the resident device loop,
+    host-scheduled waves, or the plain FIFO baseline."""
 
-    def __init__(self, backend: CudaBackend, hbm_budget_bytes: int, max_slots: int, wave_tiles: int, plain: bool):
+    def __init__(self, backend: CudaBackend, hbm_budget_bytes: int, max_slots: int, wave_tiles: int, mode: str):
         self.backend = backend
         self.lib = backend.lib
+        self.mode = mode
         opts = abi.ServerOptions(
-            hbm_budget_bytes=hbm_budget_bytes, max_slots=max_slots, wave_tiles=wave_tiles, mode=1 if plain else 0
+            hbm_budget_bytes=hbm_budget_bytes, max_slots=max_slots, wave_tiles=wave_tiles, mode=SERVER_MODES[mode]
         )
         handle = c_void_p()
         status = self.lib.mpc_server_start(backend.handle, byref(opts), byref(handle))

@@ -1064,6 +1064,51 @@ constexpr int fused_min_blocks(int fam, int smp) {
   return fam < 0 ? 2 : ((fam == FAM_GBM_STEP || fam == FAM_GBM_TERMINAL) && smp == SMP_COUNTER ? 6 : 4);
 }
 
+// One tile of request `sq`: its units through the model, the block's moment
+// sums written as the tile's partial, and *s_last (shared) set when this was
+// the request's last tile to finish.  Ends with the block synchronised.
+template <int FAM, int SMP>
+__device__ __forceinline__ void fused_tile(const DevReq& sq, const SrcCtx& ctx, uint32_t tile, double (*red)[5],
+                                           int* s_last) {
+  const uint64_t first = (uint64_t)tile * sq.tile_units;
+  const uint64_t last = min(first + (uint64_t)sq.tile_units, sq.n_units);
+  double v[5] = {0, 0, 0, 0, 0};
+  const bool cv = sq.cv != 0;
+  double* per_unit = sq.per_unit;
+  // Every thread runs the same number of units so that block-synchronous
+  // sources stay in lockstep; a thread past the tile end repeats the first
+  // unit and discards it.
+  const uint32_t iters = (uint32_t)((last - first + blockDim.x - 1) / blockDim.x);
+  for (uint32_t it = 0; it < iters; ++it) {
+    uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
+    const bool valid = u < last;
+    if (!valid) u = first;
+    double p, c;
+    if constexpr (FAM >= 0)
+      fused_unit<FAM, SMP>(sq, ctx, u, p, c);
+    else
+      fused_unit_any<SMP>(sq, ctx, u, p, c);
+    if (!valid) continue;
+    v[0] += p;
+    v[1] += p * p;
+    if (cv) {
+      v[2] += c;
+      v[3] += c * c;
+      v[4] += p * c;
+    }
+    if (per_unit) per_unit[u] = p;
+  }
+  block_reduce5(v, red);
+  if (threadIdx.x == 0) {
+    double* pt = sq.partials + (size_t)tile * MPC_MOMENTS;
+    pt[0] = (double)(last - first);
+    for (int i = 0; i < 5; ++i) pt[1 + i] = v[i];
+    __threadfence();
+    *s_last = (atomicAdd(sq.tiles_done, 1u) == sq.n_tiles - 1) ? 1 : 0;
+  }
+  __syncthreads();
+}
+
 // FAM >= 0: every request in the list has that family; FAM < 0: switch per tile.
 template <int FAM, int SMP>
 __global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused_kernel(const DevReq* __restrict__ reqs,
@@ -1097,43 +1142,7 @@ __global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused
       for (uint32_t i = threadIdx.x; i < sizeof(DevReq) / sizeof(uint4); i += blockDim.x) dst[i] = src[i];
     }
     __syncthreads();
-    const uint64_t first = (uint64_t)tl.tile * sq.tile_units;
-    const uint64_t last = min(first + (uint64_t)sq.tile_units, sq.n_units);
-    double v[5] = {0, 0, 0, 0, 0};
-    const bool cv = sq.cv != 0;
-    double* per_unit = sq.per_unit;
-    // Every thread runs the same number of units so that block-synchronous
-    // sources stay in lockstep; a thread past the tile end repeats the first
-    // unit and discards it.
-    const uint32_t iters = (uint32_t)((last - first + blockDim.x - 1) / blockDim.x);
-    for (uint32_t it = 0; it < iters; ++it) {
-      uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
-      const bool valid = u < last;
-      if (!valid) u = first;
-      double p, c;
-      if constexpr (FAM >= 0)
-        fused_unit<FAM, SMP>(sq, ctx, u, p, c);
-      else
-        fused_unit_any<SMP>(sq, ctx, u, p, c);
-      if (!valid) continue;
-      v[0] += p;
-      v[1] += p * p;
-      if (cv) {
-        v[2] += c;
-        v[3] += c * c;
-        v[4] += p * c;
-      }
-      if (per_unit) per_unit[u] = p;
-    }
-    block_reduce5(v, red);
-    if (threadIdx.x == 0) {
-      double* pt = sq.partials + (size_t)tl.tile * MPC_MOMENTS;
-      pt[0] = (double)(last - first);
-      for (int i = 0; i < 5; ++i) pt[1 + i] = v[i];
-      __threadfence();
-      s_last = (atomicAdd(sq.tiles_done, 1u) == sq.n_tiles - 1) ? 1 : 0;
-    }
-    __syncthreads();
+    fused_tile<FAM, SMP>(sq, ctx, tl.tile, red, &s_last);
     if (s_last) {
       __threadfence();
       finalize_request(sq, red);
@@ -1205,6 +1214,146 @@ cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_t
     default:
       return cudaErrorInvalidValue;
   }
+}
+
+// ---------------------------------------------------- resident serving loop ---
+__device__ __forceinline__ uint32_t ld_acquire_sys(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_sys(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t loop_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Thread 0: the next tile to run, or 0 when the block should leave (stop,
+// pause, or idle_ns without claimable work).  Every poll of host memory is
+// followed by a sleep that doubles up to 32 us while idle.
+__device__ __forceinline__ int loop_claim(const LoopArgs& a, uint32_t& cursor, uint32_t* slot, uint32_t* tile,
+                                          uint32_t* gen) {
+  uint64_t idle_since = 0;
+  uint32_t nap = 1000;
+  for (;;) {
+    if (ld_acquire_sys(a.control) | ld_acquire_sys(a.control + 1)) return 0;
+    const uint32_t tail = ld_acquire_sys(a.tail);
+    for (uint32_t pos = cursor; pos != tail; ++pos) {
+      const LoopEntry* ep = a.ring + (pos % a.ring_cap);
+      LoopEntry e;
+      asm volatile("ld.volatile.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+                   : "=r"(e.slot), "=r"(e.gen), "=r"(e.n_tiles), "=r"(e.pos)
+                   : "l"(ep));
+      bool exhausted = e.pos != pos || e.slot >= a.max_slots;  // overwritten entries were finished
+      if (!exhausted) {
+        unsigned long long* cw = a.claim + e.slot;
+        unsigned long long v = atomicAdd(cw, 0ull);
+        for (int tries = 0; tries < 64; ++tries) {  // bounded: contention leaves the entry for the next pass
+          if ((uint32_t)(v >> 32) != e.gen || (uint32_t)v >= e.n_tiles) {
+            exhausted = true;
+            break;
+          }
+          const unsigned long long w = atomicCAS(cw, v, v + 1ull);
+          if (w == v) {
+            *slot = e.slot;
+            *tile = (uint32_t)v;
+            *gen = e.gen;
+            return 1;
+          }
+          v = w;
+        }
+      }
+      if (exhausted && pos == cursor) cursor = pos + 1;
+    }
+    const uint64_t now = loop_ns();
+    if (idle_since == 0)
+      idle_since = now;
+    else if (now - idle_since > a.idle_ns)
+      return 0;
+    __nanosleep(nap);
+    nap = nap < 32000u ? 2u * nap : 32000u;
+  }
+}
+
+// The loop's tile body per sampler, kept out of line so that each sampler's
+// register allocation stands on its own.
+template <int SMP>
+__device__ __noinline__ void loop_tile(const DevReq& sq, const SrcCtx& ctx, uint32_t tile, double (*red)[5],
+                                       int* s_last) {
+  fused_tile<-1, SMP>(sq, ctx, tile, red, s_last);
+}
+
+__global__ void __launch_bounds__(kFusedBlock, 2) serve_loop_kernel(LoopArgs a, SrcCtx ctx) {
+  extern __shared__ __align__(16) uint32_t sobol_window[];
+  {  // Sobol window rows, then the inverse-normal segments (staged once per launch)
+    float4* seg = reinterpret_cast<float4*>(sobol_window + kSobolWindowWords);
+    const float4* src = reinterpret_cast<const float4*>(ctx.sobol + MPC_ICDF_OFFSET);
+    for (uint32_t i = threadIdx.x; i < MPC_ICDF_SEGMENTS; i += blockDim.x) seg[i] = src[i];
+    ctx.win = sobol_window;
+    ctx.icdf = seg;
+  }
+  __shared__ DevReq sq;
+  __shared__ double red[kWarps][5];
+  __shared__ uint32_t s_slot, s_tile, s_gen, s_go;
+  __shared__ int s_last;
+  uint32_t cursor = 0;  // thread 0: ring entries before it have no tile left to claim
+  for (;;) {
+    if (threadIdx.x == 0) s_go = loop_claim(a, cursor, &s_slot, &s_tile, &s_gen);
+    __syncthreads();
+    if (!s_go) break;
+    {  // the slot's descriptor, through L2 (the host rewrites slots between requests)
+      const uint4* src = reinterpret_cast<const uint4*>(a.slots + s_slot);
+      uint4* dst = reinterpret_cast<uint4*>(&sq);
+      for (uint32_t i = threadIdx.x; i < sizeof(DevReq) / sizeof(uint4); i += blockDim.x) dst[i] = __ldcg(src + i);
+    }
+    __syncthreads();
+    switch (sq.sampling) {
+      case MPC_SAMPLING_PSEUDORANDOM:
+        loop_tile<SMP_XORSHIFT>(sq, ctx, s_tile, red, &s_last);
+        break;
+      case MPC_SAMPLING_COUNTER_HASH:
+        loop_tile<SMP_COUNTER>(sq, ctx, s_tile, red, &s_last);
+        break;
+      default:  // scrambled Sobol (the host publishes no other sampler)
+        loop_tile<SMP_SOBOL>(sq, ctx, s_tile, red, &s_last);
+        break;
+    }
+    if (s_last) {
+      __threadfence();
+      finalize_request(sq, red);  // moments go to mapped host memory
+      if (threadIdx.x == 0) {
+        __threadfence_system();
+        st_release_sys(a.done + s_slot, s_gen);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+constexpr size_t kLoopSmem = kSobolWindowWords * sizeof(uint32_t) + MPC_ICDF_SEGMENTS * sizeof(float4);
+
+cudaError_t launch_serve_loop(const LoopArgs& a, const DeviceTables& tabs, int grid, cudaStream_t stream) {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(serve_loop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kLoopSmem));
+  });
+  SrcCtx ctx{tabs.sobol, tabs.jump, nullptr, nullptr};
+  serve_loop_kernel<<<grid, kFusedBlock, kLoopSmem, stream>>>(a, ctx);
+  count_launch();
+  return cudaGetLastError();
+}
+
+int serve_loop_blocks_per_sm() {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(serve_loop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kLoopSmem));
+  });
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, serve_loop_kernel, kFusedBlock, kLoopSmem);
+  return n;
 }
 
 template <int FAM, int SMP>

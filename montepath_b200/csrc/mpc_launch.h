@@ -22,6 +22,33 @@ cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_t
                          cudaStream_t stream);
 int fused_max_blocks_per_sm(int family, int sampler, int block);
 
+// Resident serving loop (mpc_server mode 2): one persistent launch that
+// takes pricing work as the host publishes it.  The host writes entries into
+// a ring in mapped host memory and advances `tail`; every block claims tiles
+// of the oldest entry that still has some (a 64-bit compare-and-swap on the
+// slot's claim word, generation << 32 | next tile, so a claim can never land
+// on a slot's later request), runs them through the fused tile body of the
+// entry's sampler (xorshift, counter hash or Sobol; any family), and the
+// block that finishes a request's last tile writes its moments into mapped
+// host memory and then the request's generation into done[slot].  Blocks
+// leave when the host sets stop or pause, or after idle_ns without work;
+// every wait is a bounded poll.
+struct LoopEntry {
+  uint32_t slot, gen, n_tiles, pos;  // pos: absolute ring position (detects a reused ring entry)
+};
+struct LoopArgs {
+  const DevReq* slots;           // device [max_slots]: slot descriptors
+  unsigned long long* claim;     // device [max_slots]: gen << 32 | next tile
+  const LoopEntry* ring;         // mapped host [ring_cap]
+  const uint32_t* tail;          // mapped host: entries published
+  const uint32_t* control;       // mapped host: [0] stop, [1] pause
+  uint32_t* done;                // mapped host [max_slots]: generation finished last
+  uint32_t ring_cap, max_slots;
+  uint64_t idle_ns;
+};
+cudaError_t launch_serve_loop(const LoopArgs& a, const DeviceTables& tabs, int grid, cudaStream_t stream);
+int serve_loop_blocks_per_sm();
+
 // FP64 plain path: materialise samples, simulate into a payoff buffer, reduce.
 cudaError_t launch_plain_generate(const DevReq& q, double* d_buf, int sampler, const DeviceTables& tabs,
                                   cudaStream_t stream);

@@ -276,7 +276,7 @@ int validate(const mpc_request_t& r, std::string* msg) {
 }
 
 // The reference's own Merton: terminal, pseudorandom (mpc_merton.cu).
-static bool merton_stream_request(const mpc_request_t& r) {
+bool merton_stream_request(const mpc_request_t& r) {
   return r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.model == MPC_MODEL_MERTON &&
          r.sampling == MPC_SAMPLING_PSEUDORANDOM && r.method != MPC_METHOD_STEPWISE;
 }
@@ -1248,14 +1248,14 @@ static int run_lsm(mpc_context* ctx, const mpc_request_t& r, mpc_result_t* out) 
 }
 
 // ------------------------------------------------------------------ MLMC ---
-static uint64_t fine_steps(const mpc_request_t& r, uint32_t level) {
+uint64_t fine_steps(const mpc_request_t& r, uint32_t level) {
   uint64_t s = r.base_steps;
   for (uint32_t l = 0; l < level; ++l) s *= r.refinement_factor;
   return s;
 }
 
 // One MLMC level as a pricing unit family (simulate_asian_mlmc_level, cpu.rs:6641-6773).
-static void level_request(const mpc_request_t& r, uint64_t seed, uint32_t level, uint64_t paths, Prepared* p) {
+void level_request(const mpc_request_t& r, uint64_t seed, uint32_t level, uint64_t paths, Prepared* p) {
   *p = Prepared();
   DevReq& q = p->q;
   std::memset(&q, 0, sizeof(q));
@@ -1335,93 +1335,159 @@ static int run_level_list(mpc_context* ctx, std::vector<Prepared>& preps, std::v
 // target_stderr > 0, for a batch of requests: every pilot level of every
 // request runs in one fused launch, then every level of every replicate.
 // Level variances and the allocation are FP64 on the host.
+uint64_t mlmc_replicates(const mpc_request_t& r) {
+  const bool pseudo = r.sampling == MPC_SAMPLING_PSEUDORANDOM || r.sampling == MPC_SAMPLING_COUNTER_HASH;
+  return pseudo ? 1 : std::max<uint32_t>(r.scramble_replicates, 1);
+}
+
+static uint64_t level_cost(const mpc_request_t& r, uint32_t l) {
+  return fine_steps(r, l) + (l == 0 ? 0 : fine_steps(r, l) / r.refinement_factor);
+}
+
+// solve_arithmetic_asian_mlmc_tolerance_cpu's allocation (cpu.rs:3352-3423,
+// 3539-3565) from the pilot level variances: fills r.paths_per_level and the
+// solver fields of `out`.
+void mlmc_allocate(mpc_request_t& r, const double* pilot_var, mpc_result_t* out) {
+  const uint32_t L = r.levels;
+  const uint64_t reps = mlmc_replicates(r);
+  std::vector<double> var(L);
+  for (uint32_t l = 0; l < L; ++l) var[l] = std::max(pilot_var[l], 1.0e-18);
+  auto allocate = [&](double target_variance, bool by_budget, uint64_t budget, std::vector<uint64_t>& paths) {
+    double denom = 0.0;
+    for (uint32_t l = 0; l < L; ++l) denom += std::sqrt(var[l] * double(level_cost(r, l)));
+    uint64_t total = 0;
+    for (uint32_t l = 0; l < L; ++l) {
+      double w = std::sqrt(var[l] / double(level_cost(r, l)));
+      double raw = by_budget ? std::ceil(double(budget) * w / denom) : std::ceil(denom * w / target_variance);
+      paths[l] = std::max<uint64_t>(uint64_t(raw), 2);
+      total += paths[l] * level_cost(r, l);
+    }
+    return total;
+  };
+  auto est_se = [&](const std::vector<uint64_t>& paths) {
+    double v = 0.0;
+    for (uint32_t l = 0; l < L; ++l) v += var[l] / double(paths[l]);
+    return std::sqrt(v / double(reps));
+  };
+  std::vector<uint64_t> paths(L);
+  uint64_t updates = allocate(r.target_stderr * r.target_stderr * double(reps), false, 0, paths) * reps;
+  double est = est_se(paths);
+  if (updates < r.min_step_updates) {
+    uint64_t per = std::max<uint64_t>((r.min_step_updates + reps - 1) / reps, 1);
+    updates = allocate(0, true, per, paths) * reps;
+    est = est_se(paths);
+  }
+  bool hit = false;
+  if (updates > r.max_step_updates) {
+    hit = true;
+    uint64_t per = std::max<uint64_t>(r.max_step_updates / reps, 1);
+    updates = allocate(0, true, per, paths) * reps;
+    est = est_se(paths);
+  }
+  for (uint32_t l = 0; l < L; ++l) r.paths_per_level[l] = paths[l];
+  out->estimated_stderr = est;
+  out->target_met = (est <= r.target_stderr && updates <= r.max_step_updates) ? 1 : 0;
+  out->max_step_updates_hit = hit ? 1 : 0;
+}
+
+// The estimator of arithmetic_asian_call_price_mlmc_{single,replicated}_cpu
+// (cpu.rs:3612-3751) from the main-phase level results, ordered replicate by
+// replicate, level by level.
+void mlmc_finish(const mpc_request_t& r, const double* mm, double* mv, double device_ms, mpc_result_t* out) {
+  const uint32_t L = r.levels;
+  const uint64_t reps = mlmc_replicates(r);
+  std::vector<double> rep_price(reps);
+  double single_se = 0.0;
+  uint64_t total_paths = 0, total_updates = 0;
+  for (uint64_t rep = 0; rep < reps; ++rep) {
+    double price = 0.0, varc = 0.0;
+    for (uint32_t l = 0; l < L; ++l) {
+      const size_t e = rep * L + l;
+      mv[e] = std::max(mv[e], 0.0);
+      price += mm[e];
+      varc += mv[e] / double(r.paths_per_level[l]);
+      total_paths += r.paths_per_level[l];
+      total_updates += r.paths_per_level[l] * level_cost(r, l);
+    }
+    rep_price[rep] = price;
+    single_se = std::sqrt(varc);
+  }
+  double price = 0.0;
+  for (double p : rep_price) price += p;
+  price /= double(reps);
+  double se = single_se;
+  if (reps > 1) {
+    double sv = 0.0;
+    for (double p : rep_price) sv += (p - price) * (p - price);
+    sv /= double(reps - 1);
+    se = std::sqrt(sv / double(reps));
+  }
+  out->price = price;
+  out->stderr = se;
+  out->n_levels = L;
+  out->total_paths = total_paths;
+  out->total_step_updates = total_updates;
+  out->path_steps = total_updates;
+  for (uint32_t l = 0; l < L; ++l) {
+    double mean = 0.0;
+    for (uint64_t rep = 0; rep < reps; ++rep) mean += mm[rep * L + l];
+    mean /= double(reps);
+    double var = mv[l];
+    if (reps > 1) {
+      var = 0.0;
+      for (uint64_t rep = 0; rep < reps; ++rep) {
+        double d = mm[rep * L + l] - mean;
+        var += d * d;
+      }
+      var /= double(reps - 1);
+    }
+    out->level_mean[l] = mean;
+    out->level_variance[l] = var;
+    out->level_paths[l] = r.paths_per_level[l] * reps;
+    out->level_fine_steps[l] = fine_steps(r, l);
+  }
+  out->runtime_ms = device_ms;
+  out->status = MPC_OK;
+}
+
+// arithmetic_asian_call_price_mlmc_{single,replicated}_cpu (cpu.rs:3612-3751)
+// with solve_arithmetic_asian_mlmc_tolerance_cpu (cpu.rs:3352-3423) when
+// target_stderr > 0, for a batch of requests: every pilot level of every
+// request runs in one fused launch, then every level of every replicate.
+// Level variances and the allocation are FP64 on the host.
 int run_mlmc_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& reqs,
                    const std::vector<mpc_result_t*>& outs) {
-  struct Job {
-    mpc_request_t r;
-    uint64_t reps;
-  };
-  std::vector<Job> jobs;
-  for (const mpc_request_t* rq : reqs) {
-    Job j;
-    j.r = *rq;
-    const bool pseudo = j.r.sampling == MPC_SAMPLING_PSEUDORANDOM || j.r.sampling == MPC_SAMPLING_COUNTER_HASH;
-    j.reps = pseudo ? 1 : std::max<uint32_t>(j.r.scramble_replicates, 1);
-    jobs.push_back(j);
-  }
+  std::vector<mpc_request_t> jobs;
+  for (const mpc_request_t* rq : reqs) jobs.push_back(*rq);
   double device_ms = 0.0;
   uint64_t launches_before = kernel_launch_count();
-  auto cost = [](const mpc_request_t& r, uint32_t l) {
-    return fine_steps(r, l) + (l == 0 ? 0 : fine_steps(r, l) / r.refinement_factor);
-  };
   // pilot phase for the tolerance solver
   std::vector<Prepared> pilot;
   std::vector<size_t> pilot_first(jobs.size(), 0);
   for (size_t i = 0; i < jobs.size(); ++i) {
     pilot_first[i] = pilot.size();
-    if (jobs[i].r.target_stderr <= 0.0) continue;
-    for (uint32_t l = 0; l < jobs[i].r.levels; ++l) {
+    if (jobs[i].target_stderr <= 0.0) continue;
+    for (uint32_t l = 0; l < jobs[i].levels; ++l) {
       pilot.emplace_back();
-      level_request(jobs[i].r, jobs[i].r.seed, l, jobs[i].r.pilot_paths_per_level, &pilot.back());
+      level_request(jobs[i], jobs[i].seed, l, jobs[i].pilot_paths_per_level, &pilot.back());
     }
   }
   if (!pilot.empty()) {
     std::vector<double> pm, pv;
     int st = run_level_list(ctx, pilot, &pm, &pv, &device_ms);
     if (st != MPC_OK) return st;
-    for (size_t i = 0; i < jobs.size(); ++i) {
-      mpc_request_t& r = jobs[i].r;
-      if (r.target_stderr <= 0.0) continue;
-      const uint32_t L = r.levels;
-      const uint64_t reps = jobs[i].reps;
-      std::vector<double> var(L);
-      for (uint32_t l = 0; l < L; ++l) var[l] = std::max(pv[pilot_first[i] + l], 1.0e-18);
-      auto allocate = [&](double target_variance, bool by_budget, uint64_t budget, std::vector<uint64_t>& paths) {
-        double denom = 0.0;
-        for (uint32_t l = 0; l < L; ++l) denom += std::sqrt(var[l] * double(cost(r, l)));
-        uint64_t total = 0;
-        for (uint32_t l = 0; l < L; ++l) {
-          double w = std::sqrt(var[l] / double(cost(r, l)));
-          double raw = by_budget ? std::ceil(double(budget) * w / denom) : std::ceil(denom * w / target_variance);
-          paths[l] = std::max<uint64_t>(uint64_t(raw), 2);
-          total += paths[l] * cost(r, l);
-        }
-        return total;
-      };
-      auto est_se = [&](const std::vector<uint64_t>& paths) {
-        double v = 0.0;
-        for (uint32_t l = 0; l < L; ++l) v += var[l] / double(paths[l]);
-        return std::sqrt(v / double(reps));
-      };
-      std::vector<uint64_t> paths(L);
-      uint64_t updates = allocate(r.target_stderr * r.target_stderr * double(reps), false, 0, paths) * reps;
-      double est = est_se(paths);
-      if (updates < r.min_step_updates) {
-        uint64_t per = std::max<uint64_t>((r.min_step_updates + reps - 1) / reps, 1);
-        updates = allocate(0, true, per, paths) * reps;
-        est = est_se(paths);
-      }
-      bool hit = false;
-      if (updates > r.max_step_updates) {
-        hit = true;
-        uint64_t per = std::max<uint64_t>(r.max_step_updates / reps, 1);
-        updates = allocate(0, true, per, paths) * reps;
-        est = est_se(paths);
-      }
-      for (uint32_t l = 0; l < L; ++l) r.paths_per_level[l] = paths[l];
-      outs[i]->estimated_stderr = est;
-      outs[i]->target_met = (est <= r.target_stderr && updates <= r.max_step_updates) ? 1 : 0;
-      outs[i]->max_step_updates_hit = hit ? 1 : 0;
-    }
+    for (size_t i = 0; i < jobs.size(); ++i)
+      if (jobs[i].target_stderr > 0.0) mlmc_allocate(jobs[i], pv.data() + pilot_first[i], outs[i]);
   }
   // main phase: every level of every replicate of every request
   std::vector<Prepared> mains;
   std::vector<size_t> main_first(jobs.size(), 0);
   for (size_t i = 0; i < jobs.size(); ++i) {
-    const mpc_request_t& r = jobs[i].r;
+    const mpc_request_t& r = jobs[i];
+    const uint64_t reps = mlmc_replicates(r);
     main_first[i] = mains.size();
-    for (uint64_t rep = 0; rep < jobs[i].reps; ++rep) {
-      uint64_t seed = jobs[i].reps > 1 ? derive_chunk_seed(r.seed, rep) : r.seed;
+    for (uint64_t rep = 0; rep < reps; ++rep) {
+      uint64_t seed = reps > 1 ? derive_chunk_seed(r.seed, rep) : r.seed;
       for (uint32_t l = 0; l < r.levels; ++l) {
         mains.emplace_back();
         level_request(r, seed, l, r.paths_per_level[l], &mains.back());
@@ -1431,64 +1497,8 @@ int run_mlmc_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& re
   std::vector<double> mm, mv;
   int st = run_level_list(ctx, mains, &mm, &mv, &device_ms);
   if (st != MPC_OK) return st;
-  for (size_t i = 0; i < jobs.size(); ++i) {
-    const mpc_request_t& r = jobs[i].r;
-    mpc_result_t* out = outs[i];
-    const uint32_t L = r.levels;
-    const uint64_t reps = jobs[i].reps;
-    std::vector<double> rep_price(reps);
-    double single_se = 0.0;
-    uint64_t total_paths = 0, total_updates = 0;
-    for (uint64_t rep = 0; rep < reps; ++rep) {
-      double price = 0.0, varc = 0.0;
-      for (uint32_t l = 0; l < L; ++l) {
-        const size_t e = main_first[i] + rep * L + l;
-        mv[e] = std::max(mv[e], 0.0);
-        price += mm[e];
-        varc += mv[e] / double(r.paths_per_level[l]);
-        total_paths += r.paths_per_level[l];
-        total_updates += r.paths_per_level[l] * cost(r, l);
-      }
-      rep_price[rep] = price;
-      single_se = std::sqrt(varc);
-    }
-    double price = 0.0;
-    for (double p : rep_price) price += p;
-    price /= double(reps);
-    double se = single_se;
-    if (reps > 1) {
-      double sv = 0.0;
-      for (double p : rep_price) sv += (p - price) * (p - price);
-      sv /= double(reps - 1);
-      se = std::sqrt(sv / double(reps));
-    }
-    out->price = price;
-    out->stderr = se;
-    out->n_levels = L;
-    out->total_paths = total_paths;
-    out->total_step_updates = total_updates;
-    out->path_steps = total_updates;
-    for (uint32_t l = 0; l < L; ++l) {
-      double mean = 0.0;
-      for (uint64_t rep = 0; rep < reps; ++rep) mean += mm[main_first[i] + rep * L + l];
-      mean /= double(reps);
-      double var = mv[main_first[i] + l];
-      if (reps > 1) {
-        var = 0.0;
-        for (uint64_t rep = 0; rep < reps; ++rep) {
-          double d = mm[main_first[i] + rep * L + l] - mean;
-          var += d * d;
-        }
-        var /= double(reps - 1);
-      }
-      out->level_mean[l] = mean;
-      out->level_variance[l] = var;
-      out->level_paths[l] = r.paths_per_level[l] * reps;
-      out->level_fine_steps[l] = fine_steps(r, l);
-    }
-    out->runtime_ms = device_ms;
-    out->status = MPC_OK;
-  }
+  for (size_t i = 0; i < jobs.size(); ++i)
+    mlmc_finish(jobs[i], mm.data() + main_first[i], mv.data() + main_first[i], device_ms, outs[i]);
   ctx->last_ms = device_ms;
   ctx->last_launches = kernel_launch_count() - launches_before;
   return MPC_OK;

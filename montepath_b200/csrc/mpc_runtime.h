@@ -104,6 +104,9 @@ int scratch(mpc_context* ctx, const std::string& name, size_t bytes, void** out)
 int validate(const mpc_request_t& r, std::string* msg);
 int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* msg);
 uint64_t estimate_bytes(const mpc_request_t& r);
+// The reference's terminal pseudorandom Merton, priced by the stream replay
+// (its own launch sequence, not a fused tile family).
+bool merton_stream_request(const mpc_request_t& r);
 Shape choose_shape(mpc_context* ctx, const Prepared& p);
 void summarize_moments(const Prepared& p, const double* m, mpc_result_t* out);
 // Longstaff-Schwartz and MLMC requests of a batch, packed into shared launches.
@@ -111,6 +114,16 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
                   const std::vector<mpc_result_t*>& outs);
 int run_mlmc_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& reqs,
                    const std::vector<mpc_result_t*>& outs);
+// MLMC pieces shared by the batch runner and the serving loop: fine steps of
+// a level, one level as a fused request, replicates of a request, the
+// tolerance solver's allocation from pilot variances and the estimator from
+// the main-phase level results (means and population variances, replicate by
+// replicate, level by level).
+uint64_t fine_steps(const mpc_request_t& r, uint32_t level);
+void level_request(const mpc_request_t& r, uint64_t seed, uint32_t level, uint64_t paths, Prepared* p);
+uint64_t mlmc_replicates(const mpc_request_t& r);
+void mlmc_allocate(mpc_request_t& r, const double* pilot_var, mpc_result_t* out);
+void mlmc_finish(const mpc_request_t& r, const double* mean, double* var, double device_ms, mpc_result_t* out);
 // Host copies of the device lookup tables: Sobol nibble tables [256][8][16]
 // and xorshift64* jump-ahead nibble tables [64][16][16].
 void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump);

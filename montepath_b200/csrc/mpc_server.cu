@@ -16,12 +16,30 @@
 // Plain mode (mode 1): one request per launch sequence, FP64, strictly FIFO
 // -- the baseline continuous batching is compared against.
 //
-// All waiting is host-side on CUDA events and condition variables with
-// timeouts; no device code spins.
+// Device-loop mode (mode 2): a persistent kernel stays resident on the GPU
+// and takes work as it arrives (serve_loop_kernel, mpc_kernels.cu).  The
+// host thread admits requests under the HBM budget, writes each admitted
+// FP32-path request (or MLMC level) into a device slot, publishes it as an
+// entry of a ring in mapped host memory and advances the ring's tail; the
+// device blocks claim the tiles of the oldest published entries, so a
+// request that arrives while others run starts on the next free block, with
+// no launch.  The block that finishes a request's last tile writes its
+// moments into mapped host memory and then the slot's generation into
+// done[slot], which the host thread polls.  MLMC requests run their pilot
+// levels, then (after the host's allocation) their main levels, through the
+// loop.  Longstaff-Schwartz requests (cooperative launches with grid
+// barriers) and requests with per-request sampler tables are batched on the
+// host: the loop is paused (its blocks leave after their current tile), the
+// batch runs, and the loop is relaunched.  The loop's blocks also leave after
+// an idle period; the host relaunches it when work is published again.
+//
+// Host waiting is on CUDA events, condition variables and short sleeps with
+// timeouts; the device loop's waits are bounded polls.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -31,6 +49,7 @@
 #include <thread>
 #include <vector>
 
+#include "mpc_device.cuh"
 #include "mpc_launch.h"
 #include "mpc_runtime.h"
 
@@ -52,6 +71,23 @@ struct Ticket {
   uint32_t tiles_finished = 0;
   bool uploaded = false;
   double t_enqueue = 0, t_admit = 0, t_complete = 0;
+  // device-loop mode
+  int route = 0;                  // 1 device loop, 2 host batch
+  int phase = 0;                  // MLMC: 1 pilot levels, 2 main levels
+  uint32_t jobs_left = 0;         // loop jobs of the current phase not yet finished
+  mpc_request_t work{};           // MLMC: the request with the solver's allocation
+  std::vector<double> lvl_mean, lvl_var;
+  double t_batch = 0;             // host batch: when it joined the batch list
+};
+
+// One unit of device-loop work: a fused request, or one MLMC level (of one
+// replicate) of a request's current phase.
+struct LoopJob {
+  uint64_t ticket = 0;
+  uint32_t index = 0;  // MLMC: replicate * levels + level (the phase's order)
+  Prepared prep;
+  int slot = -1;
+  uint32_t gen = 0;
 };
 
 }  // namespace
@@ -86,6 +122,27 @@ struct mpc_server {
   uint32_t max_tiles_per_slot = 16384;
   uint32_t wave_tiles = 0;
   double busy_ms = 0.0;
+  // device-loop mode (mode 2)
+  cudaStream_t loop_stream = nullptr, upload_stream = nullptr;
+  LoopEntry* h_ring = nullptr;       // mapped host memory, device alias d_ring
+  LoopEntry* d_ring = nullptr;
+  uint32_t* h_ctl = nullptr;         // mapped: [0] tail, [1] stop, [2] pause
+  uint32_t* d_ctl = nullptr;
+  uint32_t* h_fin = nullptr;         // mapped [slots]: generation finished last per slot
+  uint32_t* d_fin = nullptr;
+  double* h_mom = nullptr;           // mapped [slots][MPC_MOMENTS]: finished moments
+  double* d_mom = nullptr;
+  unsigned long long* d_claim = nullptr;  // device [slots]
+  unsigned long long* h_claim = nullptr;  // pinned staging
+  uint32_t ring_cap = 0, ring_tail = 0, next_gen = 1;
+  std::vector<uint32_t> ring_gen;    // generation published at each ring entry
+  std::vector<LoopJob> pending;      // waiting for a slot
+  std::map<int, LoopJob> running;    // by slot
+  std::vector<int> free_slots;
+  std::vector<uint64_t> host_batch;  // tickets for the next host batch
+  int loop_grid = 0;
+  bool loop_launched = false;
+  uint64_t live_requests = 0;        // admitted, not finished (at most max_slots)
 };
 
 namespace {
@@ -105,6 +162,7 @@ double percentile(std::vector<double> v, double q) {
 }
 
 void complete(mpc_server* s, Ticket& t, int status) {
+  if (t.state == 1 && s->live_requests > 0) s->live_requests--;
   t.res.status = status;
   t.t_complete = now_ms(s);
   t.res.t_enqueue_ms = t.t_enqueue;
@@ -122,6 +180,15 @@ void complete(mpc_server* s, Ticket& t, int status) {
   } else {
     s->stats.rejected++;
   }
+}
+
+// Tile size of a slot request: the autotuner's shape, doubled until the work
+// list fits the slot's partials.
+void shape_for_slot(const mpc_server* s, Prepared* p) {
+  Shape sh = choose_shape(s->ctx, *p);
+  p->q.tile_units = sh.block * sh.ppt;
+  while ((p->q.n_units + p->q.tile_units - 1) / p->q.tile_units > s->max_tiles_per_slot) p->q.tile_units *= 2;
+  p->q.n_tiles = uint32_t((p->q.n_units + p->q.tile_units - 1) / p->q.tile_units);
 }
 
 bool fused_eligible(const Ticket& t) {
@@ -310,7 +377,14 @@ int run_wave(mpc_server* s, std::unique_lock<std::mutex>& lk) {
   return 1;
 }
 
+void serve_device_loop(mpc_server* s);
+
 void serve(mpc_server* s) {
+  cudaSetDevice(s->ctx->device);
+  if (s->opt.mode == 2) {
+    serve_device_loop(s);
+    return;
+  }
   std::unique_lock<std::mutex> lk(s->mu);
   while (!s->stop) {
     if (s->opt.mode == 1) {
@@ -367,6 +441,321 @@ void serve(mpc_server* s) {
   }
 }
 
+// ------------------------------------------------------ device-loop mode ---
+bool loop_sampler(const Prepared& p) {
+  return p.sampler == SMP_XORSHIFT || p.sampler == SMP_COUNTER || p.sampler == SMP_SOBOL;
+}
+
+// A finished loop job: level mean and population variance from its moments.
+void level_stats(const double* m, double* mean, double* var) {
+  const double n = m[0];
+  *mean = m[1] / n;
+  *var = (m[2] / n) - (*mean) * (*mean);
+}
+
+// Queues the loop jobs of an MLMC phase: pilot levels at pilot_paths_per_level
+// (phase 1) or every level of every replicate at the allocation (phase 2).
+void queue_mlmc_phase(mpc_server* s, Ticket& t, int phase) {
+  const mpc_request_t& r = t.work;
+  t.phase = phase;
+  const uint64_t reps = phase == 1 ? 1 : mlmc_replicates(r);
+  const uint32_t L = r.levels;
+  t.lvl_mean.assign(reps * L, 0.0);
+  t.lvl_var.assign(reps * L, 0.0);
+  t.jobs_left = uint32_t(reps * L);
+  for (uint64_t rep = 0; rep < reps; ++rep) {
+    const uint64_t seed = reps > 1 ? derive_chunk_seed(r.seed, rep) : r.seed;
+    for (uint32_t l = 0; l < L; ++l) {
+      LoopJob j;
+      j.ticket = t.id;
+      j.index = uint32_t(rep * L + l);
+      level_request(r, seed, l, phase == 1 ? r.pilot_paths_per_level : r.paths_per_level[l], &j.prep);
+      shape_for_slot(s, &j.prep);
+      s->pending.push_back(std::move(j));
+    }
+  }
+}
+
+// Admission under the HBM budget (FIFO); routes each admitted request to the
+// device loop or to the host batch.
+void admit_loop(mpc_server* s) {
+  while (!s->queue.empty()) {
+    Ticket& t = s->tickets[s->queue.front()];
+    if (t.state == 3) {
+      s->queue.pop_front();
+      continue;
+    }
+    uint64_t need = estimate_bytes(t.req);
+    if (need > s->opt.hbm_budget_bytes) {
+      s->queue.pop_front();
+      complete(s, t, MPC_E_OOM_BUDGET);
+      continue;
+    }
+    if (s->live_bytes + need > s->opt.hbm_budget_bytes) break;
+    if (s->live_requests >= s->slot_owner.size()) break;  // max_slots live requests
+    s->queue.pop_front();
+    t.state = 1;
+    t.bytes = need;
+    t.t_admit = now_ms(s);
+    s->live_bytes += need;
+    s->live_requests++;
+    s->stats.admitted++;
+    s->stats.peak_bytes = std::max(s->stats.peak_bytes, s->live_bytes);
+    const bool mlmc = t.req.workload == MPC_WORKLOAD_ASIAN_MLMC;
+    const int smp = mlmc ? (t.req.sampling == MPC_SAMPLING_PSEUDORANDOM ? SMP_XORSHIFT
+                            : t.req.sampling == MPC_SAMPLING_COUNTER_HASH ? SMP_COUNTER
+                            : t.req.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL ? SMP_SOBOL : -1)
+                         : t.prep.sampler;
+    if (mlmc && t.req.precision == MPC_PRECISION_FP32_PATH && smp >= 0) {
+      t.route = 1;
+      t.work = t.req;
+      queue_mlmc_phase(s, t, t.req.target_stderr > 0.0 ? 1 : 2);
+    } else if (!mlmc && fused_eligible(t) && loop_sampler(t.prep)) {
+      t.route = 1;
+      t.jobs_left = 1;
+      LoopJob j;
+      j.ticket = t.id;
+      j.prep = t.prep;
+      s->pending.push_back(std::move(j));
+    } else {
+      t.route = 2;
+      t.t_batch = now_ms(s);
+      s->host_batch.push_back(t.id);
+    }
+  }
+}
+
+// Writes pending jobs into free slots and publishes them on the ring.
+// Returns the number published.
+int publish(mpc_server* s) {
+  std::vector<int> slots;
+  size_t i = 0;
+  while (i < s->pending.size() && !s->free_slots.empty()) {
+    // the ring entry about to be reused must belong to a finished job
+    const uint32_t pos = s->ring_tail + uint32_t(slots.size());
+    const uint32_t old_gen = s->ring_gen[pos % s->ring_cap];
+    bool old_live = false;
+    for (const auto& kv : s->running)
+      if (kv.second.gen == old_gen) old_live = true;
+    if (old_live) break;
+    LoopJob j = std::move(s->pending[i]);
+    ++i;
+    const int slot = s->free_slots.back();
+    s->free_slots.pop_back();
+    j.slot = slot;
+    j.gen = s->next_gen++;
+    if (s->next_gen == 0) s->next_gen = 1;
+    DevReq q = j.prep.q;
+    // the loop kernel picks the tile body from the descriptor's sampling (MLMC
+    // level descriptors leave it unset)
+    q.sampling = j.prep.sampler == SMP_XORSHIFT  ? MPC_SAMPLING_PSEUDORANDOM
+                 : j.prep.sampler == SMP_COUNTER ? MPC_SAMPLING_COUNTER_HASH
+                                                 : MPC_SAMPLING_SCRAMBLED_SOBOL;
+    q.partials = s->d_partials + size_t(slot) * s->max_tiles_per_slot * MPC_MOMENTS;
+    q.moments = s->d_mom + size_t(slot) * MPC_MOMENTS;
+    q.tiles_done = s->d_done + slot;
+    q.per_unit = nullptr;
+    s->h_slots[slot] = q;
+    s->h_claim[slot] = (unsigned long long)j.gen << 32;
+    slots.push_back(slot);
+    s->running[slot] = std::move(j);
+  }
+  s->pending.erase(s->pending.begin(), s->pending.begin() + long(i));
+  if (slots.empty()) return 0;
+  cudaError_t e = cudaSuccess;
+  for (int slot : slots) {
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->d_slots + slot, s->h_slots + slot, sizeof(DevReq), cudaMemcpyHostToDevice,
+                          s->upload_stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->d_claim + slot, s->h_claim + slot, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                          s->upload_stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload_stream);  // slots visible before their entries
+  if (e != cudaSuccess) return -1;
+  for (int slot : slots) {
+    const LoopJob& j = s->running[slot];
+    const uint32_t pos = s->ring_tail++;
+    LoopEntry& en = s->h_ring[pos % s->ring_cap];
+    en.slot = uint32_t(slot);
+    en.gen = j.gen;
+    en.n_tiles = j.prep.q.n_tiles;
+    en.pos = pos;
+    s->ring_gen[pos % s->ring_cap] = j.gen;
+  }
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[0] = s->ring_tail;
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  return int(slots.size());
+}
+
+// (Re)launches the resident loop when it is not running and work is published.
+int ensure_loop(mpc_server* s) {
+  if (s->running.empty()) return MPC_OK;
+  if (s->loop_launched && cudaStreamQuery(s->loop_stream) == cudaErrorNotReady) return MPC_OK;
+  LoopArgs a{};
+  a.slots = s->d_slots;
+  a.claim = s->d_claim;
+  a.ring = s->d_ring;
+  a.tail = s->d_ctl;
+  a.control = s->d_ctl + 1;
+  a.done = s->d_fin;
+  a.ring_cap = s->ring_cap;
+  a.max_slots = uint32_t(s->slot_owner.size());
+  a.idle_ns = 20ull * 1000 * 1000;  // blocks leave after 20 ms without work
+  cudaError_t e = launch_serve_loop(a, s->ctx->tabs, s->loop_grid, s->loop_stream);
+  s->loop_launched = true;
+  s->stats.waves++;
+  return e == cudaSuccess ? MPC_OK : MPC_E_CUDA;
+}
+
+// Finished loop jobs: fused requests complete; MLMC phases advance.
+int reap(mpc_server* s) {
+  int n = 0;
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  for (auto it = s->running.begin(); it != s->running.end();) {
+    const int slot = it->first;
+    LoopJob& j = it->second;
+    if (reinterpret_cast<volatile uint32_t*>(s->h_fin)[slot] != j.gen) {
+      ++it;
+      continue;
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    double m[MPC_MOMENTS];
+    for (int k = 0; k < MPC_MOMENTS; ++k) m[k] = reinterpret_cast<volatile double*>(s->h_mom)[slot * MPC_MOMENTS + k];
+    Ticket& t = s->tickets[j.ticket];
+    if (t.req.workload == MPC_WORKLOAD_ASIAN_MLMC) {
+      level_stats(m, &t.lvl_mean[j.index], &t.lvl_var[j.index]);
+      if (--t.jobs_left == 0) {
+        if (t.phase == 1) {
+          mlmc_allocate(t.work, t.lvl_var.data(), &t.res);
+          queue_mlmc_phase(s, t, 2);
+        } else {
+          const double est = t.res.estimated_stderr;
+          const uint32_t met = t.res.target_met, hit = t.res.max_step_updates_hit;
+          mlmc_finish(t.work, t.lvl_mean.data(), t.lvl_var.data(), 0.0, &t.res);
+          t.res.estimated_stderr = est;
+          t.res.target_met = met;
+          t.res.max_step_updates_hit = hit;
+          complete(s, t, MPC_OK);
+        }
+      }
+    } else {
+      summarize_moments(j.prep, m, &t.res);
+      t.res.path_steps = j.prep.path_steps;
+      t.res.runtime_ms = 0.0;
+      complete(s, t, MPC_OK);
+    }
+    s->free_slots.push_back(slot);
+    it = s->running.erase(it);
+    ++n;
+  }
+  return n;
+}
+
+// Host batch: pauses the loop (its blocks leave after their current tile),
+// prices the batch through mpc_price_batch, clears the pause.
+int run_host_batch(mpc_server* s, std::unique_lock<std::mutex>& lk) {
+  std::vector<uint64_t> ids;
+  ids.swap(s->host_batch);
+  std::vector<mpc_request_t> lsm_req, other_req;
+  std::vector<uint64_t> lsm_ids, other_ids;
+  for (uint64_t id : ids) {
+    const Ticket& t = s->tickets[id];
+    if (t.req.workload == MPC_WORKLOAD_AMERICAN_PUT || t.req.workload == MPC_WORKLOAD_BERMUDAN_PUT) {
+      lsm_ids.push_back(id);
+      lsm_req.push_back(t.req);
+    } else {
+      other_ids.push_back(id);
+      other_req.push_back(t.req);
+    }
+  }
+  lk.unlock();
+  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[2] = 1;  // pause
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  cudaStreamSynchronize(s->loop_stream);
+  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[2] = 0;
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  std::vector<mpc_result_t> lsm_res(lsm_req.size()), other_res(other_req.size());
+  int st_lsm = MPC_OK, st_other = MPC_OK;
+  {
+    std::lock_guard<std::recursive_mutex> g(s->ctx->mu);
+    cudaSetDevice(s->ctx->device);
+    if (!lsm_req.empty()) {
+      st_lsm = mpc_price_batch(s->ctx, lsm_req.data(), lsm_req.size(), lsm_res.data());
+      s->busy_ms += s->ctx->last_ms;
+    }
+    if (!other_req.empty()) {
+      st_other = mpc_price_batch(s->ctx, other_req.data(), other_req.size(), other_res.data());
+      s->busy_ms += s->ctx->last_ms;
+    }
+  }
+  lk.lock();
+  for (size_t i = 0; i < lsm_ids.size(); ++i) {
+    Ticket& t = s->tickets[lsm_ids[i]];
+    t.res = lsm_res[i];
+    complete(s, t, lsm_res[i].status != MPC_OK ? lsm_res[i].status : st_lsm);
+  }
+  for (size_t i = 0; i < other_ids.size(); ++i) {
+    Ticket& t = s->tickets[other_ids[i]];
+    t.res = other_res[i];
+    complete(s, t, other_res[i].status != MPC_OK ? other_res[i].status : st_other);
+  }
+  s->loop_launched = false;  // the paused loop has left; relaunch on the next pass
+  return int(ids.size());
+}
+
+void fail_running(mpc_server* s, int status) {
+  for (auto& kv : s->running) {
+    Ticket& t = s->tickets[kv.second.ticket];
+    if (t.state != 2) complete(s, t, status);
+  }
+  for (LoopJob& j : s->pending) {
+    Ticket& t = s->tickets[j.ticket];
+    if (t.state != 2) complete(s, t, status);
+  }
+  s->running.clear();
+  s->pending.clear();
+  s->free_slots.clear();
+  for (int i = int(s->slot_owner.size()) - 1; i >= 0; --i) s->free_slots.push_back(i);
+}
+
+void serve_device_loop(mpc_server* s) {
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop) {
+    admit_loop(s);
+    int progress = 0;
+    const int pub = publish(s);
+    if (pub < 0 || ensure_loop(s) != MPC_OK) {
+      fail_running(s, MPC_E_CUDA);
+      progress = 1;
+    } else {
+      progress += pub;
+    }
+    const int finished = reap(s);
+    progress += finished;
+    // host batch: when its oldest request has waited 1 ms, it holds 16
+    // requests, or the loop has nothing to do
+    if (!s->host_batch.empty()) {
+      const Ticket& oldest = s->tickets[s->host_batch.front()];
+      if (now_ms(s) - oldest.t_batch > 1.0 || s->host_batch.size() >= 16 || (s->running.empty() && s->pending.empty())) {
+        progress += run_host_batch(s, lk);
+      }
+    }
+    if (finished || progress) s->cv_done.notify_all();
+    if (!progress) {
+      if (s->running.empty() && s->pending.empty() && s->host_batch.empty() && s->queue.empty())
+        s->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+      else
+        s->cv_work.wait_for(lk, std::chrono::microseconds(20));
+    }
+  }
+  lk.unlock();
+  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[1] = 1;  // stop
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  cudaStreamSynchronize(s->loop_stream);
+}
+
 }  // namespace
 
 extern "C" {
@@ -405,6 +794,40 @@ int mpc_server_start(mpc_context_t* ctx, const mpc_server_options_t* options, mp
     return e == cudaErrorMemoryAllocation ? MPC_E_OOM_BUDGET : MPC_E_CUDA;
   }
   std::memset(s->h_slots, 0, slots * sizeof(DevReq));
+  if (s->opt.mode == 2) {
+    s->ring_cap = uint32_t(4 * slots);
+    s->ring_gen.assign(s->ring_cap, 0);
+    for (int i = int(slots) - 1; i >= 0; --i) s->free_slots.push_back(i);
+    const unsigned mapped = cudaHostAllocMapped;
+    e = cudaStreamCreateWithFlags(&s->loop_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_ring, s->ring_cap * sizeof(LoopEntry), mapped);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_ctl, 64 * sizeof(uint32_t), mapped);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_fin, slots * sizeof(uint32_t), mapped);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_mom, slots * MPC_MOMENTS * sizeof(double), mapped);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_claim, slots * sizeof(unsigned long long), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_claim, slots * sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+      std::memset(s->h_ring, 0xFF, s->ring_cap * sizeof(LoopEntry));
+      std::memset(s->h_ctl, 0, 64 * sizeof(uint32_t));
+      std::memset(s->h_fin, 0, slots * sizeof(uint32_t));
+      std::memset(s->h_mom, 0, slots * MPC_MOMENTS * sizeof(double));
+      e = cudaHostGetDevicePointer((void**)&s->d_ring, s->h_ring, 0);
+    }
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->d_ctl, s->h_ctl, 0);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->d_fin, s->h_fin, 0);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->d_mom, s->h_mom, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_claim, 0, slots * sizeof(unsigned long long), s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    const int per_sm = serve_loop_blocks_per_sm();
+    s->loop_grid = ctx->sm_count * std::max(per_sm, 1);
+    if (e != cudaSuccess || per_sm < 1) {
+      ctx->last_error = std::string("device-loop server set-up: ") +
+                        (e != cudaSuccess ? cudaGetErrorString(e) : "the loop kernel cannot be resident");
+      mpc_server_stop(s);
+      return MPC_E_CUDA;
+    }
+  }
   s->worker = std::thread(serve, s);
   *out = s;
   return MPC_OK;
@@ -420,16 +843,11 @@ int mpc_submit(mpc_server_t* s, const mpc_request_t* req, uint64_t* ticket) {
   if (st == MPC_OK && req->workload != MPC_WORKLOAD_ASIAN_MLMC && req->workload != MPC_WORKLOAD_AMERICAN_PUT &&
       req->workload != MPC_WORKLOAD_BERMUDAN_PUT) {
     st = prepare(s->ctx, *req, &t.prep, &msg);
-    if (st == MPC_OK && !t.prep.plain && s->opt.mode == 0) {
-      if (!t.prep.halton_primes.empty() || !t.prep.lhs.empty() || t.prep.q.bridge)
-        t.prep.plain = true;  // samplers with per-request tables run as their own launch
-      else {
-        Shape sh = choose_shape(s->ctx, t.prep);
-        t.prep.q.tile_units = sh.block * sh.ppt;
-        while ((t.prep.q.n_units + t.prep.q.tile_units - 1) / t.prep.q.tile_units > s->max_tiles_per_slot)
-          t.prep.q.tile_units *= 2;
-        t.prep.q.n_tiles = uint32_t((t.prep.q.n_units + t.prep.q.tile_units - 1) / t.prep.q.tile_units);
-      }
+    if (st == MPC_OK && !t.prep.plain && s->opt.mode != 1) {
+      if (!t.prep.halton_primes.empty() || !t.prep.lhs.empty() || t.prep.q.bridge || merton_stream_request(*req))
+        t.prep.plain = true;  // per-request tables or the Merton stream replay: their own launches
+      else
+        shape_for_slot(s, &t.prep);
     }
   } else if (st == MPC_OK) {
     t.prep.lsm = req->workload != MPC_WORKLOAD_ASIAN_MLMC;
@@ -538,6 +956,18 @@ int mpc_server_stop(mpc_server_t* s) {
   if (s->h_slots) cudaFreeHost(s->h_slots);
   if (s->h_tiles) cudaFreeHost(s->h_tiles);
   if (s->h_moments) cudaFreeHost(s->h_moments);
+  if (s->loop_stream) {
+    if (s->h_ctl) reinterpret_cast<volatile uint32_t*>(s->h_ctl)[1] = 1;  // stop a loop still resident
+    cudaStreamSynchronize(s->loop_stream);
+    cudaStreamDestroy(s->loop_stream);
+  }
+  if (s->upload_stream) cudaStreamDestroy(s->upload_stream);
+  if (s->h_ring) cudaFreeHost(s->h_ring);
+  if (s->h_ctl) cudaFreeHost(s->h_ctl);
+  if (s->h_fin) cudaFreeHost(s->h_fin);
+  if (s->h_mom) cudaFreeHost(s->h_mom);
+  if (s->h_claim) cudaFreeHost(s->h_claim);
+  cudaFree(s->d_claim);
   if (s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return MPC_OK;

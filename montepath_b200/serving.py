@@ -13,7 +13,8 @@ from .backend import CudaBackend
 
 
 def replay(backend: CudaBackend, stream: Sequence[tuple[float, str, abi.Request]], plain: bool = False,
-           hbm_budget_bytes: int = 64 << 30, max_slots: int = 256, drain_timeout_s: float = 600.0) -> dict:
+           hbm_budget_bytes: int = 64 << 30, max_slots: int = 256, drain_timeout_s: float = 600.0,
+           mode: str | None = None) -> dict:
     """Runs the stream (arrival seconds, kind, request) through a fresh server.
 
     Arrivals are open-loop: submissions follow the schedule whether or not
@@ -23,7 +24,8 @@ def replay(backend: CudaBackend, stream: Sequence[tuple[float, str, abi.Request]
 
     tickets: list[tuple[int, str, abi.Request]] = []
     lock = threading.Lock()
-    with backend.server(hbm_budget_bytes=hbm_budget_bytes, max_slots=max_slots, plain=plain) as srv:
+    mode = mode or ("plain" if plain else "device_loop")
+    with backend.server(hbm_budget_bytes=hbm_budget_bytes, max_slots=max_slots, mode=mode) as srv:
         t0 = time.perf_counter()
         lag = 0.0
         for arrival, kind, req in stream:
@@ -59,7 +61,8 @@ def replay(backend: CudaBackend, stream: Sequence[tuple[float, str, abi.Request]
     path_steps = sum(r.path_steps for _, _, r in results)
     span_s = (max(r.t_complete_ms for _, _, r in results) - min(r.t_enqueue_ms for _, _, r in results)) / 1e3
     return {
-        "mode": "plain_fifo_fp64" if plain else "continuous_batching_fp32",
+        "mode": {"plain": "plain_fifo_fp64", "waves": "continuous_batching_fp32_waves",
+                 "device_loop": "continuous_batching_fp32_device_loop"}[mode],
         "requests": len(results),
         "offered_seconds": stream[-1][0] if stream else 0.0,
         "submit_lag_max_ms": lag * 1e3,
@@ -99,12 +102,15 @@ def main(argv: Sequence[str] | None = None) -> None:
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--budget-gb", type=float, default=64.0, help="HBM budget of the server")
     ap.add_argument("--plain", action="store_true", help="plain FIFO FP64 server, one request per launch")
+    ap.add_argument("--mode", default="", choices=["", "device_loop", "waves", "plain"],
+                    help="server mode (default device_loop; --plain selects plain)")
     ap.add_argument("--out", default="", help="also write the summary to this file")
     args = ap.parse_args(argv)
     stream = workloads.serving_stream(args.seed, rate=args.rate, duration_s=args.seconds,
                                       precision="fp64_plain" if args.plain else "fp32_path")
     with CudaBackend(0) as backend:
-        summary = replay(backend, stream, plain=args.plain, hbm_budget_bytes=int(args.budget_gb * (1 << 30)))
+        summary = replay(backend, stream, plain=args.plain, hbm_budget_bytes=int(args.budget_gb * (1 << 30)),
+                         mode=args.mode or None)
     summary.update({"rate": args.rate, "seed": args.seed, "budget_gb": args.budget_gb})
     line = json.dumps(summary)
     print(line)
