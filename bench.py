@@ -564,14 +564,19 @@ def leg_book(backend, contracts: int = 4096) -> dict:
 
 
 def leg_serving(backend) -> dict:
-    """Poisson serving stream at 2,000 requests/s: continuous batching on a
-    2 s slice of arrivals, plain FIFO FP64 on a 0.25 s slice."""
+    """Poisson serving stream at 2,000 requests/s, seed 42: the full 60 s
+    stream (about 120,000 requests) through the resident device loop; the
+    host-scheduled waves and the plain FIFO FP64 baseline at the same offered
+    load on the first 10 s and 2 s of the same stream (the FIFO baseline
+    cannot keep up with this load, so its queue only grows with the window)."""
 
     from montepath_b200 import serving, workloads
 
-    fused = serving.replay(backend, workloads.serving_stream(42, duration_s=2.0))
-    plain = serving.replay(backend, workloads.serving_stream(42, duration_s=0.25, precision="fp64_plain"), plain=True)
-    return {"continuous_batching": fused, "plain_fifo": plain}
+    loop = serving.replay(backend, workloads.serving_stream(42, duration_s=60.0), mode="device_loop")
+    waves = serving.replay(backend, workloads.serving_stream(42, duration_s=10.0), mode="waves")
+    plain = serving.replay(backend, workloads.serving_stream(42, duration_s=2.0, precision="fp64_plain"),
+                           mode="plain")
+    return {"device_loop_60s": loop, "waves_10s": waves, "plain_fifo_2s": plain, "rate_per_s": 2000.0}
 
 
 LEGS = {"gbm_european_20000x64": leg_gbm_european_small, "heston_merton_1048576x256": leg_heston_merton, "american_put_lsm_524288x50": leg_american_put_lsm, "book_4096": leg_book,

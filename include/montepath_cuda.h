@@ -301,7 +301,8 @@ typedef struct mpc_server_options {
   uint32_t wave_tiles;       /* tiles per scheduling wave (0 = auto) */
   uint32_t mode;             /* 0 = continuous batching in host-scheduled waves, 1 = plain FIFO, one request
                                 per launch in FP64, 2 = continuous batching in a resident device loop */
-  uint32_t _pad0;
+  uint32_t reserve_sms;      /* mode 2: SMs the loop leaves free for Longstaff-Schwartz and the other
+                                host-batched launches, which then run beside it (0 = 32) */
 } mpc_server_options_t;
 
 typedef struct mpc_server_stats {

@@ -275,7 +275,7 @@ class ServerOptions(Structure):
         ("max_slots", c_uint32),
         ("wave_tiles", c_uint32),
         ("mode", c_uint32),
-        ("_pad0", c_uint32),
+        ("reserve_sms", c_uint32),
     ]
 
 

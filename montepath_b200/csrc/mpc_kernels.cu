@@ -1217,11 +1217,6 @@ cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_t
 }
 
 // ---------------------------------------------------- resident serving loop ---
-__device__ __forceinline__ uint32_t ld_acquire_sys(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.acquire.sys.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
 __device__ __forceinline__ void st_release_sys(uint32_t* p, uint32_t v) {
   asm volatile("st.release.sys.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -1231,42 +1226,64 @@ __device__ __forceinline__ uint64_t loop_ns() {
   return t;
 }
 
+__device__ __forceinline__ LoopEntry loop_entry(const LoopArgs& a, uint32_t pos) {
+  const LoopEntry* ep = a.ring + (pos % a.ring_cap);
+  LoopEntry e;
+  asm volatile("ld.relaxed.gpu.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(e.slot), "=r"(e.gen), "=r"(e.n_tiles), "=r"(e.pos)
+               : "l"(ep)
+               : "memory");
+  return e;
+}
+
+// 0: the entry at `pos` has no tile left to claim (its claim word has moved
+// past its last tile or on to a later request of the slot, or the ring entry
+// was reused by a later request, which happens only after it finished);
+// otherwise its claim word.
+__device__ __forceinline__ unsigned long long loop_open(const LoopArgs& a, const LoopEntry& e, uint32_t pos) {
+  if (e.pos != pos || e.slot >= a.max_slots) return 0ull;
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(a.claim + e.slot) : "memory");
+  if ((uint32_t)(v >> 32) != e.gen || (uint32_t)v >= e.n_tiles) return 0ull;
+  return v;
+}
+
 // Thread 0: the next tile to run, or 0 when the block should leave (stop,
-// pause, or idle_ns without claimable work).  Every poll of host memory is
-// followed by a sleep that doubles up to 32 us while idle.
-__device__ __forceinline__ int loop_claim(const LoopArgs& a, uint32_t& cursor, uint32_t* slot, uint32_t* tile,
-                                          uint32_t* gen) {
+// pause, or idle_ns without claimable work).  The live entries are the ring
+// positions [cursor, tail) after the exhausted front ones are skipped; each
+// claim starts its scan at a position that rotates per block and per claim,
+// so concurrent requests share the blocks tile by tile (a large request does
+// not hold back the small ones behind it).  The doorbell, ring and claim
+// words are device memory read through L2; an idle poll is followed by a
+// sleep that doubles up to 4 us.
+__device__ __forceinline__ int loop_claim(const LoopArgs& a, uint32_t& cursor, uint32_t& turn, uint32_t* slot,
+                                          uint32_t* tile, uint32_t* gen) {
   uint64_t idle_since = 0;
-  uint32_t nap = 1000;
+  uint32_t nap = 500;
   for (;;) {
-    if (ld_acquire_sys(a.control) | ld_acquire_sys(a.control + 1)) return 0;
-    const uint32_t tail = ld_acquire_sys(a.tail);
-    for (uint32_t pos = cursor; pos != tail; ++pos) {
-      const LoopEntry* ep = a.ring + (pos % a.ring_cap);
-      LoopEntry e;
-      asm volatile("ld.volatile.global.v4.u32 {%0, %1, %2, %3}, [%4];"
-                   : "=r"(e.slot), "=r"(e.gen), "=r"(e.n_tiles), "=r"(e.pos)
-                   : "l"(ep));
-      bool exhausted = e.pos != pos || e.slot >= a.max_slots;  // overwritten entries were finished
-      if (!exhausted) {
-        unsigned long long* cw = a.claim + e.slot;
-        unsigned long long v = atomicAdd(cw, 0ull);
-        for (int tries = 0; tries < 64; ++tries) {  // bounded: contention leaves the entry for the next pass
-          if ((uint32_t)(v >> 32) != e.gen || (uint32_t)v >= e.n_tiles) {
-            exhausted = true;
-            break;
-          }
-          const unsigned long long w = atomicCAS(cw, v, v + 1ull);
-          if (w == v) {
-            *slot = e.slot;
-            *tile = (uint32_t)v;
-            *gen = e.gen;
-            return 1;
-          }
-          v = w;
+    uint32_t tail, stop, pause, pad;
+    asm volatile("ld.acquire.gpu.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(tail), "=r"(stop), "=r"(pause), "=r"(pad)
+                 : "l"(a.doorbell)
+                 : "memory");
+    if (stop | pause) return 0;
+    while (cursor != tail && loop_open(a, loop_entry(a, cursor), cursor) == 0ull) ++cursor;
+    const uint32_t live = tail - cursor;
+    const uint32_t first = live ? turn++ % live : 0u;
+    for (uint32_t k = 0; k < live; ++k) {
+      const uint32_t pos = cursor + (first + k) % live;
+      const LoopEntry e = loop_entry(a, pos);
+      unsigned long long v = loop_open(a, e, pos);
+      for (int tries = 0; v != 0ull && tries < 64; ++tries) {  // bounded: contention leaves the entry for the next pass
+        const unsigned long long w = atomicCAS(a.claim + e.slot, v, v + 1ull);
+        if (w == v) {
+          *slot = e.slot;
+          *tile = (uint32_t)v;
+          *gen = e.gen;
+          return 1;
         }
+        v = ((uint32_t)(w >> 32) == e.gen && (uint32_t)w < e.n_tiles) ? w : 0ull;
       }
-      if (exhausted && pos == cursor) cursor = pos + 1;
     }
     const uint64_t now = loop_ns();
     if (idle_since == 0)
@@ -1274,7 +1291,7 @@ __device__ __forceinline__ int loop_claim(const LoopArgs& a, uint32_t& cursor, u
     else if (now - idle_since > a.idle_ns)
       return 0;
     __nanosleep(nap);
-    nap = nap < 32000u ? 2u * nap : 32000u;
+    nap = nap < 4000u ? 2u * nap : 4000u;
   }
 }
 
@@ -1288,6 +1305,11 @@ __device__ __noinline__ void loop_tile(const DevReq& sq, const SrcCtx& ctx, uint
 
 __global__ void __launch_bounds__(kFusedBlock, 2) serve_loop_kernel(LoopArgs a, SrcCtx ctx) {
   extern __shared__ __align__(16) uint32_t sobol_window[];
+  {  // SMs kept free for the host-batched launches
+    uint32_t smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    if (smid < a.reserve_sms) return;
+  }
   {  // Sobol window rows, then the inverse-normal segments (staged once per launch)
     float4* seg = reinterpret_cast<float4*>(sobol_window + kSobolWindowWords);
     const float4* src = reinterpret_cast<const float4*>(ctx.sobol + MPC_ICDF_OFFSET);
@@ -1299,9 +1321,10 @@ __global__ void __launch_bounds__(kFusedBlock, 2) serve_loop_kernel(LoopArgs a, 
   __shared__ double red[kWarps][5];
   __shared__ uint32_t s_slot, s_tile, s_gen, s_go;
   __shared__ int s_last;
-  uint32_t cursor = 0;  // thread 0: ring entries before it have no tile left to claim
+  uint32_t cursor = 0;            // thread 0: ring entries before it have no tile left to claim
+  uint32_t turn = blockIdx.x;     // thread 0: rotation of the scan start
   for (;;) {
-    if (threadIdx.x == 0) s_go = loop_claim(a, cursor, &s_slot, &s_tile, &s_gen);
+    if (threadIdx.x == 0) s_go = loop_claim(a, cursor, turn, &s_slot, &s_tile, &s_gen);
     __syncthreads();
     if (!s_go) break;
     {  // the slot's descriptor, through L2 (the host rewrites slots between requests)

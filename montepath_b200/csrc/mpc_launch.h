@@ -23,8 +23,10 @@ cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_t
 int fused_max_blocks_per_sm(int family, int sampler, int block);
 
 // Resident serving loop (mpc_server mode 2): one persistent launch that
-// takes pricing work as the host publishes it.  The host writes entries into
-// a ring in mapped host memory and advances `tail`; every block claims tiles
+// takes pricing work as the host publishes it.  The host copies entries into
+// a ring in device memory and then advances `tail` (the doorbell, also in
+// device memory, copied after the entries on the same stream, so the loop's
+// polls stay in L2 and never cross PCIe); every block claims tiles
 // of the oldest entry that still has some (a 64-bit compare-and-swap on the
 // slot's claim word, generation << 32 | next tile, so a claim can never land
 // on a slot's later request), runs them through the fused tile body of the
@@ -39,12 +41,13 @@ struct LoopEntry {
 struct LoopArgs {
   const DevReq* slots;           // device [max_slots]: slot descriptors
   unsigned long long* claim;     // device [max_slots]: gen << 32 | next tile
-  const LoopEntry* ring;         // mapped host [ring_cap]
-  const uint32_t* tail;          // mapped host: entries published
-  const uint32_t* control;       // mapped host: [0] stop, [1] pause
+  const LoopEntry* ring;         // device [ring_cap]
+  const uint32_t* doorbell;      // device, 16-byte aligned: [0] tail (entries published), [1] stop, [2] pause
   uint32_t* done;                // mapped host [max_slots]: generation finished last
   uint32_t ring_cap, max_slots;
   uint64_t idle_ns;
+  uint32_t reserve_sms;          // blocks that start on an SM with %smid below this leave at once
+  uint32_t _pad;
 };
 cudaError_t launch_serve_loop(const LoopArgs& a, const DeviceTables& tabs, int grid, cudaStream_t stream);
 int serve_loop_blocks_per_sm();

@@ -1071,6 +1071,11 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     // capacity is one 512-thread block per SM)
     uint64_t want = (r.n_paths + 4 * kLsmThreads - 1) / (4 * kLsmThreads);
     want = std::min<uint64_t>(want, std::min<uint64_t>(cap, 2ull * uint64_t(ctx->sm_count)));
+    if (ctx->lsm_block_cap) {  // a caller that keeps only part of the device free for LSM launches
+      if (need > ctx->lsm_block_cap)
+        return fail(ctx, MPC_E_UNSUPPORTED, "LSM request needs more blocks than the SMs kept free for it");
+      want = std::min<uint64_t>(want, ctx->lsm_block_cap);
+    }
     j.blocks = uint32_t(std::max<uint64_t>(need, want));
     LsmArgs& a = j.args;
     std::memset(&a, 0, sizeof(a));
@@ -1096,7 +1101,8 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
   for (size_t first = 0; first < jobs.size(); ++first) {
     if (done[first]) continue;
     const int fp64 = jobs[first].fp64, sampler = jobs[first].sampler;
-    const uint32_t cap = lsm_capacity(fp64, sampler);
+    const uint32_t cap = ctx->lsm_block_cap ? std::min(lsm_capacity(fp64, sampler), ctx->lsm_block_cap)
+                                            : lsm_capacity(fp64, sampler);
     std::vector<size_t> group;
     uint32_t blocks = 0;
     for (size_t i = first; i < jobs.size(); ++i) {

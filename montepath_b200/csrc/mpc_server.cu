@@ -124,10 +124,10 @@ struct mpc_server {
   double busy_ms = 0.0;
   // device-loop mode (mode 2)
   cudaStream_t loop_stream = nullptr, upload_stream = nullptr;
-  LoopEntry* h_ring = nullptr;       // mapped host memory, device alias d_ring
-  LoopEntry* d_ring = nullptr;
-  uint32_t* h_ctl = nullptr;         // mapped: [0] tail, [1] stop, [2] pause
-  uint32_t* d_ctl = nullptr;
+  LoopEntry* h_ring = nullptr;       // pinned staging of new ring entries
+  LoopEntry* d_ring = nullptr;       // device ring
+  uint32_t* h_ctl = nullptr;         // pinned staging of the doorbell: [0] tail, [1] stop, [2] pause
+  uint32_t* d_ctl = nullptr;         // device doorbell
   uint32_t* h_fin = nullptr;         // mapped [slots]: generation finished last per slot
   uint32_t* d_fin = nullptr;
   double* h_mom = nullptr;           // mapped [slots][MPC_MOMENTS]: finished moments
@@ -571,8 +571,7 @@ int publish(mpc_server* s) {
       e = cudaMemcpyAsync(s->d_claim + slot, s->h_claim + slot, sizeof(unsigned long long), cudaMemcpyHostToDevice,
                           s->upload_stream);
   }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload_stream);  // slots visible before their entries
-  if (e != cudaSuccess) return -1;
+  // entries after their slots, the doorbell after the entries: one stream, in order
   for (int slot : slots) {
     const LoopJob& j = s->running[slot];
     const uint32_t pos = s->ring_tail++;
@@ -582,11 +581,23 @@ int publish(mpc_server* s) {
     en.n_tiles = j.prep.q.n_tiles;
     en.pos = pos;
     s->ring_gen[pos % s->ring_cap] = j.gen;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(s->d_ring + pos % s->ring_cap, &en, sizeof(LoopEntry), cudaMemcpyHostToDevice,
+                          s->upload_stream);
   }
-  std::atomic_thread_fence(std::memory_order_seq_cst);
-  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[0] = s->ring_tail;
-  std::atomic_thread_fence(std::memory_order_seq_cst);
+  s->h_ctl[0] = s->ring_tail;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_ctl, s->h_ctl, sizeof(uint32_t), cudaMemcpyHostToDevice, s->upload_stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->upload_stream);  // staging reusable
+  if (e != cudaSuccess) return -1;
   return int(slots.size());
+}
+
+// Writes doorbell word `index` (1 stop, 2 pause) on the device.
+void set_control(mpc_server* s, int index, uint32_t value) {
+  s->h_ctl[index] = value;
+  cudaMemcpyAsync(s->d_ctl + index, s->h_ctl + index, sizeof(uint32_t), cudaMemcpyHostToDevice, s->upload_stream);
+  cudaStreamSynchronize(s->upload_stream);
 }
 
 // (Re)launches the resident loop when it is not running and work is published.
@@ -597,12 +608,12 @@ int ensure_loop(mpc_server* s) {
   a.slots = s->d_slots;
   a.claim = s->d_claim;
   a.ring = s->d_ring;
-  a.tail = s->d_ctl;
-  a.control = s->d_ctl + 1;
+  a.doorbell = s->d_ctl;
   a.done = s->d_fin;
   a.ring_cap = s->ring_cap;
   a.max_slots = uint32_t(s->slot_owner.size());
   a.idle_ns = 20ull * 1000 * 1000;  // blocks leave after 20 ms without work
+  a.reserve_sms = s->opt.reserve_sms;
   cudaError_t e = launch_serve_loop(a, s->ctx->tabs, s->loop_grid, s->loop_stream);
   s->loop_launched = true;
   s->stats.waves++;
@@ -653,55 +664,62 @@ int reap(mpc_server* s) {
   return n;
 }
 
-// Host batch: pauses the loop (its blocks leave after their current tile),
-// prices the batch through mpc_price_batch, clears the pause.
+// Host batch, beside the running loop: Longstaff-Schwartz requests run one
+// cooperative launch each on the SMs the loop keeps free (at most
+// reserve_sms blocks per launch); the other requests (per-request sampler
+// tables, FP64 plain, the Merton stream replay) are ordinary launches.  An
+// LSM request that needs more blocks than the free SMs hold pauses the loop
+// (its blocks leave after their current tile) for its own launch.
 int run_host_batch(mpc_server* s, std::unique_lock<std::mutex>& lk) {
   std::vector<uint64_t> ids;
   ids.swap(s->host_batch);
-  std::vector<mpc_request_t> lsm_req, other_req;
-  std::vector<uint64_t> lsm_ids, other_ids;
+  std::vector<std::pair<uint64_t, mpc_request_t>> lsm_fit, lsm_big, other;
+  const uint64_t per_block_max = uint64_t(kLsmThreads) * kLsmPathsPerThreadMax;
   for (uint64_t id : ids) {
     const Ticket& t = s->tickets[id];
     if (t.req.workload == MPC_WORKLOAD_AMERICAN_PUT || t.req.workload == MPC_WORKLOAD_BERMUDAN_PUT) {
-      lsm_ids.push_back(id);
-      lsm_req.push_back(t.req);
+      const uint64_t need = (t.req.n_paths + per_block_max - 1) / per_block_max;
+      (need <= s->opt.reserve_sms ? lsm_fit : lsm_big).push_back({id, t.req});
     } else {
-      other_ids.push_back(id);
-      other_req.push_back(t.req);
+      other.push_back({id, t.req});
     }
   }
   lk.unlock();
-  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[2] = 1;  // pause
-  std::atomic_thread_fence(std::memory_order_seq_cst);
-  cudaStreamSynchronize(s->loop_stream);
-  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[2] = 0;
-  std::atomic_thread_fence(std::memory_order_seq_cst);
-  std::vector<mpc_result_t> lsm_res(lsm_req.size()), other_res(other_req.size());
-  int st_lsm = MPC_OK, st_other = MPC_OK;
-  {
+  std::vector<std::pair<uint64_t, mpc_result_t>> done;
+  auto price = [&](const std::vector<std::pair<uint64_t, mpc_request_t>>& list, bool one_by_one, uint32_t cap) {
+    if (list.empty()) return;
     std::lock_guard<std::recursive_mutex> g(s->ctx->mu);
     cudaSetDevice(s->ctx->device);
-    if (!lsm_req.empty()) {
-      st_lsm = mpc_price_batch(s->ctx, lsm_req.data(), lsm_req.size(), lsm_res.data());
+    s->ctx->lsm_block_cap = cap;
+    const size_t step = one_by_one ? 1 : list.size();
+    for (size_t i = 0; i < list.size(); i += step) {
+      std::vector<mpc_request_t> reqs;
+      for (size_t k = i; k < std::min(list.size(), i + step); ++k) reqs.push_back(list[k].second);
+      std::vector<mpc_result_t> res(reqs.size());
+      int st = mpc_price_batch(s->ctx, reqs.data(), reqs.size(), res.data());
       s->busy_ms += s->ctx->last_ms;
+      for (size_t k = 0; k < reqs.size(); ++k) {
+        if (res[k].status == MPC_OK && st != MPC_OK) res[k].status = st;
+        done.push_back({list[i + k].first, res[k]});
+      }
     }
-    if (!other_req.empty()) {
-      st_other = mpc_price_batch(s->ctx, other_req.data(), other_req.size(), other_res.data());
-      s->busy_ms += s->ctx->last_ms;
-    }
+    s->ctx->lsm_block_cap = 0;
+  };
+  price(other, false, 0);
+  price(lsm_fit, true, s->opt.reserve_sms);
+  if (!lsm_big.empty()) {
+    set_control(s, 2, 1);  // pause: the loop's blocks leave after their current tile
+    cudaStreamSynchronize(s->loop_stream);
+    set_control(s, 2, 0);
+    price(lsm_big, false, 0);
   }
   lk.lock();
-  for (size_t i = 0; i < lsm_ids.size(); ++i) {
-    Ticket& t = s->tickets[lsm_ids[i]];
-    t.res = lsm_res[i];
-    complete(s, t, lsm_res[i].status != MPC_OK ? lsm_res[i].status : st_lsm);
+  for (auto& d : done) {
+    Ticket& t = s->tickets[d.first];
+    t.res = d.second;
+    complete(s, t, d.second.status);
   }
-  for (size_t i = 0; i < other_ids.size(); ++i) {
-    Ticket& t = s->tickets[other_ids[i]];
-    t.res = other_res[i];
-    complete(s, t, other_res[i].status != MPC_OK ? other_res[i].status : st_other);
-  }
-  s->loop_launched = false;  // the paused loop has left; relaunch on the next pass
+  if (!lsm_big.empty()) s->loop_launched = false;  // the paused loop has left; relaunch on the next pass
   return int(ids.size());
 }
 
@@ -734,25 +752,23 @@ void serve_device_loop(mpc_server* s) {
     }
     const int finished = reap(s);
     progress += finished;
-    // host batch: when its oldest request has waited 1 ms, it holds 16
-    // requests, or the loop has nothing to do
-    if (!s->host_batch.empty()) {
-      const Ticket& oldest = s->tickets[s->host_batch.front()];
-      if (now_ms(s) - oldest.t_batch > 1.0 || s->host_batch.size() >= 16 || (s->running.empty() && s->pending.empty())) {
-        progress += run_host_batch(s, lk);
-      }
-    }
+    // host-batched requests run beside the loop as soon as they are admitted
+    if (!s->host_batch.empty()) progress += run_host_batch(s, lk);
     if (finished || progress) s->cv_done.notify_all();
-    if (!progress) {
-      if (s->running.empty() && s->pending.empty() && s->host_batch.empty() && s->queue.empty())
-        s->cv_work.wait_for(lk, std::chrono::milliseconds(20));
-      else
-        s->cv_work.wait_for(lk, std::chrono::microseconds(20));
+    if (progress || !s->running.empty()) {
+      // poll the finished flags while work runs; let submitters and waiters
+      // take the lock between passes
+      lk.unlock();
+      std::this_thread::yield();
+      lk.lock();
+    } else if (s->running.empty() && s->pending.empty() && s->host_batch.empty() && s->queue.empty()) {
+      s->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+    } else {
+      s->cv_work.wait_for(lk, std::chrono::microseconds(20));
     }
   }
   lk.unlock();
-  reinterpret_cast<volatile uint32_t*>(s->h_ctl)[1] = 1;  // stop
-  std::atomic_thread_fence(std::memory_order_seq_cst);
+  set_control(s, 1, 1);  // stop
   cudaStreamSynchronize(s->loop_stream);
 }
 
@@ -795,14 +811,18 @@ int mpc_server_start(mpc_context_t* ctx, const mpc_server_options_t* options, mp
   }
   std::memset(s->h_slots, 0, slots * sizeof(DevReq));
   if (s->opt.mode == 2) {
+    if (s->opt.reserve_sms == 0) s->opt.reserve_sms = 32;
+    s->opt.reserve_sms = std::min<uint32_t>(s->opt.reserve_sms, uint32_t(ctx->sm_count) - 1);
     s->ring_cap = uint32_t(4 * slots);
     s->ring_gen.assign(s->ring_cap, 0);
     for (int i = int(slots) - 1; i >= 0; --i) s->free_slots.push_back(i);
     const unsigned mapped = cudaHostAllocMapped;
     e = cudaStreamCreateWithFlags(&s->loop_stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_ring, s->ring_cap * sizeof(LoopEntry), mapped);
-    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_ctl, 64 * sizeof(uint32_t), mapped);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_ring, s->ring_cap * sizeof(LoopEntry), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(&s->h_ctl, 64 * sizeof(uint32_t), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_ring, s->ring_cap * sizeof(LoopEntry));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_ctl, 64 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaHostAlloc(&s->h_fin, slots * sizeof(uint32_t), mapped);
     if (e == cudaSuccess) e = cudaHostAlloc(&s->h_mom, slots * MPC_MOMENTS * sizeof(double), mapped);
     if (e == cudaSuccess) e = cudaHostAlloc(&s->h_claim, slots * sizeof(unsigned long long), cudaHostAllocDefault);
@@ -812,9 +832,9 @@ int mpc_server_start(mpc_context_t* ctx, const mpc_server_options_t* options, mp
       std::memset(s->h_ctl, 0, 64 * sizeof(uint32_t));
       std::memset(s->h_fin, 0, slots * sizeof(uint32_t));
       std::memset(s->h_mom, 0, slots * MPC_MOMENTS * sizeof(double));
-      e = cudaHostGetDevicePointer((void**)&s->d_ring, s->h_ring, 0);
+      e = cudaMemcpyAsync(s->d_ring, s->h_ring, s->ring_cap * sizeof(LoopEntry), cudaMemcpyHostToDevice, s->stream);
     }
-    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->d_ctl, s->h_ctl, 0);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->d_ctl, 0, 64 * sizeof(uint32_t), s->stream);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->d_fin, s->h_fin, 0);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&s->d_mom, s->h_mom, 0);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->d_claim, 0, slots * sizeof(unsigned long long), s->stream);
@@ -957,10 +977,12 @@ int mpc_server_stop(mpc_server_t* s) {
   if (s->h_tiles) cudaFreeHost(s->h_tiles);
   if (s->h_moments) cudaFreeHost(s->h_moments);
   if (s->loop_stream) {
-    if (s->h_ctl) reinterpret_cast<volatile uint32_t*>(s->h_ctl)[1] = 1;  // stop a loop still resident
+    if (s->h_ctl && s->d_ctl && s->upload_stream) set_control(s, 1, 1);  // stop a loop still resident
     cudaStreamSynchronize(s->loop_stream);
     cudaStreamDestroy(s->loop_stream);
   }
+  cudaFree(s->d_ring);
+  cudaFree(s->d_ctl);
   if (s->upload_stream) cudaStreamDestroy(s->upload_stream);
   if (s->h_ring) cudaFreeHost(s->h_ring);
   if (s->h_ctl) cudaFreeHost(s->h_ctl);
