@@ -327,6 +327,11 @@ def run_ours(args) -> None:
         for r in fused + plain:
             r.n_paths = args.paths
     path_steps = sum(r.n_paths * r.n_steps for r in fused)
+    # compile step (mpc_prepare): the autotuner measures each request kind's block size
+    shapes = {}
+    for name, r in zip(("heston", "merton"), fused):
+        art = backend.prepare(r)
+        shapes[name] = {"block": art.block_size, "paths_per_thread": art.paths_per_thread, "tiles": art.tiles}
 
     for _ in range(max(args.warmup, 3)):
         backend.price_batch(fused)
@@ -410,6 +415,7 @@ def run_ours(args) -> None:
                 "precision": "fp32_path",
                 "parallelism": f"replicas x{world}",
                 "l2": "flushed between steps (256 MiB write); samples never touch HBM",
+                "launch_shapes": shapes,
             },
             "e2e": {"value": e2e_value, "unit": "path-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
@@ -536,6 +542,10 @@ def leg_book(backend, contracts: int = 4096) -> dict:
 
     book = workloads.book(42)[:contracts]
     total = workloads.book_path_steps(book)
+    blocks = {}
+    for r in book:  # the autotuner measures each contract kind once (family, sampler, step bucket)
+        b = backend.prepare(r).block_size
+        blocks[b] = blocks.get(b, 0) + 1
     backend.price_batch(book)
     res, ms = _timed(backend, lambda: backend.price_batch(book))
     _, launches = backend.last_timing()
@@ -559,6 +569,7 @@ def leg_book(backend, contracts: int = 4096) -> dict:
         "plain_fp64_sampled": {"contracts_timed": len(sample), "ms_sample": plain_ms, "path_steps_per_sec": plain_rate,
                                "estimated_ms_full_book": total / plain_rate * 1e3},
         "speedup_batched_vs_plain": (total / (ms * 1e-3)) / plain_rate,
+        "contracts_by_block_size": {str(k): v for k, v in sorted(blocks.items())},
         "price_checksum": sum(x.price for x in res),
     }
 

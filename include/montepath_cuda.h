@@ -142,11 +142,12 @@ typedef struct mpc_request {
   uint64_t paths_per_level[MPC_MAX_LEVELS];
   double target_stderr;
   uint64_t pilot_paths_per_level, min_step_updates, max_step_updates;
-  /* Launch hints (0 = let the autotuner choose).  block_size: 0 or 256 (the
-   * kernels run 256-thread blocks; other values return MPC_E_UNSUPPORTED);
-   * paths_per_thread: 1..64 units per thread per tile, i.e. tiles of
-   * 256 * paths_per_thread paths (the tile partition fixes the order of the
-   * sums, so a hint changes results at rounding level only). */
+  /* Launch hints (0 = let the autotuner choose).  block_size: 0, 128, 256 or
+   * 512 threads per block of the fused launch (other values return
+   * MPC_E_UNSUPPORTED); paths_per_thread: 1..64 units per thread per tile,
+   * i.e. tiles of block_size * paths_per_thread paths (the tile partition and
+   * the block fix the order of the sums, so a hint changes results at
+   * rounding level only). */
   uint32_t block_size, paths_per_thread;
   uint64_t _reserved[4];
 } mpc_request_t;
@@ -269,8 +270,9 @@ typedef struct mpc_options {
   int32_t deterministic;    /* reductions always run in fixed tile order, so results
                                are deterministic for 0 and 1 alike */
   uint64_t hbm_budget_bytes; /* 0 = 64 GiB */
-  uint32_t default_block_size; /* 0 or 256 (the kernels run 256-thread blocks;
-                                  other values: MPC_E_UNSUPPORTED) */
+  uint32_t default_block_size; /* 0 (autotuner), 128, 256 or 512: block size of fused
+                                  launches when a request gives no hint and mpc_prepare
+                                  has not tuned its kind (other values: MPC_E_UNSUPPORTED) */
   uint32_t _pad0;
 } mpc_options_t;
 

@@ -1007,6 +1007,10 @@ __device__ __forceinline__ void fused_unit_any(const DevReq& q, const SrcCtx& ct
 // ----------------------------------------------------- block reduction ----
 constexpr int kFusedBlock = 256;
 constexpr int kWarps = kFusedBlock / 32;
+// The fused pricing kernel runs 128-, 256- or 512-thread blocks (the
+// autotuner's choice); its launch bounds are written for 512 threads.
+constexpr int kMaxFusedBlock = 512;
+constexpr int kMaxWarps = kMaxFusedBlock / 32;
 
 // Reduces v[0..4] over the block in a fixed order; result valid in thread 0.
 // The leading barrier keeps a previous call's reader of `red` safe, so calls
@@ -1063,6 +1067,9 @@ __device__ void finalize_request(DevReq& q, double (*red)[5]) {
 constexpr int fused_min_blocks(int fam, int smp) {
   return fam < 0 ? 2 : ((fam == FAM_GBM_STEP || fam == FAM_GBM_TERMINAL) && smp == SMP_COUNTER ? 6 : 4);
 }
+// The same resident threads per SM (hence the same register budget per
+// thread) expressed in 512-thread blocks, for the launch bounds.
+constexpr int fused_min_blocks512(int fam, int smp) { return fused_min_blocks(fam, smp) * kFusedBlock / kMaxFusedBlock; }
 
 // One tile of request `sq`: its units through the model, the block's moment
 // sums written as the tile's partial, and *s_last (shared) set when this was
@@ -1111,7 +1118,7 @@ __device__ __forceinline__ void fused_tile(const DevReq& sq, const SrcCtx& ctx, 
 
 // FAM >= 0: every request in the list has that family; FAM < 0: switch per tile.
 template <int FAM, int SMP>
-__global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused_kernel(const DevReq* __restrict__ reqs,
+__global__ void __launch_bounds__(kMaxFusedBlock, fused_min_blocks512(FAM, SMP)) fused_kernel(const DevReq* __restrict__ reqs,
                                                             const Tile* __restrict__ tiles, uint32_t n_tiles,
                                                             uint32_t* __restrict__ counter, SrcCtx ctx) {
   extern __shared__ __align__(16) uint32_t sobol_window[];
@@ -1127,7 +1134,7 @@ __global__ void __launch_bounds__(kFusedBlock, fused_min_blocks(FAM, SMP)) fused
     ctx.icdf = nullptr;
   }
   __shared__ DevReq sq;
-  __shared__ double red[kWarps][5];
+  __shared__ double red[kMaxWarps][5];
   __shared__ uint32_t s_tile;
   __shared__ int s_last;
   for (;;) {
@@ -1199,7 +1206,7 @@ cudaError_t launch_fused(const DevReq* d_reqs, const Tile* d_tiles, uint32_t n_t
                          int family, int sampler, const DeviceTables& tabs, int grid, int block,
                          cudaStream_t stream) {
   SrcCtx ctx{tabs.sobol, tabs.jump, nullptr};
-  if (block != kFusedBlock) return cudaErrorInvalidValue;
+  if (block != 128 && block != 256 && block != kMaxFusedBlock) return cudaErrorInvalidValue;
   switch (sampler) {
     case SMP_XORSHIFT:
       return launch_fused_s<SMP_XORSHIFT>(family, d_reqs, d_tiles, n_tiles, d_tile_counter, ctx, grid, block, stream);

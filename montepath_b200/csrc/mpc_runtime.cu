@@ -162,8 +162,8 @@ int validate(const mpc_request_t& r, std::string* msg) {
     return invalid(msg, "unknown precision");
   if (r.method < 0 || r.method > MPC_METHOD_STEPWISE) return invalid(msg, "unknown method");
   // launch hints: the kernels are built for 256-thread blocks
-  if (r.block_size != 0 && r.block_size != 256)
-    return unsupported(msg, "block_size: the kernels run 256-thread blocks (0 or 256)");
+  if (r.block_size != 0 && r.block_size != 128 && r.block_size != 256 && r.block_size != 512)
+    return unsupported(msg, "block_size: the fused kernels run 128-, 256- or 512-thread blocks (0 = autotuner)");
   if (r.paths_per_thread > 64) return invalid(msg, "paths_per_thread must be 0 (autotuner) to 64");
   for (double x : {r.s0, r.k, r.r, r.sigma, r.t})
     if (!finite(x)) return invalid(msg, "market parameters must be finite");
@@ -438,6 +438,7 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
   std::memset(&q, 0, sizeof(q));
   p->sampler = sampler_of(r.sampling);
   p->ppt_hint = r.paths_per_thread;
+  p->block_hint = r.block_size;
   p->plain = r.precision == MPC_PRECISION_FP64_PLAIN;
   p->lsm = is_lsm(r.workload);
   p->mlmc = r.workload == MPC_WORKLOAD_ASIAN_MLMC;
@@ -562,21 +563,33 @@ int prepare(mpc_context* ctx, const mpc_request_t& r, Prepared* p, std::string* 
   return MPC_OK;
 }
 
+uint64_t block_key(const Prepared& p) {
+  const int steps_bucket = 32 - __builtin_clz(std::max<uint32_t>(p.q.n_steps, 1));
+  return (uint64_t(uint32_t(p.family)) << 48) | (uint64_t(p.sampler) << 40) | uint64_t(steps_bucket);
+}
+
+// Autotuner: the block size is the request's hint, else the one mpc_prepare
+// measured for the request's kind (family, sampler, step bucket), else the
+// context default; paths-per-thread is the hint, else picked so that a
+// request spreads over at least four waves of resident blocks.  Cached per
+// context.
 Shape choose_shape(mpc_context* ctx, const Prepared& p) {
+  std::lock_guard<std::mutex> lock(ctx->tuner.mu);
+  uint32_t block = p.block_hint;
+  if (!block) {
+    auto bt = ctx->tuner.block.find(block_key(p));
+    block = bt != ctx->tuner.block.end() ? bt->second : ctx->tuner.default_block;
+  }
   if (p.ppt_hint) {  // the caller's paths-per-thread hint, not cached
     Shape s;
-    s.block = 256;
+    s.block = block;
     s.ppt = p.ppt_hint;
     return s;
   }
-  // Autotuner: paths-per-thread per (family, sampler, step bucket, size
-  // bucket), picked so that a request spreads over at least four waves of
-  // resident blocks; cached per context.
   const int steps_bucket = 32 - __builtin_clz(std::max<uint32_t>(p.q.n_steps, 1));
   const int size_bucket = 64 - __builtin_clzll(std::max<uint64_t>(p.q.n_units, 1));
-  const uint64_t key = (uint64_t(p.family) << 48) | (uint64_t(p.sampler) << 40) | (uint64_t(steps_bucket) << 8) |
-                       uint64_t(size_bucket);
-  std::lock_guard<std::mutex> lock(ctx->tuner.mu);
+  const uint64_t key = (uint64_t(uint32_t(p.family)) << 48) | (uint64_t(p.sampler) << 40) |
+                       (uint64_t(block) << 16) | (uint64_t(steps_bucket) << 8) | uint64_t(size_bucket);
   auto it = ctx->tuner.cache.find(key);
   if (it != ctx->tuner.cache.end()) {
     ++ctx->tuner.hits;
@@ -584,9 +597,9 @@ Shape choose_shape(mpc_context* ctx, const Prepared& p) {
   }
   ++ctx->tuner.misses;
   Shape s;
-  s.block = 256;
-  int occ = std::max(1, fused_max_blocks_per_sm(p.family, p.sampler, 256));
-  uint64_t resident = uint64_t(ctx->sm_count) * occ * 256;
+  s.block = block;
+  int occ = std::max(1, fused_max_blocks_per_sm(p.family, p.sampler, int(block)));
+  uint64_t resident = uint64_t(ctx->sm_count) * occ * block;
   uint64_t want = p.q.n_units / std::max<uint64_t>(resident * 4, 1);
   uint32_t ppt = 1;
   while (ppt < 8 && uint64_t(ppt) * 2 <= want) ppt *= 2;
@@ -677,12 +690,13 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
   if (n == 0) return MPC_OK;
   int st = upload_aux(ctx, reqs);
   if (st != MPC_OK) return st;
-  // tiles: each request split into tiles of 256 * ppt units
-  std::vector<uint32_t> tile_base(n);
+  // tiles: each request split into tiles of block * ppt units
+  std::vector<uint32_t> tile_base(n), block_of(n);
   uint64_t total_tiles = 0;
   for (size_t i = 0; i < n; ++i) {
     Shape s = choose_shape(ctx, *reqs[i]);
     DevReq& q = reqs[i]->q;
+    block_of[i] = s.block;
     q.tile_units = s.block * s.ppt;
     q.n_tiles = uint32_t((q.n_units + q.tile_units - 1) / q.tile_units);
     tile_base[i] = uint32_t(total_tiles);
@@ -714,6 +728,7 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
   // ordered by per-tile cost, longest first.
   struct Group {
     int sampler, family;
+    uint32_t block;
     std::vector<size_t> members;
   };
   const bool split_families = true;
@@ -721,9 +736,11 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
   for (size_t i = 0; i < n; ++i) {
     Group* g = nullptr;
     for (Group& x : gl)
-      if (x.sampler == reqs[i]->sampler && (!split_families || x.family == reqs[i]->family)) g = &x;
+      if (x.sampler == reqs[i]->sampler && x.block == block_of[i] &&
+          (!split_families || x.family == reqs[i]->family))
+        g = &x;
     if (!g) {
-      gl.push_back({reqs[i]->sampler, reqs[i]->family, {}});
+      gl.push_back({reqs[i]->sampler, reqs[i]->family, block_of[i], {}});
       g = &gl.back();
     }
     if (g->family != reqs[i]->family) g->family = -1;
@@ -755,7 +772,7 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
   double* hm = reinterpret_cast<double*>(hp + desc_bytes + tile_bytes);
   std::vector<uint64_t> grids(groups);
   for (size_t g = 0; g < groups; ++g) {
-    int occ = std::max(1, fused_max_blocks_per_sm(gl[g].family, gl[g].sampler, 256));
+    int occ = std::max(1, fused_max_blocks_per_sm(gl[g].family, gl[g].sampler, int(gl[g].block)));
     grids[g] = std::max<uint64_t>(1, std::min<uint64_t>(uint64_t(ctx->sm_count) * occ, group_count[g]));
   }
   // The sequence between the events: descriptors and tile list in, counters
@@ -779,7 +796,7 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
       }
       e = launch_fused(static_cast<DevReq*>(d_reqs), static_cast<Tile*>(d_tiles) + group_first[g], group_count[g],
                        static_cast<uint32_t*>(d_counter) + g, gl[g].family, gl[g].sampler, ctx->tabs, int(grids[g]),
-                       256, st);
+                       int(gl[g].block), st);
     }
     for (int k = 0; k < mpc_context::kSideStreams; ++k) {  // join every forked stream, also after an error
       if (!used[k]) continue;
@@ -795,8 +812,8 @@ int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_re
                                uint64_t(uintptr_t(d_counter)), uint64_t(uintptr_t(d_mom)),
                                uint64_t(uintptr_t(ctx->tabs.sobol)), desc_bytes, tile_bytes, mom_bytes, groups};
   for (size_t g = 0; g < groups; ++g)
-    key.insert(key.end(), {uint64_t(int64_t(gl[g].family)), uint64_t(gl[g].sampler), grids[g], group_first[g],
-                           group_count[g]});
+    key.insert(key.end(), {uint64_t(int64_t(gl[g].family)), uint64_t(gl[g].sampler), uint64_t(gl[g].block), grids[g],
+                           group_first[g], group_count[g]});
   uint64_t launches_before = kernel_launch_count();
   bool replay = ctx->graph_exec && key == ctx->graph_key;
   if (!replay && key == ctx->last_batch_key) {  // second time in a row: capture (host only), then replay
@@ -2092,7 +2109,9 @@ int mpc_create(const mpc_options_t* options, mpc_context_t** out) {
   if (!out) return MPC_E_INVALID_CONFIG;
   *out = nullptr;
   // the kernels run 256-thread blocks
-  if (options && options->default_block_size != 0 && options->default_block_size != 256) return MPC_E_UNSUPPORTED;
+  if (options && options->default_block_size != 0 && options->default_block_size != 128 &&
+      options->default_block_size != 256 && options->default_block_size != 512)
+    return MPC_E_UNSUPPORTED;
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return MPC_E_NO_DEVICE;
   mpc_context* ctx = new mpc_context();
@@ -2102,6 +2121,7 @@ int mpc_create(const mpc_options_t* options, mpc_context_t** out) {
     return MPC_E_NO_DEVICE;
   }
   ctx->budget = (options && options->hbm_budget_bytes) ? options->hbm_budget_bytes : (64ull << 30);
+  if (options && options->default_block_size) ctx->tuner.default_block = options->default_block_size;
   auto bail = [&](cudaError_t e, const char* what) {
     std::fprintf(stderr, "montepath_cuda: %s failed: %s\n", what, cudaGetErrorString(e));
     delete ctx;
@@ -2161,6 +2181,49 @@ int mpc_destroy(mpc_context_t* ctx) {
 
 const char* mpc_last_error_message(const mpc_context_t* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
 
+namespace mpc {
+// Measures the fused launch of a request's kind (family, sampler, step
+// bucket) at 128, 256 and 512 threads per block, on a probe of the request
+// itself (at most 8 waves of resident blocks), and keeps the fastest for the
+// kind; 256 is kept unless another size is more than 2% faster, so the
+// choice does not flip on timing noise.  Once per kind and context.
+static int tune_block(mpc_context* ctx, const Prepared& p0) {
+  const uint64_t key = block_key(p0);
+  {
+    std::lock_guard<std::mutex> lock(ctx->tuner.mu);
+    if (ctx->tuner.block.count(key)) return MPC_OK;
+  }
+  const uint32_t cands[3] = {128, 256, 512};
+  double ms[3];
+  for (int c = 0; c < 3; ++c) {
+    ms[c] = 1e300;
+    const int occ = fused_max_blocks_per_sm(p0.family, p0.sampler, int(cands[c]));
+    if (occ < 1) continue;
+    Prepared p = p0;
+    p.block_hint = cands[c];
+    const uint64_t probe = std::min<uint64_t>(p.q.n_units, uint64_t(ctx->sm_count) * occ * cands[c] * 8);
+    p.q.n_units = probe;
+    p.q.n_paths = p.q.anti ? std::min<uint64_t>(p0.q.n_paths, 2 * probe) : probe;
+    for (int rep = 0; rep < 3; ++rep) {
+      std::vector<Prepared*> one{&p};
+      mpc_result_t r;
+      std::vector<mpc_result_t*> outs{&r};
+      const int st = run_fused(ctx, one, outs, nullptr, 0);
+      if (st != MPC_OK) return st;
+      if (rep > 0) ms[c] = std::min(ms[c], ctx->last_ms);  // the first run warms up
+    }
+  }
+  int best = 1;
+  for (int c = 0; c < 3; ++c)
+    if (ms[c] < ms[best]) best = c;
+  if (ms[1] <= 1.02 * ms[best]) best = 1;
+  std::lock_guard<std::mutex> lock(ctx->tuner.mu);
+  ctx->tuner.block[key] = cands[best];
+  ctx->tuner.measured++;
+  return MPC_OK;
+}
+}  // namespace mpc
+
 int mpc_prepare(mpc_context_t* ctx, const mpc_request_t* req, mpc_artifact_t* out) {
   if (!ctx || !req || !out) return MPC_E_INVALID_CONFIG;
   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
@@ -2179,6 +2242,10 @@ int mpc_prepare(mpc_context_t* ctx, const mpc_request_t* req, mpc_artifact_t* ou
   Prepared p;
   int st = prepare(ctx, *req, &p, &msg);
   if (st != MPC_OK) return fail(ctx, st, msg);
+  if (!p.plain && !p.block_hint && !merton_stream_request(*req)) {  // the autotuner measures the request's kind
+    st = tune_block(ctx, p);
+    if (st != MPC_OK) return st;
+  }
   Shape s = choose_shape(ctx, p);
   out->kernel_family = p.family;
   out->block_size = s.block;

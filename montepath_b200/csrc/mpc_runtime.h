@@ -37,6 +37,7 @@ struct Prepared {
   bool lsm = false;
   bool mlmc = false;
   uint32_t ppt_hint = 0;  // request's paths_per_thread (0: autotuner)
+  uint32_t block_hint = 0;  // request's block_size (0: autotuner)
   double cv_expectation = 0.0;
   std::vector<uint32_t> halton_primes;
   std::vector<double> halton_shifts;
@@ -48,8 +49,10 @@ struct Prepared {
 
 struct Autotuner {
   std::mutex mu;
-  std::map<uint64_t, Shape> cache;  // key: family | sampler | steps bucket | size bucket
-  uint64_t hits = 0, misses = 0;
+  std::map<uint64_t, Shape> cache;     // key: family | sampler | steps bucket | size bucket | block
+  std::map<uint64_t, uint32_t> block;  // measured block size per family | sampler | steps bucket
+  uint64_t hits = 0, misses = 0, measured = 0;
+  uint32_t default_block = 256;        // block of untuned kinds (context option)
 };
 
 }  // namespace mpc
@@ -111,6 +114,8 @@ uint64_t estimate_bytes(const mpc_request_t& r);
 // (its own launch sequence, not a fused tile family).
 bool merton_stream_request(const mpc_request_t& r);
 Shape choose_shape(mpc_context* ctx, const Prepared& p);
+// Key of the measured block size of a request kind.
+uint64_t block_key(const Prepared& p);
 void summarize_moments(const Prepared& p, const double* m, mpc_result_t* out);
 // Longstaff-Schwartz and MLMC requests of a batch, packed into shared launches.
 int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& reqs,

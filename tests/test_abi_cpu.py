@@ -98,7 +98,7 @@ def validate(r):
          abi.E_INVALID_CONFIG),
         ("arithmetic_asian_mlmc", dict(refinement_factor=1), abi.E_INVALID_CONFIG),
         ("arithmetic_asian_mlmc", dict(levels=0), abi.E_INVALID_CONFIG),
-        ("european_call", dict(block_size=128), abi.E_UNSUPPORTED),
+        ("european_call", dict(block_size=192), abi.E_UNSUPPORTED),
         ("european_call", dict(paths_per_thread=65), abi.E_INVALID_CONFIG),
     ],
 )
@@ -114,7 +114,8 @@ def test_valid_requests_pass():
         assert validate(make_request(w))[0] == abi.OK, w
     assert validate(make_request("european_call", model="merton", sampling="counter_hash"))[0] == abi.OK
     assert validate(make_request("european_call", model="merton", sampling="pseudorandom"))[0] == abi.OK
-    assert validate(make_request("european_call", block_size=256, paths_per_thread=4))[0] == abi.OK
+    for block in (128, 256, 512):
+        assert validate(make_request("european_call", block_size=block, paths_per_thread=4))[0] == abi.OK
 
 
 def test_unknown_enum_rejected():
@@ -146,10 +147,10 @@ def test_create_without_device_reports_no_device():
     assert lib().mpc_create(None, ctypes.byref(handle)) == abi.E_NO_DEVICE
 
 
-def test_create_rejects_block_size_other_than_256():
+def test_create_rejects_unsupported_block_size():
     # checked before any device call, so it holds with or without a GPU
     handle = ctypes.c_void_p()
-    opts = abi.Options(device=0, deterministic=1, hbm_budget_bytes=0, default_block_size=128)
+    opts = abi.Options(device=0, deterministic=1, hbm_budget_bytes=0, default_block_size=384)
     assert lib().mpc_create(ctypes.byref(opts), ctypes.byref(handle)) == abi.E_UNSUPPORTED
     assert not handle.value
 
