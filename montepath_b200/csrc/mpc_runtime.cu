@@ -2183,10 +2183,12 @@ const char* mpc_last_error_message(const mpc_context_t* ctx) { return ctx ? ctx-
 
 namespace mpc {
 // Measures the fused launch of a request's kind (family, sampler, step
-// bucket) at 128, 256 and 512 threads per block, on a probe of the request
-// itself (at most 8 waves of resident blocks), and keeps the fastest for the
-// kind; 256 is kept unless another size is more than 2% faster, so the
-// choice does not flip on timing noise.  Once per kind and context.
+// bucket) at 128, 256 and 512 threads per block, on the request itself (its
+// first 4,194,304 units at most: a probe much shorter than the request
+// misjudges the tail of the launch), and keeps the fastest for the kind; 256
+// is kept unless another size is more than 1% faster (the best of three
+// timed runs each), so the choice does not flip on timing noise.  Once per
+// kind and context.
 static int tune_block(mpc_context* ctx, const Prepared& p0) {
   const uint64_t key = block_key(p0);
   {
@@ -2201,10 +2203,10 @@ static int tune_block(mpc_context* ctx, const Prepared& p0) {
     if (occ < 1) continue;
     Prepared p = p0;
     p.block_hint = cands[c];
-    const uint64_t probe = std::min<uint64_t>(p.q.n_units, uint64_t(ctx->sm_count) * occ * cands[c] * 8);
+    const uint64_t probe = std::min<uint64_t>(p.q.n_units, 1ull << 22);
     p.q.n_units = probe;
     p.q.n_paths = p.q.anti ? std::min<uint64_t>(p0.q.n_paths, 2 * probe) : probe;
-    for (int rep = 0; rep < 3; ++rep) {
+    for (int rep = 0; rep < 4; ++rep) {
       std::vector<Prepared*> one{&p};
       mpc_result_t r;
       std::vector<mpc_result_t*> outs{&r};
@@ -2216,7 +2218,7 @@ static int tune_block(mpc_context* ctx, const Prepared& p0) {
   int best = 1;
   for (int c = 0; c < 3; ++c)
     if (ms[c] < ms[best]) best = c;
-  if (ms[1] <= 1.02 * ms[best]) best = 1;
+  if (ms[1] <= 1.01 * ms[best]) best = 1;
   std::lock_guard<std::mutex> lock(ctx->tuner.mu);
   ctx->tuner.block[key] = cands[best];
   ctx->tuner.measured++;
