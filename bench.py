@@ -54,6 +54,8 @@ SFU_PER_STEP = {"heston": 2 * 1 + 1, "merton": 1}
 # kernels are issue-bound, so this gives the fraction of the SMs' issue slots
 # (4 warp instructions per cycle per SM) the measured rate uses.
 WARP_INSTR_PER_32_STEPS = {"heston": 106.0, "merton": 99.7}
+# Lane instructions per path-step of the same capture (smsp__thread_inst_executed.sum / path-steps).
+LANE_INSTR_PER_STEP = {"heston": 105.9, "merton": 96.1}
 
 
 def requests(precision: str):
@@ -428,6 +430,7 @@ def run_ours(args) -> None:
                 "frac": frac,
                 "traffic": traffic,
                 "fractions": {"fp32": fr_fp32, "sfu": fr_sfu, "issue": fr_issue},
+                "lane_instructions_per_path_step": LANE_INSTR_PER_STEP,
                 "peak_source": "measured by mpc_measure_peaks on this GPU (FP32 FMA chains / MUFU ex2 chains)",
                 "hbm_peak_gbs": load_peaks().get("hbm_gbs"),
             },
