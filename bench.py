@@ -577,6 +577,28 @@ def leg_book(backend, contracts: int = 4096) -> dict:
     }
 
 
+def leg_merton_reference(backend) -> dict:
+    """The reference's own Merton estimator (terminal, pseudorandom
+    MonteCarloRng stream per chunk, 8 chunks) at 1,048,576 paths: the stream
+    replay of mpc_merton.cu, device time with L2 flushed, median of 10."""
+
+    from montepath_b200.requests import make_request
+
+    r = make_request("european_call", dict(model="merton", n_paths=1 << 20, seed=9303, n_threads=8,
+                                           jump_intensity=0.5, jump_mean=-0.1, jump_volatility=0.15))
+    for _ in range(3):
+        backend.price(r)
+    ts = []
+    res = None
+    for _ in range(10):
+        backend.flush_l2()
+        res = backend.price(r)
+        ts.append(backend.last_timing()[0])
+    ms = sorted(ts)[len(ts) // 2]
+    return {"paths": r.n_paths, "chunks": 8, "ms": ms, "paths_per_sec": r.n_paths / (ms * 1e-3),
+            "price": res.price, "stderr": res.stderr}
+
+
 def leg_serving(backend) -> dict:
     """Poisson serving stream at 2,000 requests/s, seed 42: the full 60 s
     stream (about 120,000 requests) through the resident device loop; the
@@ -594,7 +616,7 @@ def leg_serving(backend) -> dict:
 
 
 LEGS = {"gbm_european_20000x64": leg_gbm_european_small, "heston_merton_1048576x256": leg_heston_merton, "american_put_lsm_524288x50": leg_american_put_lsm, "book_4096": leg_book,
-        "serving_2000rps": leg_serving}
+        "serving_2000rps": leg_serving, "merton_reference_1048576": leg_merton_reference}
 
 
 def main() -> None:
@@ -606,7 +628,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP64 plain comparison of the headline")
     ap.add_argument("--paths", type=int, default=0, help="override the path count (profiling cases)")
-    ap.add_argument("--legs", default="all", help="comma list of gbm_european_20000x64, heston_merton_1048576x256, american_put_lsm_524288x50, book_4096, serving_2000rps; all or none")
+    ap.add_argument("--legs", default="all", help="comma list of gbm_european_20000x64, heston_merton_1048576x256, american_put_lsm_524288x50, book_4096, serving_2000rps, merton_reference_1048576; all or none")
     ap.add_argument("--book-contracts", type=int, default=4096,
                     help="first contracts of the book in the book_4096 leg (profiling cases)")
     args = ap.parse_args()
