@@ -45,11 +45,13 @@ MERTON = dict(model="merton", jump_intensity=0.5, jump_mean=-0.1, jump_volatilit
     (20_000, 1, dict(jump_intensity=6.0, jump_mean=0.02)),        # several jumps per path, long Poisson loops
     (20_000, 3, dict(jump_intensity=0.0)),                        # no Poisson uniform drawn at all
     (30_000, 1, dict(t=0.25, jump_intensity=2.0, s0=90.0, k=95.0)),
+    (200_003, 32, {}),                                            # many chunks, each with its own chain
+    (65_536, 1, dict(seed=0)),                                    # seed 0 maps to MonteCarloRng's fixed state
 ])
 @pytest.mark.parametrize("precision", ["fp64_plain", "fp32_path"])
 def test_merton_pseudorandom_per_path(backend, n_paths, threads, kw, precision):
     cfg = dict(MERTON, n_paths=n_paths, seed=9303, n_threads=threads, precision=precision)
-    cfg.update(kw)
+    cfg.update(kw)  # may override the seed
     r = req("european_call", **cfg)
     _, ref = O.price_paths(r)
     got = backend.price_paths(r)

@@ -105,3 +105,39 @@ def test_device_loop_mlmc_meets_rmse_target(backend):
     assert res.estimated_stderr <= 1e-3
     ref = O.price(req("arithmetic_asian_mlmc", target_stderr=2e-2, precision="fp64_plain", **cfg))
     assert abs(res.price - ref.price) < 3 * (res.stderr ** 2 + ref.stderr ** 2) ** 0.5, (res.price, ref.price)
+
+
+def test_device_loop_budget_cancel_and_stop(backend):
+    """Admission under the HBM budget, cancellation of a queued request, a
+    request too large for the budget refused with MPC_E_OOM_BUDGET, and a
+    stop while work is still running: the loop leaves, the server returns
+    promptly and the context prices on afterwards."""
+
+    from montepath_b200.backend import BackendError
+
+    big = req("european_call", model="heston", n_paths=1 << 22, n_steps=256, seed=1, sampling="scrambled_sobol")
+    small = req("european_call", method="stepwise", n_paths=10_000, n_steps=16, seed=2, sampling="counter_hash")
+    huge = req("european_call", model="heston", n_paths=1 << 30, n_steps=256, seed=3, sampling="scrambled_sobol",
+               precision="fp64_plain")
+    with backend.server(max_slots=1, mode="device_loop", hbm_budget_bytes=1 << 30) as srv:
+        t_big = srv.submit(big)
+        t_small = srv.submit(small)
+        assert srv.poll(t_small) is None
+        assert srv.cancel(t_small) == abi.OK
+        with pytest.raises(BackendError) as err:
+            srv.wait(t_small, 10_000)
+        assert err.value.status == abi.E_CANCELLED
+        t_huge = srv.submit(huge)
+        done = srv.wait(t_big, 60_000)
+        assert done.status == abi.OK
+        with pytest.raises(BackendError) as err:
+            srv.wait(t_huge, 60_000)
+        assert err.value.status == abi.E_OOM_BUDGET
+    with backend.server(max_slots=4, mode="device_loop") as srv:
+        for i in range(4):
+            srv.submit(req("european_call", model="heston", n_paths=1 << 21, n_steps=256, seed=10 + i,
+                           sampling="scrambled_sobol"))
+        t0 = time.perf_counter()
+    assert time.perf_counter() - t0 < 5.0  # stop with work in flight: the loop leaves at its next claim
+    after = backend.price(small)
+    assert after.status == abi.OK and after.price > 0
