@@ -2298,9 +2298,9 @@ __device__ __forceinline__ uint32_t reduce_scatter16_index(uint32_t lane) {
 
 // One exercise date's regression across the job's blocks (round = the date's
 // position in the backward pass).  Every block has written its 15 moments to
-// partials[buf][lb]; thread 0 adds one to the job's arrival count, which the
-// host zeroes before the launch and which only grows, and waits until it
-// reaches nb (round + 1).  Then every block sums the partials itself in the
+// partials[buf][lb]; thread 0 adds one to its arrival counter (lb % 4 of
+// the job's four, which the host zeroes before the launch and which only
+// grow), and waits until their sum reaches nb (round + 1).  Then every block sums the partials itself in the
 // same fixed order (thread t: moment t % 16 over blocks t / 16, t / 16 + 16,
 // ...; then one thread per moment over the 16 lanes) and solves the normal
 // equations in thread 0: the same operations on the same data, so every block
@@ -2311,22 +2311,27 @@ __device__ __forceinline__ uint32_t reduce_scatter16_index(uint32_t lane) {
 // it.  The wait is bounded: after timeout_ns the block records
 // kLsmErrTimeout and every block of the job leaves at its next check.
 // Returns false when the job's error flag is set.
-__device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint32_t nb, uint32_t round, int coeffs,
-                                                 double* fold, double* s_mom, double* s_beta, int* s_ok) {
+__device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint32_t nb, uint32_t lb, uint32_t round,
+                                                 int coeffs, double* fold, double* s_mom, double* s_beta, int* s_ok) {
   __shared__ int s_good;
   __syncthreads();
   if (threadIdx.x == 0) {
+    // arrivals spread over kLsmArrivalLanes counters (one L2 line each); the
+    // date is complete when their sum reaches nb * (round + 1)
     const unsigned target = nb * (round + 1u);
     __threadfence();
-    if (atomicAdd(a.barrier, 1u) + 1u != target) {
-      volatile unsigned* count = a.barrier;
-      const uint64_t start = global_ns();
-      while (*count < target) {
-        if (*((volatile int*)a.error) != 0) break;
-        if (global_ns() - start > a.timeout_ns) {
-          atomicCAS(a.error, 0, kLsmErrTimeout);
-          break;
-        }
+    atomicAdd(a.barrier + kLsmArrivalStride * (lb % kLsmArrivalLanes), 1u);
+    const uint64_t start = global_ns();
+    for (;;) {
+      unsigned sum = 0;
+#pragma unroll
+      for (uint32_t c = 0; c < kLsmArrivalLanes; ++c)
+        sum += *((volatile unsigned*)(a.barrier + kLsmArrivalStride * c));
+      if (sum >= target) break;
+      if (*((volatile int*)a.error) != 0) break;
+      if (global_ns() - start > a.timeout_ns) {
+        atomicCAS(a.error, 0, kLsmErrTimeout);
+        break;
       }
     }
     __threadfence();
@@ -2338,8 +2343,19 @@ __device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint
   const uint32_t mom = threadIdx.x & 15u, lane_grp = threadIdx.x >> 4, n_grp = blockDim.x >> 4;
   double acc = 0.0;
   if (mom < (uint32_t)kLsmMom && lsm_ok(a, base_at + (uint64_t)nb * 16 - 1, a.partials_len, kLsmErrPartials)) {
-#pragma unroll 4
-    for (uint32_t blk = lane_grp; blk < nb; blk += n_grp) acc += __ldcg(a.partials + base_at + (size_t)blk * 16 + mom);
+    // every load of the thread's blocks issued before the first add (one L2
+    // round trip for up to 8 blocks per lane group), then summed in block order
+    constexpr int kBatch = 8;
+    for (uint32_t blk0 = lane_grp; blk0 < nb; blk0 += kBatch * n_grp) {
+      double v[kBatch];
+#pragma unroll
+      for (int i = 0; i < kBatch; ++i) {
+        const uint32_t blk = blk0 + (uint32_t)i * n_grp;
+        v[i] = blk < nb ? __ldcg(a.partials + base_at + (size_t)blk * 16 + mom) : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < kBatch; ++i) acc += v[i];
+    }
   }
   acc += __shfl_xor_sync(0xffffffffu, acc, 16);  // the warp's two lane groups
   if ((threadIdx.x & 31u) < 16u) fold[(threadIdx.x >> 5) * 16 + mom] = acc;
@@ -2541,7 +2557,7 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
     if (si > 0) load_date(si - 1);  // next date's values, in flight during the wait
     // Every block waits (bounded) for all blocks' partials of this date, then
     // sums them in block order and solves the normal equations itself.
-    if (!lsm_gather_solve(a, buf, nb, round++, coeffs, s_fold, s_mom, s_beta, &s_ok)) return;
+    if (!lsm_gather_solve(a, buf, nb, lb, round++, coeffs, s_fold, s_mom, s_beta, &s_ok)) return;
     if (s_ok) {
       ++regressions;
       const Real b0 = (Real)s_beta[0], b1 = (Real)s_beta[1], b2 = (Real)s_beta[2], b3 = (Real)s_beta[3];
