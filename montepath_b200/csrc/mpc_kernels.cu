@@ -54,10 +54,16 @@ struct SrcCtx {
 
 // Dimensions of the Sobol table rows staged in shared memory at a time, and
 // the row stride in words: kSobolWindow + 4 is 4 mod 32, so the 16 rows one
-// warp touches with a 128-bit load fall into two wavefronts.
+// warp touches with a 128-bit load fall into two wavefronts.  The window
+// holds the 64 rows of the index's four low nibbles and one constant row:
+// for points below 2^16 in their block, the upper 16 bits of the Owen-shuffled
+// index depend on the seed alone (a bit of the shuffled index depends only on
+// the bits above it, and those are zero), so the XOR of their four nibble rows
+// is one word per dimension, the same for every point of the block.
 constexpr uint32_t kSobolWindow = 64;
 constexpr uint32_t kSobolRowStride = kSobolWindow + 4;
-constexpr uint32_t kSobolWindowWords = 128 * kSobolRowStride;  // 34,816 bytes
+constexpr uint32_t kSobolLowRows = 64;  // nibble positions 0..3, 16 values each
+constexpr uint32_t kSobolWindowWords = (kSobolLowRows + 1) * kSobolRowStride;  // 17,680 bytes
 
 // Phi^-1(u) for a 23-bit midpoint uniform u from the segment table: v =
 // min(u, 1 - u) (exact) selects binade and one of 32 segments from its
@@ -254,12 +260,12 @@ struct Source<SMP_XORSHIFT> {
 // and the output scramble skips its first reversal.
 struct SobolQuad {
   const uint32_t* rows_global;  // [128][256] bit-reversed rows
-  uint32_t* win;                // [128][kSobolRowStride] shared-memory window
+  uint32_t* win;                // [kSobolLowRows + 1][kSobolRowStride] shared-memory window
   const float4* icdf;           // inverse-normal segments in shared memory
   uint32_t win_first;           // first dimension in the window (multiple of 4)
   uint32_t local, block_seed, group, seed_g, combine_g, quad;
   uint32_t qbase;               // (quad's first dimension mod 256) + combine_g
-  uint32_t rows[8];             // window word offset of this point's row per nibble position
+  uint32_t rows[4];             // window word offset of this point's row per low nibble position
   uint32_t x0, x1, x2, x3;      // reversed products of the dimensions of `quad`
   template <bool FP64>
   __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
@@ -274,21 +280,32 @@ struct SobolQuad {
   }
   // Block-synchronous: restages the window at d0 rounded down to a multiple
   // of 4 when [d0, d0 + count) is not inside it.  Requires
-  // count <= kSobolWindow - 3 so that the step fits the aligned window.
-  // The copy is 16-byte asynchronous global-to-shared transfers (four
-  // dimensions of one row each; an aligned quad never crosses the 256-dimension
-  // wrap), all in flight at once, then one wait.
+  // count <= kSobolWindow - 3 so that the step fits the aligned window, and
+  // every point of the block in one 2^16-point block (tiles are at most 2^16
+  // units and aligned), so that the constant row is the block's.  The low
+  // rows are 16-byte asynchronous global-to-shared transfers (four dimensions
+  // of one row each; an aligned quad never crosses the 256-dimension wrap),
+  // all in flight at once while the constant row is computed, then one wait.
   __device__ __forceinline__ void at_step(uint32_t d0, uint32_t count) {
     if (win_first != 0xFFFFFFFFu && d0 >= win_first && d0 + count <= win_first + kSobolWindow) return;
     __syncthreads();
     const uint32_t w0 = d0 & ~3u;
     constexpr uint32_t kQuadsPerRow = kSobolWindow / 4;
     const uint32_t win_s = (uint32_t)__cvta_generic_to_shared(win);
-    for (uint32_t i = threadIdx.x; i < 128 * kQuadsPerRow; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < kSobolLowRows * kQuadsPerRow; i += blockDim.x) {
       const uint32_t row = i / kQuadsPerRow, j = 4 * (i % kQuadsPerRow);
       const uint32_t* src = rows_global + row * MPC_SOBOL_TABLE_DIMS + ((w0 + j) & (MPC_SOBOL_TABLE_DIMS - 1));
       const uint32_t dst = win_s + 4u * (row * kSobolRowStride + j);
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+    }
+    for (uint32_t j = threadIdx.x; j < kSobolWindow; j += blockDim.x) {
+      const uint32_t d = w0 + j;
+      const uint32_t hi = nested_uniform_scramble(0u, block_seed + d / MPC_SOBOL_TABLE_DIMS) >> 16;
+      const uint32_t dm = d & (MPC_SOBOL_TABLE_DIMS - 1);
+      uint32_t c = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) c ^= __ldg(rows_global + (16u * (4 + k) + ((hi >> (4 * k)) & 0xFu)) * MPC_SOBOL_TABLE_DIMS + dm);
+      win[kSobolLowRows * kSobolRowStride + j] = c;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
@@ -303,15 +320,15 @@ struct SobolQuad {
       seed_g = block_seed + g;
       const uint32_t shuffled = nested_uniform_scramble(local, seed_g);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) rows[k] = (16u * k + ((shuffled >> (4 * k)) & 0xFu)) * kSobolRowStride;
+      for (int k = 0; k < 4; ++k) rows[k] = (16u * k + ((shuffled >> (4 * k)) & 0xFu)) * kSobolRowStride;
       combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
     }
     quad = d0 >> 2;
     qbase = (d0 & (MPC_SOBOL_TABLE_DIMS - 1)) + combine_g;
     const uint32_t* base = win + (d0 - win_first);
-    uint4 a = *reinterpret_cast<const uint4*>(base + rows[0]);
+    uint4 a = *reinterpret_cast<const uint4*>(base + kSobolLowRows * kSobolRowStride);  // the constant row
 #pragma unroll
-    for (int k = 1; k < 8; ++k) {
+    for (int k = 0; k < 4; ++k) {
       const uint4 b = *reinterpret_cast<const uint4*>(base + rows[k]);
       a.x ^= b.x;
       a.y ^= b.y;

@@ -183,12 +183,17 @@ void complete(mpc_server* s, Ticket& t, int status) {
 }
 
 // Tile size of a slot request: the autotuner's shape, doubled until the work
-// list fits the slot's partials.
-void shape_for_slot(const mpc_server* s, Prepared* p) {
+// list fits the slot's partials, up to 2^16 units (a fused tile stays inside
+// one 2^16-point Sobol block).  False when the request needs more tiles than
+// a slot holds even then (over 2^30 units): it runs as its own batch.
+bool shape_for_slot(const mpc_server* s, Prepared* p) {
   Shape sh = choose_shape(s->ctx, *p);
   p->q.tile_units = sh.block * sh.ppt;
-  while ((p->q.n_units + p->q.tile_units - 1) / p->q.tile_units > s->max_tiles_per_slot) p->q.tile_units *= 2;
+  while ((p->q.n_units + p->q.tile_units - 1) / p->q.tile_units > s->max_tiles_per_slot &&
+         p->q.tile_units < 65536u)
+    p->q.tile_units *= 2;
   p->q.n_tiles = uint32_t((p->q.n_units + p->q.tile_units - 1) / p->q.tile_units);
+  return p->q.n_tiles <= s->max_tiles_per_slot;
 }
 
 bool fused_eligible(const Ticket& t) {
@@ -455,14 +460,15 @@ void level_stats(const double* m, double* mean, double* var) {
 
 // Queues the loop jobs of an MLMC phase: pilot levels at pilot_paths_per_level
 // (phase 1) or every level of every replicate at the allocation (phase 2).
-void queue_mlmc_phase(mpc_server* s, Ticket& t, int phase) {
+// False when a level needs more tiles than a slot holds (over 2^30 paths).
+bool queue_mlmc_phase(mpc_server* s, Ticket& t, int phase) {
   const mpc_request_t& r = t.work;
   t.phase = phase;
   const uint64_t reps = phase == 1 ? 1 : mlmc_replicates(r);
   const uint32_t L = r.levels;
   t.lvl_mean.assign(reps * L, 0.0);
   t.lvl_var.assign(reps * L, 0.0);
-  t.jobs_left = uint32_t(reps * L);
+  std::vector<LoopJob> jobs;
   for (uint64_t rep = 0; rep < reps; ++rep) {
     const uint64_t seed = reps > 1 ? derive_chunk_seed(r.seed, rep) : r.seed;
     for (uint32_t l = 0; l < L; ++l) {
@@ -470,10 +476,13 @@ void queue_mlmc_phase(mpc_server* s, Ticket& t, int phase) {
       j.ticket = t.id;
       j.index = uint32_t(rep * L + l);
       level_request(r, seed, l, phase == 1 ? r.pilot_paths_per_level : r.paths_per_level[l], &j.prep);
-      shape_for_slot(s, &j.prep);
-      s->pending.push_back(std::move(j));
+      if (!shape_for_slot(s, &j.prep)) return false;
+      jobs.push_back(std::move(j));
     }
   }
+  t.jobs_left = uint32_t(jobs.size());
+  for (LoopJob& j : jobs) s->pending.push_back(std::move(j));
+  return true;
 }
 
 // Admission under the HBM budget (FIFO); routes each admitted request to the
@@ -509,7 +518,7 @@ void admit_loop(mpc_server* s) {
     if (mlmc && t.req.precision == MPC_PRECISION_FP32_PATH && smp >= 0) {
       t.route = 1;
       t.work = t.req;
-      queue_mlmc_phase(s, t, t.req.target_stderr > 0.0 ? 1 : 2);
+      if (!queue_mlmc_phase(s, t, t.req.target_stderr > 0.0 ? 1 : 2)) complete(s, t, MPC_E_UNSUPPORTED);
     } else if (!mlmc && fused_eligible(t) && loop_sampler(t.prep)) {
       t.route = 1;
       t.jobs_left = 1;
@@ -640,7 +649,7 @@ int reap(mpc_server* s) {
       if (--t.jobs_left == 0) {
         if (t.phase == 1) {
           mlmc_allocate(t.work, t.lvl_var.data(), &t.res);
-          queue_mlmc_phase(s, t, 2);
+          if (!queue_mlmc_phase(s, t, 2)) complete(s, t, MPC_E_UNSUPPORTED);
         } else {
           const double est = t.res.estimated_stderr;
           const uint32_t met = t.res.target_met, hit = t.res.max_step_updates_hit;
@@ -866,8 +875,8 @@ int mpc_submit(mpc_server_t* s, const mpc_request_t* req, uint64_t* ticket) {
     if (st == MPC_OK && !t.prep.plain && s->opt.mode != 1) {
       if (!t.prep.halton_primes.empty() || !t.prep.lhs.empty() || t.prep.q.bridge || merton_stream_request(*req))
         t.prep.plain = true;  // per-request tables or the Merton stream replay: their own launches
-      else
-        shape_for_slot(s, &t.prep);
+      else if (!shape_for_slot(s, &t.prep))
+        t.prep.plain = true;  // too many tiles for a slot: priced as its own batch
     }
   } else if (st == MPC_OK) {
     t.prep.lsm = req->workload != MPC_WORKLOAD_ASIAN_MLMC;
