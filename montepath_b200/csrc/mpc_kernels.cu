@@ -55,15 +55,18 @@ struct SrcCtx {
 // Dimensions of the Sobol table rows staged in shared memory at a time, and
 // the row stride in words: kSobolWindow + 4 is 4 mod 32, so the 16 rows one
 // warp touches with a 128-bit load fall into two wavefronts.  The window
-// holds the 64 rows of the index's four low nibbles and one constant row:
-// for points below 2^16 in their block, the upper 16 bits of the Owen-shuffled
-// index depend on the seed alone (a bit of the shuffled index depends only on
-// the bits above it, and those are zero), so the XOR of their four nibble rows
-// is one word per dimension, the same for every point of the block.
+// holds the 48 rows of the index's three low nibbles and one constant row:
+// a bit of the Owen-shuffled index depends only on the point's bits at and
+// above it (and the seed), so bits 12..31 of the shuffled index are the same
+// for every point of one aligned 4,096-point group, and the XOR of their five
+// nibble rows is one word per dimension.  The points a block runs together
+// (one iteration of a tile: at most 512 consecutive aligned units, the tile's
+// idle threads repeating the iteration's first unit) lie in one such group.
 constexpr uint32_t kSobolWindow = 64;
 constexpr uint32_t kSobolRowStride = kSobolWindow + 4;
-constexpr uint32_t kSobolLowRows = 64;  // nibble positions 0..3, 16 values each
-constexpr uint32_t kSobolWindowWords = (kSobolLowRows + 1) * kSobolRowStride;  // 17,680 bytes
+constexpr uint32_t kSobolLowNibbles = 3;                        // nibble positions 0..2 staged per point
+constexpr uint32_t kSobolLowRows = 16 * kSobolLowNibbles;       // 48 rows
+constexpr uint32_t kSobolWindowWords = (kSobolLowRows + 1) * kSobolRowStride;  // 13,328 bytes
 
 // Phi^-1(u) for a 23-bit midpoint uniform u from the segment table: v =
 // min(u, 1 - u) (exact) selects binade and one of 32 segments from its
@@ -265,7 +268,7 @@ struct SobolQuad {
   uint32_t win_first;           // first dimension in the window (multiple of 4)
   uint32_t local, block_seed, group, seed_g, combine_g, quad;
   uint32_t qbase;               // (quad's first dimension mod 256) + combine_g
-  uint32_t rows[4];             // window word offset of this point's row per low nibble position
+  uint32_t rows[kSobolLowNibbles];  // window word offset of this point's row per low nibble position
   uint32_t x0, x1, x2, x3;      // reversed products of the dimensions of `quad`
   template <bool FP64>
   __device__ __forceinline__ void begin(const DevReq& q, const SrcCtx& c, uint64_t u) {
@@ -281,8 +284,8 @@ struct SobolQuad {
   // Block-synchronous: restages the window at d0 rounded down to a multiple
   // of 4 when [d0, d0 + count) is not inside it.  Requires
   // count <= kSobolWindow - 3 so that the step fits the aligned window, and
-  // every point of the block in one 2^16-point block (tiles are at most 2^16
-  // units and aligned), so that the constant row is the block's.  The low
+  // every point the block runs together in one aligned 4,096-point group, so
+  // that the constant row is theirs.  The low
   // rows are 16-byte asynchronous global-to-shared transfers (four dimensions
   // of one row each; an aligned quad never crosses the 256-dimension wrap),
   // all in flight at once while the constant row is computed, then one wait.
@@ -300,11 +303,14 @@ struct SobolQuad {
     }
     for (uint32_t j = threadIdx.x; j < kSobolWindow; j += blockDim.x) {
       const uint32_t d = w0 + j;
-      const uint32_t hi = nested_uniform_scramble(0u, block_seed + d / MPC_SOBOL_TABLE_DIMS) >> 16;
+      // bits 12..31 of the shuffled index of this block's points (its bits
+      // below 12 do not reach them)
+      const uint32_t hi = nested_uniform_scramble(local & 0xF000u, block_seed + d / MPC_SOBOL_TABLE_DIMS);
       const uint32_t dm = d & (MPC_SOBOL_TABLE_DIMS - 1);
       uint32_t c = 0;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) c ^= __ldg(rows_global + (16u * (4 + k) + ((hi >> (4 * k)) & 0xFu)) * MPC_SOBOL_TABLE_DIMS + dm);
+      for (int k = kSobolLowNibbles; k < 8; ++k)
+        c ^= __ldg(rows_global + (16u * k + ((hi >> (4 * k)) & 0xFu)) * MPC_SOBOL_TABLE_DIMS + dm);
       win[kSobolLowRows * kSobolRowStride + j] = c;
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
@@ -320,7 +326,7 @@ struct SobolQuad {
       seed_g = block_seed + g;
       const uint32_t shuffled = nested_uniform_scramble(local, seed_g);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) rows[k] = (16u * k + ((shuffled >> (4 * k)) & 0xFu)) * kSobolRowStride;
+      for (int k = 0; k < (int)kSobolLowNibbles; ++k) rows[k] = (16u * k + ((shuffled >> (4 * k)) & 0xFu)) * kSobolRowStride;
       combine_g = 0x9e3779b9u + (seed_g << 6) + (seed_g >> 2);
     }
     quad = d0 >> 2;
@@ -328,7 +334,7 @@ struct SobolQuad {
     const uint32_t* base = win + (d0 - win_first);
     uint4 a = *reinterpret_cast<const uint4*>(base + kSobolLowRows * kSobolRowStride);  // the constant row
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < (int)kSobolLowNibbles; ++k) {
       const uint4 b = *reinterpret_cast<const uint4*>(base + rows[k]);
       a.x ^= b.x;
       a.y ^= b.y;
@@ -1106,7 +1112,7 @@ __device__ __forceinline__ void fused_tile(const DevReq& sq, const SrcCtx& ctx, 
   for (uint32_t it = 0; it < iters; ++it) {
     uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
     const bool valid = u < last;
-    if (!valid) u = first;
+    if (!valid) u = first + (uint64_t)it * blockDim.x;  // the iteration's first unit: same Sobol index bits 12..31
     double p, c;
     if constexpr (FAM >= 0)
       fused_unit<FAM, SMP>(sq, ctx, u, p, c);
@@ -1692,7 +1698,7 @@ __global__ void __launch_bounds__(kFusedBlock, 2) scenario_kernel(const DevReq* 
     for (uint32_t it = 0; it < iters; ++it) {
       uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
       const bool valid = u < last;
-      if (!valid) u = first;  // keeps block-synchronous sources in lockstep; discarded below
+      if (!valid) u = first + (uint64_t)it * blockDim.x;  // lockstep for block-synchronous sources; discarded below
       typename FusedUnitSource<FAM, SMP>::type src;  // the samples fused_unit<FAM, SMP> draws
       src.template begin<false>(sq, ctx, u);
       float pay[kMaxScen], pay2[kMaxScen], ctl[kMaxScen];
@@ -1938,7 +1944,7 @@ __global__ void __launch_bounds__(kFusedBlock, 2) basket_scenario_kernel(const D
     for (uint32_t it = 0; it < iters; ++it) {
       uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
       const bool valid = u < last;
-      if (!valid) u = first;  // keeps block-synchronous sources in lockstep; discarded below
+      if (!valid) u = first + (uint64_t)it * blockDim.x;  // lockstep for block-synchronous sources; discarded below
       typename FusedUnitSource<FAM_BASKET, SMP>::type src;  // the samples fused_unit<FAM_BASKET, SMP> draws
       src.template begin<false>(sq, ctx, u);
       float pay[kBasketScen];
