@@ -1602,7 +1602,10 @@ static double inverse_normal_refined(double p) {
 // binade [2^e, 2^(e+1)), e = -24 .. -2, is cut into 32 equal segments, and a
 // segment's cubic in t in [0, 1) (the position inside the segment)
 // interpolates Phi^-1(v) at the 4 Chebyshev nodes.  Max error over all 2^23
-// uniforms: 4.5e-7.
+// uniforms: 4.5e-7.  The kernels evaluate it at t / 32 (the segment's 18
+// mantissa bits read as a float in [0, 1/32) without a shift), so
+// coefficient k is stored times 32^k: a power-of-two scaling that every
+// Horner step carries exactly, so the values equal those of the cubic in t.
 static void build_icdf_segments(uint32_t* out) {
   for (int e = 0; e < 23; ++e)
     for (int s = 0; s < 32; ++s) {
@@ -1625,7 +1628,7 @@ static void build_icdf_segments(uint32_t* out) {
         for (int k = 0; k < 4; ++k) poly[k] = next[k];
       }
       for (int k = 0; k < 4; ++k) {
-        const float c = (float)poly[k];
+        const float c = std::ldexp((float)poly[k], 5 * k);
         std::memcpy(&out[(e * 32 + s) * 4 + k], &c, sizeof(c));
       }
     }
