@@ -53,9 +53,9 @@ SFU_PER_STEP = {"heston": 2 * 1 + 1, "merton": 1}
 # (smsp__inst_executed.sum of the quarter-size ncu capture in profiles/): the
 # kernels are issue-bound, so this gives the fraction of the SMs' issue slots
 # (4 warp instructions per cycle per SM) the measured rate uses.
-WARP_INSTR_PER_32_STEPS = {"heston": 91.7, "merton": 77.1}
+WARP_INSTR_PER_32_STEPS = {"heston": 84.7, "merton": 69.8}
 # Lane instructions per path-step of the same capture (smsp__thread_inst_executed.sum / path-steps).
-LANE_INSTR_PER_STEP = {"heston": 91.6, "merton": 73.6}
+LANE_INSTR_PER_STEP = {"heston": 84.6, "merton": 66.4}
 
 
 def requests(precision: str):

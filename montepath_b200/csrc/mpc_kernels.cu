@@ -2251,7 +2251,7 @@ __device__ __forceinline__ void laguerre4(Real x, Real b[4]) {
 // Gauss-Jordan with partial pivoting in FP64, the reference's operations in
 // its order, with every index static (the pivot row swap is a predicated exchange), so the
 // system stays in registers.
-template <int DIM>
+template <int DIM, bool RECIP = false>
 __device__ __forceinline__ bool solve_fixed(double a[4][4], double rhs[4]) {
 #pragma unroll
   for (int piv = 0; piv < DIM; ++piv) {
@@ -2281,9 +2281,16 @@ __device__ __forceinline__ bool solve_fixed(double a[4][4], double rhs[4]) {
       }
     }
     const double pv = a[piv][piv];
+    if constexpr (RECIP) {
+      const double ip = 1.0 / pv;
 #pragma unroll
-    for (int c = piv; c < DIM; ++c) a[piv][c] /= pv;
-    rhs[piv] /= pv;
+      for (int c = piv; c < DIM; ++c) a[piv][c] *= ip;
+      rhs[piv] *= ip;
+    } else {
+#pragma unroll
+      for (int c = piv; c < DIM; ++c) a[piv][c] /= pv;
+      rhs[piv] /= pv;
+    }
 #pragma unroll
     for (int row = 0; row < DIM; ++row) {
       if (row == piv) continue;
@@ -2339,73 +2346,93 @@ __device__ __forceinline__ uint32_t reduce_scatter16_index(uint32_t lane) {
 }
 
 // One exercise date's regression across the job's blocks (round = the date's
-// position in the backward pass).  Every block has written its 15 moments to
-// partials[buf][lb]; thread 0 adds one to its arrival counter (lb % 4 of
-// the job's four, which the host zeroes before the launch and which only
-// grow), and waits until their sum reaches nb (round + 1).  Then every block sums the partials itself in the
-// same fixed order (thread t: moment t % 16 over blocks t / 16, t / 16 + 16,
-// ...; then one thread per moment over the 16 lanes) and solves the normal
-// equations in thread 0: the same operations on the same data, so every block
-// holds the same coefficients, with no publication round trip after the
-// solve (~35 KB of L2 reads per block and date instead).  The partials of
-// date round + 1 go to the other buffer, and no block writes this buffer
-// again before every block has arrived at round + 1, i.e. finished reading
-// it.  The wait is bounded: after timeout_ns the block records
+// position in the backward pass).  Every block writes its 15 moments to its
+// own slot row partials[round][lb] with relaxed stores; the host marks every
+// slot empty (all bits set) before the launch and no slot is written twice,
+// so the data is its own arrival flag: each block reads every block's slots
+// of the round at once and re-reads (bounded) only those still empty, with no
+// fence, counter or separate poll between the write and the read.  Then every
+// block sums the partials itself in the same fixed order (thread t: moment
+// t % 16 over blocks t / 16, t / 16 + 32, ...; the lane groups' sums by
+// shuffles, then a fixed shuffle tree per moment over the 16 warps) and solves
+// the normal equations in thread 0: the same operations on the same data, so
+// every block holds the same coefficients, with no publication round trip
+// after the solve.  The FP32 path scales each pivot row by the pivot's
+// reciprocal instead of dividing every entry (the FP64 path divides, as the
+// reference does).  The wait is bounded: after timeout_ns the block records
 // kLsmErrTimeout and every block of the job leaves at its next check.
 // Returns false when the job's error flag is set.
-__device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint32_t nb, uint32_t lb, uint32_t round,
+// Empty marker of a date's partial slot (all bits set); the host fills the
+// partials with it before the launch, and a written value never equals it.
+constexpr unsigned long long kLsmEmpty = 0xFFFFFFFFFFFFFFFFull;
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_f64(double* p, double x) {
+  unsigned long long v = (unsigned long long)__double_as_longlong(x);
+  if (v == kLsmEmpty) v = 0x7FF8000000000001ull;  // a NaN with the marker's bits: keep it a NaN
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+template <bool RECIP>
+__device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, uint32_t nb, uint32_t lb, uint32_t round,
                                                  int coeffs, double* fold, double* s_mom, double* s_beta, int* s_ok) {
-  __shared__ int s_good;
+  __shared__ int s_bad;
+  if (threadIdx.x == 0) s_bad = 0;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    // arrivals spread over kLsmArrivalLanes counters (one L2 line each); the
-    // date is complete when their sum reaches nb * (round + 1)
-    const unsigned target = nb * (round + 1u);
-    __threadfence();
-    atomicAdd(a.barrier + kLsmArrivalStride * (lb % kLsmArrivalLanes), 1u);
-    const uint64_t start = global_ns();
-    for (;;) {
-      unsigned sum = 0;
-#pragma unroll
-      for (uint32_t c = 0; c < kLsmArrivalLanes; ++c)
-        sum += *((volatile unsigned*)(a.barrier + kLsmArrivalStride * c));
-      if (sum >= target) break;
-      if (*((volatile int*)a.error) != 0) break;
-      if (global_ns() - start > a.timeout_ns) {
-        atomicCAS(a.error, 0, kLsmErrTimeout);
-        break;
-      }
-    }
-    __threadfence();
-    s_good = *((volatile int*)a.error) == 0;
-  }
-  __syncthreads();
-  if (!s_good) return false;
-  const uint64_t base_at = (uint64_t)buf * nb * 16;
+  const uint64_t base_at = (uint64_t)round * nb * 16;
   const uint32_t mom = threadIdx.x & 15u, lane_grp = threadIdx.x >> 4, n_grp = blockDim.x >> 4;
   double acc = 0.0;
   if (mom < (uint32_t)kLsmMom && lsm_ok(a, base_at + (uint64_t)nb * 16 - 1, a.partials_len, kLsmErrPartials)) {
-    // every load of the thread's blocks issued before the first add (one L2
-    // round trip for up to 8 blocks per lane group), then summed in block order
+    // every load of the thread's blocks issued at once; the slots still empty
+    // are read again (bounded) until their blocks have written them; then
+    // the values are summed in block order
     constexpr int kBatch = 8;
+    const uint64_t start = global_ns();
     for (uint32_t blk0 = lane_grp; blk0 < nb; blk0 += kBatch * n_grp) {
-      double v[kBatch];
+      unsigned long long v[kBatch];
 #pragma unroll
       for (int i = 0; i < kBatch; ++i) {
         const uint32_t blk = blk0 + (uint32_t)i * n_grp;
-        v[i] = blk < nb ? __ldcg(a.partials + base_at + (size_t)blk * 16 + mom) : 0.0;
+        v[i] = blk < nb ? ld_relaxed_u64(a.partials + base_at + (size_t)blk * 16 + mom) : 0ull;
+      }
+      for (;;) {
+        bool pending = false;
+#pragma unroll
+        for (int i = 0; i < kBatch; ++i) {
+          if (v[i] != kLsmEmpty) continue;
+          pending = true;
+          v[i] = ld_relaxed_u64(a.partials + base_at + (size_t)(blk0 + (uint32_t)i * n_grp) * 16 + mom);
+        }
+        if (!pending) break;
+        if (*((volatile int*)a.error) != 0) {
+          s_bad = 1;
+          break;
+        }
+        if (global_ns() - start > a.timeout_ns) {
+          atomicCAS(a.error, 0, kLsmErrTimeout);
+          s_bad = 1;
+          break;
+        }
       }
 #pragma unroll
-      for (int i = 0; i < kBatch; ++i) acc += v[i];
+      for (int i = 0; i < kBatch; ++i) acc += __longlong_as_double((long long)v[i]);
     }
   }
-  acc += __shfl_xor_sync(0xffffffffu, acc, 16);  // the warp's two lane groups
-  if ((threadIdx.x & 31u) < 16u) fold[(threadIdx.x >> 5) * 16 + mom] = acc;
   __syncthreads();
-  if (threadIdx.x < (uint32_t)kLsmMom) {
-    double t = 0.0;
-    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) t += fold[w * 16 + threadIdx.x];
-    s_mom[threadIdx.x] = t;
+  if (s_bad) return false;
+  acc += __shfl_xor_sync(0xffffffffu, acc, 16);  // the warp's two lane groups
+  if ((threadIdx.x & 31u) < 16u) fold[(threadIdx.x >> 5) * 17 + mom] = acc;
+  __syncthreads();
+  if (threadIdx.x < 256u) {  // 16 warps (512-thread blocks): moment t / 16 over warp t % 16
+    const uint32_t mo = threadIdx.x >> 4, w = threadIdx.x & 15u;
+    double t = mo < (uint32_t)kLsmMom ? fold[w * 17 + mo] : 0.0;
+    t += __shfl_xor_sync(0xffffffffu, t, 8);
+    t += __shfl_xor_sync(0xffffffffu, t, 4);
+    t += __shfl_xor_sync(0xffffffffu, t, 2);
+    t += __shfl_xor_sync(0xffffffffu, t, 1);
+    if (w == 0 && mo < (uint32_t)kLsmMom) s_mom[mo] = t;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -2430,7 +2457,7 @@ __device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint
       for (int c = 0; c < 4; ++c) ata[r][c] = ata[c][r] = 0.0;
     }
     int ok = s_mom[14] >= (double)coeffs ? 1 : 0;
-    if (ok) ok = (coeffs == 2 ? solve_fixed<2>(ata, atb) : coeffs == 3 ? solve_fixed<3>(ata, atb) : solve_fixed<4>(ata, atb)) ? 1 : 0;
+    if (ok) ok = (coeffs == 2 ? solve_fixed<2, RECIP>(ata, atb) : coeffs == 3 ? solve_fixed<3, RECIP>(ata, atb) : solve_fixed<4, RECIP>(ata, atb)) ? 1 : 0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) s_beta[r] = (ok && r < coeffs) ? atb[r] : 0.0;
     *s_ok = ok;
@@ -2440,8 +2467,8 @@ __device__ __forceinline__ bool lsm_gather_solve(const LsmArgs& a, int buf, uint
 }
 
 // One 512-thread block per SM: the same warps per SM as two 256-thread
-// blocks, but half the block partials to fold and arrivals to count per date
-// (the per-date cross-block round is this kernel's critical path).
+// blocks, but half the block partials to fold per date (the per-date
+// cross-block round is this kernel's critical path).
 template <class Real, int SMP>
 __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __restrict__ jobs, uint32_t n_jobs, SrcCtx ctx) {
   __shared__ double red[kLsmBlock / 32][5];
@@ -2449,7 +2476,7 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
   __shared__ double s_beta[4];
   __shared__ int s_ok;
   __shared__ uint32_t s_job;
-  __shared__ double s_red15[kLsmBlock / 32][16];
+  __shared__ double s_red15[kLsmBlock / 32][17];
   __shared__ double s_fold[kLsmBlock];  // 16 lanes x 16 moments of the last block's fold
   __shared__ Real s_disc[512];
   if (threadIdx.x == 0) {
@@ -2525,7 +2552,6 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
     if (step == 0 || step > steps) {
       if (threadIdx.x == 0) lsm_report(a, kLsmErrSched, step);
     }
-    const int buf = si & 1;
     double m[kLsmMom];
 #pragma unroll
     for (int i = 0; i < kLsmMom; ++i) m[i] = 0.0;
@@ -2579,7 +2605,7 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
     }
     // block reduction of the 15 moments: warp sums by reduce-scatter, then
     // one thread per moment folds the warps in order
-    const uint64_t part_at = ((uint64_t)buf * nb + lb) * 16;
+    const uint64_t part_at = ((uint64_t)round * nb + lb) * 16;
     {
       double mv[16];
 #pragma unroll
@@ -2589,17 +2615,23 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
       if ((lane & 1u) == 0) s_red15[threadIdx.x >> 5][reduce_scatter16_index(lane)] = w;
     }
     __syncthreads();
-    if (threadIdx.x < (uint32_t)kLsmMom) {
-      double t = 0.0;
-      for (int w = 0; w < kLsmBlock / 32; ++w) t += s_red15[w][threadIdx.x];
-      // published by thread 0's fence before its arrival in lsm_gather_solve:
-      // the block barrier orders these stores before that (cumulative) fence
-      if (lsm_ok(a, part_at + threadIdx.x, a.partials_len, kLsmErrPartials)) a.partials[part_at + threadIdx.x] = t;
+    if (threadIdx.x < 256u) {
+      // moment m = t / 16 over the 16 warps w = t % 16: a shuffle tree per
+      // 16-lane group
+      const uint32_t mo = threadIdx.x >> 4, w = threadIdx.x & 15u;
+      double t = mo < (uint32_t)kLsmMom ? s_red15[w][mo] : 0.0;
+      t += __shfl_xor_sync(0xffffffffu, t, 8);
+      t += __shfl_xor_sync(0xffffffffu, t, 4);
+      t += __shfl_xor_sync(0xffffffffu, t, 2);
+      t += __shfl_xor_sync(0xffffffffu, t, 1);
+      // the slot's own value marks its arrival (lsm_gather_solve)
+      if (w == 0 && mo < (uint32_t)kLsmMom && lsm_ok(a, part_at + mo, a.partials_len, kLsmErrPartials))
+        st_relaxed_f64(a.partials + part_at + mo, t);
     }
     if (si > 0) load_date(si - 1);  // next date's values, in flight during the wait
     // Every block waits (bounded) for all blocks' partials of this date, then
     // sums them in block order and solves the normal equations itself.
-    if (!lsm_gather_solve(a, buf, nb, lb, round++, coeffs, s_fold, s_mom, s_beta, &s_ok)) return;
+    if (!lsm_gather_solve<sizeof(Real) == 4>(a, nb, lb, round++, coeffs, s_fold, s_mom, s_beta, &s_ok)) return;
     if (s_ok) {
       ++regressions;
       const Real b0 = (Real)s_beta[0], b1 = (Real)s_beta[1], b2 = (Real)s_beta[2], b3 = (Real)s_beta[3];

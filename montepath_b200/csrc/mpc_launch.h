@@ -75,10 +75,10 @@ struct LsmArgs {
   const uint32_t* sched;     // exercise dates (ascending, ends with n_steps)
   const double* disc_pow;    // disc_step^j, j = 0..n_steps
   void* paths;               // [n_steps][n_paths] float or double
-  double* partials;          // [2][grid][16]
+  double* partials;          // [rounds][grid][16], every slot empty (all bits set) at launch
   double* final_partials;    // [grid][4]
   double* out;               // [8]: n, sum, sumsq, early, maturity, regressions, -, -
-  unsigned* barrier;         // counter area (kLsmCounterBytes): arrival count (all dates), ...
+  unsigned* barrier;         // counter area (kLsmCounterBytes)
   unsigned* done;            // last-block counter
   int* error;                // first failure: kLsmErr* code (0 = none)
   unsigned long long* diag;  // offending index of a failed self-check
@@ -112,13 +112,9 @@ cudaError_t launch_lsm_batch(const LsmArgs* d_jobs, uint32_t n_jobs, uint32_t to
 uint32_t lsm_capacity(int fp64, int sampler);
 constexpr uint32_t kLsmPathsPerThreadMax = 8;
 constexpr uint32_t kLsmThreads = 512;
-// Counter area of an LSM job (zeroed per launch): four arrival counters 64
-// bytes apart (blocks arrive at counter lb % 4, so the per-date atomics of a
-// job spread over four L2 lines), the last-block counter at uint 4, the error
-// code at uint 8 and its index at uint 10.
+// Counter area of an LSM job (zeroed per launch): the last-block counter at
+// uint 4, the error code at uint 8 and its index at uint 10.
 constexpr size_t kLsmCounterBytes = 256;
-constexpr uint32_t kLsmArrivalLanes = 4;
-constexpr uint32_t kLsmArrivalStride = 16;  // uints between arrival counters
 
 // Bump-and-revalue legs sharing every normal: one request d_req (GBM step,
 // GBM terminal or Heston; xorshift, Sobol or counter-hash samples; any

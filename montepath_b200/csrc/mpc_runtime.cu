@@ -296,7 +296,9 @@ uint64_t estimate_bytes(const mpc_request_t& r) {
   uint64_t units = r.technique == MPC_TECHNIQUE_ANTITHETIC ? (r.n_paths + 1) / 2 : r.n_paths;
   if (is_lsm(r.workload)) {
     uint64_t elem = r.precision == MPC_PRECISION_FP64_PLAIN ? 8 : 4;
-    return r.n_paths * r.n_steps * elem + 2 * 8192 * 16 * 8 + 4096;
+    // path matrix, one row of 16-double slots per exercise date for up to
+    // 512 blocks (one block per SM), estimator partials and counters
+    return r.n_paths * r.n_steps * elem + uint64_t(std::max<uint32_t>(r.n_steps, 1)) * 512 * 16 * 8 + 512 * 4 * 8 + 4096;
   }
   uint64_t dims = r.n_steps;
   if (r.model == MPC_MODEL_HESTON) dims = 2ull * r.n_steps;
@@ -1066,6 +1068,8 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     int fp64, sampler;
     LsmArgs args;
   };
+  // regression rounds of a schedule (one per date before maturity; at least one slot row)
+  auto lsm_rounds = [](size_t n_sched) -> uint64_t { return n_sched > 1 ? uint64_t(n_sched - 1) : 1ull; };
   std::vector<Job> jobs(reqs.size());
   for (size_t i = 0; i < reqs.size(); ++i) {
     const mpc_request_t& r = *reqs[i];
@@ -1129,7 +1133,7 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       blocks += jobs[i].blocks;
       done[i] = true;
     }
-    // device arena layout per job: paths | sched | disc | partials | final | out | counters
+    // device arena layout per job: paths | sched | disc | partials (one slot row per date) | final | out | counters
     auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     std::vector<size_t> offs;
     size_t bytes = align(group.size() * sizeof(LsmArgs));
@@ -1138,7 +1142,7 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       offs.push_back(bytes);
       const size_t elem = j.fp64 ? 8 : 4;
       bytes += align(j.args.n_paths * j.args.n_steps * elem) + align(j.sched.size() * 4) +
-               align(j.disc_pow.size() * 8) + align(2ull * j.blocks * 16 * 8) + align(j.blocks * 4ull * 8) +
+               align(j.disc_pow.size() * 8) + align(lsm_rounds(j.sched.size()) * j.blocks * 16 * 8) + align(j.blocks * 4ull * 8) +
                align(8 * 8) + align(kLsmCounterBytes);
     }
     void* arena = nullptr;
@@ -1164,20 +1168,22 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       h2d += j.disc_pow.size() * 8;
       o += align(j.disc_pow.size() * 8);
       a.partials = reinterpret_cast<double*>(base + o);
-      o += align(2ull * j.blocks * 16 * 8);
+      // one slot row per exercise date, all marked empty (every byte 0xFF)
+      MPC_CUDA(ctx, cudaMemsetAsync(a.partials, 0xFF, lsm_rounds(j.sched.size()) * j.blocks * 16 * 8, ctx->stream));
+      o += align(lsm_rounds(j.sched.size()) * j.blocks * 16 * 8);
       a.final_partials = reinterpret_cast<double*>(base + o);
       o += align(j.blocks * 4ull * 8);
       a.out = reinterpret_cast<double*>(base + o);
       o += align(8 * 8);
-      // counters (zeroed per launch): arrival count (grows by nb per date)
-      // at 0, block-done counter at 16, error code at 32, failed index at 40
+      // counters (zeroed per launch): block-done counter at 16, error code
+      // at 32, failed index at 40
       a.barrier = reinterpret_cast<unsigned*>(base + o);
       a.done = a.barrier + 4;
       a.error = reinterpret_cast<int*>(a.barrier + 8);
       a.diag = reinterpret_cast<unsigned long long*>(a.barrier + 10);
       MPC_CUDA(ctx, cudaMemsetAsync(a.barrier, 0, kLsmCounterBytes, ctx->stream));
       a.paths_len = a.n_paths * a.n_steps;
-      a.partials_len = 2u * j.blocks * 16u;
+      a.partials_len = uint32_t(lsm_rounds(j.sched.size()) * j.blocks * 16u);
       a.final_len = j.blocks * 4u;
       a.block_first = block_first;
       a.n_blocks = j.blocks;
