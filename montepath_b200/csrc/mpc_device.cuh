@@ -97,13 +97,13 @@ struct XorshiftStream {
     has_cached = true;
     return radius * -c;
   }
-  // Position the stream of `seed` so that the next normal is normal number
-  // `normal_index` of the sequential stream.
-  __device__ __forceinline__ void seek(const uint64_t* __restrict__ nibble, uint64_t seed,
-                                       uint64_t normal_index, bool fp32) {
-    uint64_t s0 = seed == 0 ? 0x9E3779B97F4A7C15ull : seed;
-    uint64_t pair = normal_index >> 1;
-    state = xorshift_jump(nibble, s0, 2 * pair);
+  // First state of the stream of `seed` (MonteCarloRng replaces seed 0).
+  __device__ __forceinline__ static uint64_t first_state(uint64_t seed) { return seed == 0 ? 0x9E3779B97F4A7C15ull : seed; }
+  // Starts from `aligned`, the state after 2 * (normal_index / 2) draws, so
+  // that the next normal is normal number `normal_index` (an odd index first
+  // draws the pair and keeps its second normal).
+  __device__ __forceinline__ void seek_aligned(uint64_t aligned, uint64_t normal_index, bool fp32) {
+    state = aligned;
     has_cached = false;
     if (normal_index & 1) {
       if (fp32)
@@ -111,6 +111,12 @@ struct XorshiftStream {
       else
         (void)normal_f64();
     }
+  }
+  // Position the stream of `seed` so that the next normal is normal number
+  // `normal_index` of the sequential stream.
+  __device__ __forceinline__ void seek(const uint64_t* __restrict__ nibble, uint64_t seed,
+                                       uint64_t normal_index, bool fp32) {
+    seek_aligned(xorshift_jump(nibble, first_state(seed), 2 * (normal_index >> 1)), normal_index, fp32);
   }
 };
 

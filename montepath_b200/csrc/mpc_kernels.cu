@@ -2514,6 +2514,11 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
   q.seed32 = a.seed32;
   q.n_chunks = 1;
   q.normals_per_unit = steps;
+  // Pseudorandom sampler: a thread's paths lie nthreads paths apart, so the
+  // stream state at each path start after the first is one jump of
+  // T^(nthreads x steps) draws (nthreads is even, so the pair alignment of
+  // the start carries over), 16 table lookups instead of a full seek.
+  uint64_t aligned = 0;
 #pragma unroll
   for (int j = 0; j < kLsmMaxP; ++j) {
     const uint64_t path = gtid + (uint64_t)j * nthreads;
@@ -2521,7 +2526,15 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
     exd[j] = steps;
     if (path >= n) continue;
     Source<SMP> src;
-    src.template begin<sizeof(Real) == 8>(q, ctx, path);
+    if constexpr (SMP == SMP_XORSHIFT) {
+      const uint64_t idx = path * steps;
+      aligned = (j == 0 || a.stride_jump == nullptr)
+                    ? xorshift_jump(ctx.jump, XorshiftStream::first_state(a.seed), 2 * (idx >> 1))
+                    : gf2_apply(a.stride_jump, aligned);
+      src.st.seek_aligned(aligned, idx, sizeof(Real) == 4);
+    } else {
+      src.template begin<sizeof(Real) == 8>(q, ctx, path);
+    }
     Real s = (Real)a.s0;
     for (uint32_t st = 1; st <= steps; ++st) {
       const Real z = normal<Real>(src, st - 1);

@@ -74,6 +74,8 @@ struct LsmArgs {
   double s0, k, drift, vol, disc_step;
   const uint32_t* sched;     // exercise dates (ascending, ends with n_steps)
   const double* disc_pow;    // disc_step^j, j = 0..n_steps
+  const uint64_t* stride_jump;  // pseudorandom sampler: nibble table [16][16] of T^(grid threads x n_steps),
+                                // the stream jump between a thread's successive paths
   void* paths;               // [n_steps][n_paths] float or double
   double* partials;          // [rounds][grid][16], every slot empty (all bits set) at launch
   double* final_partials;    // [grid][4]

@@ -1063,6 +1063,7 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     size_t index;
     std::vector<uint32_t> sched;
     std::vector<double> disc_pow;
+    std::vector<uint64_t> stride_tab;  // pseudorandom sampler: nibble table of the per-thread path stride jump
     bool normalised;
     uint32_t degree, blocks;
     int fp64, sampler;
@@ -1098,6 +1099,8 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       want = std::min<uint64_t>(want, ctx->lsm_block_cap);
     }
     j.blocks = uint32_t(std::max<uint64_t>(need, want));
+    if (j.sampler == SMP_XORSHIFT)
+      j.stride_tab = xorshift_jump_table(uint64_t(j.blocks) * kLsmThreads * uint64_t(r.n_steps));
     LsmArgs& a = j.args;
     std::memset(&a, 0, sizeof(a));
     a.n_paths = r.n_paths;
@@ -1142,7 +1145,8 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       offs.push_back(bytes);
       const size_t elem = j.fp64 ? 8 : 4;
       bytes += align(j.args.n_paths * j.args.n_steps * elem) + align(j.sched.size() * 4) +
-               align(j.disc_pow.size() * 8) + align(lsm_rounds(j.sched.size()) * j.blocks * 16 * 8) + align(j.blocks * 4ull * 8) +
+               align(j.disc_pow.size() * 8) + align(256 * 8) + align(lsm_rounds(j.sched.size()) * j.blocks * 16 * 8) +
+               align(j.blocks * 4ull * 8) +
                align(8 * 8) + align(kLsmCounterBytes);
     }
     void* arena = nullptr;
@@ -1167,6 +1171,13 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
                                     ctx->stream));
       h2d += j.disc_pow.size() * 8;
       o += align(j.disc_pow.size() * 8);
+      a.stride_jump = nullptr;
+      if (!j.stride_tab.empty()) {
+        a.stride_jump = reinterpret_cast<const uint64_t*>(base + o);
+        MPC_CUDA(ctx, cudaMemcpyAsync(base + o, j.stride_tab.data(), 256 * 8, cudaMemcpyHostToDevice, ctx->stream));
+        h2d += 256 * 8;
+      }
+      o += align(256 * 8);
       a.partials = reinterpret_cast<double*>(base + o);
       // one slot row per exercise date, all marked empty (every byte 0xFF)
       MPC_CUDA(ctx, cudaMemsetAsync(a.partials, 0xFF, lsm_rounds(j.sched.size()) * j.blocks * 16 * 8, ctx->stream));
@@ -1638,6 +1649,42 @@ static void build_icdf_segments(uint32_t* out) {
         std::memcpy(&out[(e * 32 + s) * 4 + k], &c, sizeof(c));
       }
     }
+}
+
+// Nibble table [q][v] of T^k, T the xorshift64* state transition: entry
+// (q, v) is T^k applied to the nibble value v placed at bit 4q, so a state x
+// jumps k draws with 16 lookups (gf2_apply).  T^k by repeated squaring of
+// the 64 x 64 bit matrix, kept as the images of the basis vectors.
+std::vector<uint64_t> xorshift_jump_table(uint64_t k) {
+  auto apply = [](const std::vector<uint64_t>& m, uint64_t x) {
+    uint64_t y = 0;
+    for (int i = 0; i < 64; ++i)
+      if ((x >> i) & 1) y ^= m[i];
+    return y;
+  };
+  std::vector<uint64_t> M(64), S(64), N(64);
+  for (int i = 0; i < 64; ++i) {
+    uint64_t x = 1ull << i;
+    x ^= x >> 12;
+    x ^= x << 25;
+    x ^= x >> 27;
+    M[i] = x;         // T
+    S[i] = 1ull << i;  // identity
+  }
+  for (; k; k >>= 1) {
+    if (k & 1) {
+      for (int i = 0; i < 64; ++i) N[i] = apply(M, S[i]);  // S <- T^(2^b) S
+      S.swap(N);
+    }
+    for (int i = 0; i < 64; ++i) N[i] = apply(M, M[i]);  // M <- M M
+    M.swap(N);
+  }
+  std::vector<uint64_t> tab(256, 0ull);
+  for (int q = 0; q < 16; ++q)
+    for (int v = 0; v < 16; ++v)
+      for (int j = 0; j < 4; ++j)
+        if ((v >> j) & 1) tab[q * 16 + v] ^= S[4 * q + j];
+  return tab;
 }
 
 void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump) {

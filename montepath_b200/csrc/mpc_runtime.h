@@ -135,6 +135,8 @@ void mlmc_finish(const mpc_request_t& r, const double* mean, double* var, double
 // Host copies of the device lookup tables: Sobol nibble tables [256][8][16]
 // and xorshift64* jump-ahead nibble tables [64][16][16].
 void build_tables(std::vector<uint32_t>& sob, std::vector<uint64_t>& jump);
+// Nibble table [16][16] of the xorshift64* jump by k draws (for gf2_apply).
+std::vector<uint64_t> xorshift_jump_table(uint64_t k);
 // Fused FP32 requests: one persistent launch per (sampler, family) group on the context stream.
 int run_fused(mpc_context* ctx, std::vector<Prepared*>& reqs, std::vector<mpc_result_t*>& outs,
               double* per_unit_host, uint64_t per_unit_cap);
