@@ -1115,6 +1115,24 @@ constexpr int fused_min_blocks512(int fam, int smp) { return fused_min_blocks(fa
 // One tile of request `sq`: its units through the model, the block's moment
 // sums written as the tile's partial, and *s_last (shared) set when this was
 // the request's last tile to finish.  Ends with the block synchronised.
+// gf2_apply with the nibble table in shared memory.
+__device__ __forceinline__ uint64_t gf2_apply_shared(const uint64_t* table, uint64_t x) {
+  uint64_t y = 0;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) y ^= table[q * 16 + ((x >> (4 * q)) & 0xF)];
+  return y;
+}
+
+// A unit of a single-family fused kernel whose pseudorandom stream is
+// already positioned: `aligned` is the chunk stream's state after
+// 2 * (idx / 2) draws, idx the unit's first normal in its chunk.
+template <int FAM>
+__device__ __forceinline__ void fused_unit_stream(const DevReq& q, uint64_t aligned, uint64_t idx, double& p, double& c) {
+  Source<SMP_XORSHIFT> src;
+  src.st.seek_aligned(aligned, idx, true);
+  run_family<float, FAM>(q, src, p, c);
+}
+
 template <int FAM, int SMP>
 __device__ __forceinline__ void fused_tile(const DevReq& sq, const SrcCtx& ctx, uint32_t tile, double (*red)[5],
                                            int* s_last) {
@@ -1127,12 +1145,52 @@ __device__ __forceinline__ void fused_tile(const DevReq& sq, const SrcCtx& ctx, 
   // sources stay in lockstep; a thread past the tile end repeats the first
   // unit and discards it.
   const uint32_t iters = (uint32_t)((last - first + blockDim.x - 1) / blockDim.x);
+  // Pseudorandom streams in a single-family kernel: a thread's units of one
+  // tile lie blockDim units apart, so inside one chunk the next unit's
+  // stream starts one jump of T^(blockDim x normals per unit) draws later
+  // (blockDim is even, so the pair alignment carries over).  The block
+  // tabulates that jump in shared memory for the tile (the images of the 64
+  // basis vectors, then the nibble table), and each unit after a thread's
+  // first in the tile takes 16 lookups instead of a full seek.
+  constexpr bool kStride = SMP == SMP_XORSHIFT && FAM >= 0;
+  uint64_t* stride_tab = nullptr;
+  if constexpr (kStride) {
+    __shared__ uint64_t s_cols[64];
+    __shared__ uint64_t s_stride[256];
+    stride_tab = s_stride;
+    if (iters > 1) {
+      const uint64_t delta = (uint64_t)blockDim.x * sq.normals_per_unit;
+      for (uint32_t i = threadIdx.x; i < 64; i += blockDim.x) s_cols[i] = xorshift_jump(ctx.jump, 1ull << i, delta);
+      __syncthreads();
+      for (uint32_t e = threadIdx.x; e < 256; e += blockDim.x) {
+        uint64_t y = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j)
+          if ((e >> j) & 1u) y ^= s_cols[4 * (e >> 4) + j];
+        s_stride[e] = y;
+      }
+      __syncthreads();
+    }
+  }
+  uint64_t aligned = 0, prev_seed = 0;
+  bool chained = false;  // `aligned` holds this thread's previous unit's start in the same tile
   for (uint32_t it = 0; it < iters; ++it) {
     uint64_t u = first + threadIdx.x + (uint64_t)it * blockDim.x;
     const bool valid = u < last;
     if (!valid) u = first + (uint64_t)it * blockDim.x;  // the iteration's first unit: same Sobol index bits 12..31
     double p, c;
-    if constexpr (FAM >= 0)
+    if constexpr (kStride) {
+      uint64_t seed, local;
+      chunk_of(sq, u, &seed, &local);
+      const uint64_t idx = local * sq.normals_per_unit;
+      if (chained && valid && seed == prev_seed)
+        aligned = gf2_apply_shared(stride_tab, aligned);
+      else
+        aligned = xorshift_jump(ctx.jump, XorshiftStream::first_state(seed), 2 * (idx >> 1));
+      chained = valid;
+      prev_seed = seed;
+      fused_unit_stream<FAM>(sq, aligned, idx, p, c);
+    } else if constexpr (FAM >= 0)
       fused_unit<FAM, SMP>(sq, ctx, u, p, c);
     else
       fused_unit_any<SMP>(sq, ctx, u, p, c);

@@ -1763,15 +1763,21 @@ enum CostRow : int {
 const RateRow kRates[ROW_COUNT] = {
     {{2.24e11, 3.25e11, 3.85e11, 9.05e10}, {1.31e11, 1.35e11, 5.96e10, 5.38e10}},  // GBM stepwise
     {{2.12e11, 2.93e11, 3.50e11, 8.84e10}, {1.12e11, 1.16e11, 5.59e10, 5.02e10}},  // arithmetic Asian
-    {{6.68e9, 1.83e10, 1.53e10, 1.11e10}, {7.38e9, 2.45e10, 1.98e10, 1.12e10}},    // GBM terminal
+    {{8.7e10, 1.83e10, 1.53e10, 1.11e10}, {7.38e9, 2.45e10, 1.98e10, 1.12e10}},    // GBM terminal (pseudorandom FP32: + kTerminalFixedMs)
     {{1.45e11, 1.93e11, 2.23e11, 5.37e10}, {7.09e10, 6.85e10, 3.02e10, 3.14e10}},  // Heston
     {{1.05e11, 1.05e11, 1.97e11, 4.30e10}, {4.16e10, 4.16e10, 2.65e10, 2.63e10}},  // Merton stepwise
     {{1.70e10, 1.70e10, 1.44e10, 7.09e9}, {1.83e10, 1.83e10, 1.30e10, 6.60e9}},    // Merton terminal
     {{5.46e9, 1.53e10, 1.28e10, 7.74e9}, {5.49e9, 1.58e10, 1.13e10, 6.77e9}},      // 2-asset basket
     {{1.41e11, 1.41e11, 1.41e11, 1.41e11}, {4.59e10, 4.59e10, 4.59e10, 4.59e10}},  // GBM stepwise, bridge
 };
-const double kLsmFixedMs = 0.24, kLsmRate = 6.4e10; // 49 cross-block date rounds, then path-steps
-                                                      // (fit to 524,288 paths x 50 dates)
+// FP32 pseudorandom terminal GBM: each thread's first path of a tile takes a
+// full stream seek and its later paths one table jump each, so the time has
+// an intercept (about one full seek per resident thread, scaled down for
+// requests with fewer paths than resident threads) beside the per-path
+// rate (fit to 2,097,152 and 4,194,304 paths on a B200: 0.157 and 0.180 ms).
+const double kTerminalFixedMs = 0.134;
+const double kLsmFixedMs = 0.22, kLsmRate = 1.7e11; // 49 cross-block date rounds, then path-steps
+                                                      // (fit to 524,288 paths x 50 dates, FP32: 0.37 ms)
 const double kCallOverheadMs = 0.035;               // events, copies, one launch
 const double kFirstCallMs = 2.0;                    // tables and buffers of a new shape
 const int kCostColumns = 4;
@@ -1797,12 +1803,21 @@ int rate_column(int sampling) {
 struct RateSource {
   const std::vector<double>* calibrated;  // [row][2][kCostColumns] or null
   double scale;
+  const std::vector<double>* fixed = nullptr;  // calibrated intercepts (ms), same layout, or null
   double at(int row, bool fp64, int col) const {
     if (calibrated && !calibrated->empty()) {
       const double v = (*calibrated)[(size_t(row) * 2 + (fp64 ? 1 : 0)) * kCostColumns + col];
       if (v > 0.0) return v;
     }
     return (fp64 ? kRates[row].fp64[col] : kRates[row].fp32[col]) * scale;
+  }
+  // per-call intercept of the terminal GBM row (ms)
+  double fixed_at(int row, bool fp64, int col) const {
+    if (calibrated && !calibrated->empty() && fixed && !fixed->empty()) {
+      const double r = (*calibrated)[(size_t(row) * 2 + (fp64 ? 1 : 0)) * kCostColumns + col];
+      if (r > 0.0) return (*fixed)[(size_t(row) * 2 + (fp64 ? 1 : 0)) * kCostColumns + col];
+    }
+    return row == ROW_GBM_TERMINAL && !fp64 && col == 0 ? kTerminalFixedMs : 0.0;
   }
   bool measured_here() const { return calibrated && !calibrated->empty(); }
 };
@@ -1851,6 +1866,9 @@ int estimate_cost_with(const mpc_request_t* req, const RateSource& rates, mpc_co
   } else if (r.workload == MPC_WORKLOAD_EUROPEAN_CALL && r.method != MPC_METHOD_STEPWISE) {
     units = double(r.n_paths);
     rate = pick(ROW_GBM_TERMINAL);
+    // the intercept is one full seek per thread that has a path: it reaches
+    // its full size once every resident thread (2,048 per SM) has one
+    fixed_ms = rates.fixed_at(ROW_GBM_TERMINAL, fp64, col) * std::min(1.0, units / (2048.0 * 148.0 * rates.scale));
   } else if (r.sampling == MPC_SAMPLING_SCRAMBLED_SOBOL_BRIDGE) {
     rate = pick(ROW_BRIDGE);
   } else {
@@ -1921,7 +1939,7 @@ int mpc_estimate_cost(const mpc_request_t* req, int sm_count, mpc_cost_t* out) {
 int mpc_estimate_cost_ctx(mpc_context_t* ctx, const mpc_request_t* req, mpc_cost_t* out) {
   if (!ctx) return MPC_E_INVALID_CONFIG;
   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
-  const RateSource rates{&ctx->cost_rates, double(ctx->sm_count) / 148.0};
+  const RateSource rates{&ctx->cost_rates, double(ctx->sm_count) / 148.0, &ctx->cost_fixed};
   return estimate_cost_with(req, rates, out);
 }
 
@@ -1930,6 +1948,7 @@ int mpc_calibrate_cost(mpc_context_t* ctx, double* seconds) {
   std::lock_guard<std::recursive_mutex> lock(ctx->mu);
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<double> rates(size_t(ROW_COUNT) * 2 * kCostColumns, 0.0);
+  std::vector<double> fixed(rates.size(), 0.0);
   const RateSource builtin{nullptr, double(ctx->sm_count) / 148.0};
   for (int row = 0; row < ROW_COUNT; ++row) {
     for (int p = 0; p < 2; ++p) {
@@ -1951,11 +1970,27 @@ int mpc_calibrate_cost(mpc_context_t* ctx, double* seconds) {
         if (st == MPC_OK) st = mpc_price(ctx, &r, &res);
         if (st == MPC_E_CUDA || st == MPC_E_NO_DEVICE) return st;
         if (st != MPC_OK) continue;
-        if (ctx->last_ms > 0.0) *cell = double(units.path_steps) / (ctx->last_ms * 1e-3);
+        if (!(ctx->last_ms > 0.0)) continue;
+        *cell = double(units.path_steps) / (ctx->last_ms * 1e-3);
+        if (row == ROW_GBM_TERMINAL) {
+          // terminal paths: a second size separates the intercept from the rate
+          const double t1 = ctx->last_ms;
+          mpc_request_t r4 = r;
+          r4.n_paths = 4 * r.n_paths;
+          st = mpc_price(ctx, &r4, &res);
+          if (st == MPC_OK) st = mpc_price(ctx, &r4, &res);
+          if (st == MPC_E_CUDA || st == MPC_E_NO_DEVICE) return st;
+          if (st == MPC_OK && ctx->last_ms > t1) {
+            const double per_path_ms = (ctx->last_ms - t1) / double(r4.n_paths - r.n_paths);
+            *cell = 1.0 / (per_path_ms * 1e-3);  // paths per second
+            fixed[(size_t(row) * 2 + p) * kCostColumns + col] = std::max(0.0, t1 - per_path_ms * double(r.n_paths));
+          }
+        }
       }
     }
   }
   ctx->cost_rates = rates;
+  ctx->cost_fixed = fixed;
   ctx->last_error.clear();  // messages of the skipped combinations
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return MPC_OK;

@@ -96,6 +96,7 @@ struct mpc_context {
   // Cost-model rates measured on this device by mpc_calibrate_cost, units
   // per second as [row][fp32, fp64][sampler column]; empty until then.
   std::vector<double> cost_rates;
+  std::vector<double> cost_fixed;  // calibrated per-call intercepts in ms, same layout (terminal GBM row)
   // At most this many blocks per LSM launch (0 = the device's co-resident
   // capacity): set by a device-loop server that keeps only some SMs free.
   uint32_t lsm_block_cap = 0;

@@ -247,10 +247,12 @@ def test_edge_sizes_match_oracle(backend, workload, kw, sampling, n_paths, n_ste
     assert math.isfinite(a.price) and a.n_samples == n_paths
 
 
-@pytest.mark.parametrize("n_paths,n_steps", [(1, 2), (5, 3), (513, 2), (513, 3)])
+@pytest.mark.parametrize("n_paths,n_steps", [(1, 2), (5, 3), (513, 2), (513, 3), (5000, 7), (70001, 9)])
 def test_lsm_edge_sizes_match_oracle(backend, n_paths, n_steps):
     """American put with one path (no regression can run), a handful of
-    paths and the fewest dates, FP64 against the oracle."""
+    paths and the fewest dates, FP64 against the oracle; the last two cases
+    give threads up to four paths with odd step counts, so the stream jump
+    between a thread's paths starts them on odd normal indices too."""
 
     r = req("american_put", n_paths=n_paths, n_steps=n_steps, seed=17, r=0.06, basis_degree=3,
             precision="fp64_plain")

@@ -8,6 +8,9 @@
 * The terminal GBM method, the ``Auto`` default of ``price_european_call``
   (cpu.rs:3191-3226, 6360-6406): FP64 per path to 1e-11, FP32 prices within
   the FP32-path tolerance of the other tests.
+* Fused FP32 pseudorandom units whose stream start comes from the per-tile
+  jump between a thread's units (eight units per thread, chunk edges inside
+  tiles): per-path payoffs against the oracle's FP64 on the same streams.
 * MLQMC scramble replicates (cpu.rs:3663-3751): FP64 against the oracle.
 * The parameter sweep (cpu.rs:3028-3096) through the mapping ABI.
 * The headline pair at full size against the oracle itself.
@@ -33,6 +36,21 @@ def req(workload, **kw):
 
 
 MERTON = dict(model="merton", jump_intensity=0.5, jump_mean=-0.1, jump_volatility=0.15)
+
+
+# ---------------------------------------------- fused pseudorandom jumps --
+@pytest.mark.parametrize("workload,kw", [
+    ("european_call", dict()),                                   # terminal (the Auto default): one normal per path
+    ("european_call", dict(method="stepwise", n_steps=37)),      # an odd number of normals per path
+    ("european_call", dict(model="heston", n_steps=16, kappa=2.0, vol_of_vol=0.5, rho=-0.7)),
+    ("arithmetic_asian_call", dict(n_steps=24, technique="antithetic")),
+])
+@pytest.mark.parametrize("threads", [1, 8])
+def test_fused_pseudorandom_stream_jumps(backend, workload, kw, threads):
+    base = dict(kw, n_paths=150_001, seed=11, n_threads=threads, sampling="pseudorandom", paths_per_thread=8)
+    _, ref = O.price_paths(req(workload, **base, precision="fp64_plain"))
+    got = backend.price_paths(req(workload, **base, precision="fp32_path"))
+    assert np.allclose(got, ref, rtol=1e-3, atol=2e-3), np.max(np.abs(got - ref))
 
 
 # ---------------------------------------------------------------- Merton --
