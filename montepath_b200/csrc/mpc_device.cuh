@@ -60,6 +60,12 @@ struct XorshiftStream {
     double v = (double)raw * (1.0 / 9007199254740992.0);
     return fmax(v, 2.2250738585072014e-308);
   }
+  // The same uniform rounded to FP32: (float)((double)(raw >> 11) * 2^-53)
+  // is one rounding of the 53-bit integer, which the direct conversion does
+  // too (the scale is an exact power of two; raw = 0 gives 0 either way).
+  __device__ __forceinline__ float next_open01_f32() {
+    return __ull2float_rn(next_u64() >> 11) * 1.1102230246251565e-16f;
+  }
   // Box-Muller in FP64 (cpu.rs:2992-3006): returns cos branch, caches sin branch.
   __device__ __forceinline__ double normal_f64() {
     if (has_cached) {
@@ -87,8 +93,8 @@ struct XorshiftStream {
     // square root) and the hardware sine and cosine of 2 pi (u2 - 1/2) in
     // [-pi, pi], where their documented error is 2^-21.4 absolute:
     // sin / cos (2 pi u2) = -sin / -cos (2 pi (u2 - 1/2)).
-    const float u1 = (float)next_open01();
-    const float u2 = (float)next_open01();
+    const float u1 = next_open01_f32();
+    const float u2 = next_open01_f32();
     float radius;
     asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(radius) : "f"(neg2_log_fast(u1)));
     float s, c;

@@ -253,7 +253,7 @@ struct Source<SMP_XORSHIFT> {
   __device__ __forceinline__ float n32(uint32_t) { return st.normal_f32(); }
   __device__ __forceinline__ double n64(uint32_t) { return st.normal_f64(); }
   __device__ __forceinline__ double u64(uint32_t) { return st.next_open01(); }
-  __device__ __forceinline__ float u32(uint32_t) { return (float)st.next_open01(); }
+  __device__ __forceinline__ float u32(uint32_t) { return st.next_open01_f32(); }
 };
 
 // ------------------------------------------------ fused FP32 sources ---
