@@ -1064,6 +1064,7 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
     std::vector<uint32_t> sched;
     std::vector<double> disc_pow;
     std::vector<uint64_t> stride_tab;  // pseudorandom sampler: nibble table of the per-thread path stride jump
+    std::vector<uint8_t> blob;         // host copy of the job's schedule, discount powers and stride table
     bool normalised;
     uint32_t degree, blocks;
     int fp64, sampler;
@@ -1162,22 +1163,20 @@ int run_lsm_batch(mpc_context* ctx, const std::vector<const mpc_request_t*>& req
       LsmArgs& a = j.args;
       a.paths = base + o;
       o += align(a.n_paths * a.n_steps * elem);
-      a.sched = reinterpret_cast<const uint32_t*>(base + o);
-      MPC_CUDA(ctx, cudaMemcpyAsync(base + o, j.sched.data(), j.sched.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
-      h2d += j.sched.size() * 4;
-      o += align(j.sched.size() * 4);
-      a.disc_pow = reinterpret_cast<const double*>(base + o);
-      MPC_CUDA(ctx, cudaMemcpyAsync(base + o, j.disc_pow.data(), j.disc_pow.size() * 8, cudaMemcpyHostToDevice,
-                                    ctx->stream));
-      h2d += j.disc_pow.size() * 8;
-      o += align(j.disc_pow.size() * 8);
-      a.stride_jump = nullptr;
-      if (!j.stride_tab.empty()) {
-        a.stride_jump = reinterpret_cast<const uint64_t*>(base + o);
-        MPC_CUDA(ctx, cudaMemcpyAsync(base + o, j.stride_tab.data(), 256 * 8, cudaMemcpyHostToDevice, ctx->stream));
-        h2d += 256 * 8;
+      {  // schedule | discount powers | stream stride table: one host-to-device copy
+        const size_t sched_b = align(j.sched.size() * 4), disc_b = align(j.disc_pow.size() * 8);
+        std::vector<uint8_t> blob(sched_b + disc_b + 256 * 8, 0);
+        std::memcpy(blob.data(), j.sched.data(), j.sched.size() * 4);
+        std::memcpy(blob.data() + sched_b, j.disc_pow.data(), j.disc_pow.size() * 8);
+        if (!j.stride_tab.empty()) std::memcpy(blob.data() + sched_b + disc_b, j.stride_tab.data(), 256 * 8);
+        a.sched = reinterpret_cast<const uint32_t*>(base + o);
+        a.disc_pow = reinterpret_cast<const double*>(base + o + sched_b);
+        a.stride_jump = j.stride_tab.empty() ? nullptr : reinterpret_cast<const uint64_t*>(base + o + sched_b + disc_b);
+        j.blob.swap(blob);  // kept alive until the stream synchronises below
+        MPC_CUDA(ctx, cudaMemcpyAsync(base + o, j.blob.data(), j.blob.size(), cudaMemcpyHostToDevice, ctx->stream));
+        h2d += j.blob.size();
+        o += sched_b + disc_b + align(256 * 8);
       }
-      o += align(256 * 8);
       a.partials = reinterpret_cast<double*>(base + o);
       // one slot row per exercise date, all marked empty (every byte 0xFF)
       MPC_CUDA(ctx, cudaMemsetAsync(a.partials, 0xFF, lsm_rounds(j.sched.size()) * j.blocks * 16 * 8, ctx->stream));
