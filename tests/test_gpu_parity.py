@@ -515,12 +515,15 @@ def test_bump_greeks_fp64_match_oracle(backend, workload, kw):
         assert abs(g.stderr - e.stderr) <= 1e-7 * e.stderr + 1e-12
 
 
+@pytest.mark.parametrize("n_paths", [50_000, 3_000_001])
 @pytest.mark.parametrize("estimator", ["pathwise", "likelihood_ratio"])
-def test_single_pass_greeks_fp64_replay_reference_stream(backend, estimator):
+def test_single_pass_greeks_fp64_replay_reference_stream(backend, estimator, n_paths):
     """european_call_pathwise / likelihood_ratio (cpu.rs:4670-4869): the
-    terminal shocks are normal i of MonteCarloRng(seed), replayed on the device."""
+    terminal shocks are normal i of MonteCarloRng(seed), replayed on the
+    device; at 3,000,001 paths (an odd count) each thread of the grid-stride
+    loop takes about ten paths, odd and even stream positions alike."""
 
-    r = req("european_call", n_paths=50_000, seed=17, precision="fp64_plain")
+    r = req("european_call", n_paths=n_paths, seed=17, precision="fp64_plain")
     got = backend.greeks(r, estimator)
     status, ref = O.greeks(r, abi.GREEK_ESTIMATORS[estimator])
     assert status == 0 and got.n_estimates == ref.n_estimates
