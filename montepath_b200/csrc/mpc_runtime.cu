@@ -14,7 +14,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "mpc_device.cuh"
@@ -1652,37 +1654,39 @@ static void build_icdf_segments(uint32_t* out) {
 
 // Nibble table [q][v] of T^k, T the xorshift64* state transition: entry
 // (q, v) is T^k applied to the nibble value v placed at bit 4q, so a state x
-// jumps k draws with 16 lookups (gf2_apply).  T^k by repeated squaring of
-// the 64 x 64 bit matrix, kept as the images of the basis vectors.
+// jumps k draws with 16 lookups (gf2_apply).  The images of the 64 basis
+// vectors come from the T^(2^b) nibble tables (16 lookups per set bit of k
+// each); tables are kept per k (a request shape needs the same one every
+// call), at most 256 of them.
 std::vector<uint64_t> xorshift_jump_table(uint64_t k) {
-  auto apply = [](const std::vector<uint64_t>& m, uint64_t x) {
-    uint64_t y = 0;
-    for (int i = 0; i < 64; ++i)
-      if ((x >> i) & 1) y ^= m[i];
-    return y;
-  };
-  std::vector<uint64_t> M(64), S(64), N(64);
+  static std::mutex mu;
+  static std::unordered_map<uint64_t, std::vector<uint64_t>> cache;
+  static std::vector<uint64_t> powers;  // [64][16][16]: T^(2^b)
+  std::lock_guard<std::mutex> lock(mu);
+  auto hit = cache.find(k);
+  if (hit != cache.end()) return hit->second;
+  if (powers.empty()) {
+    std::vector<uint32_t> sob;
+    build_tables(sob, powers);
+  }
+  std::vector<uint64_t> cols(64);
   for (int i = 0; i < 64; ++i) {
     uint64_t x = 1ull << i;
-    x ^= x >> 12;
-    x ^= x << 25;
-    x ^= x >> 27;
-    M[i] = x;         // T
-    S[i] = 1ull << i;  // identity
-  }
-  for (; k; k >>= 1) {
-    if (k & 1) {
-      for (int i = 0; i < 64; ++i) N[i] = apply(M, S[i]);  // S <- T^(2^b) S
-      S.swap(N);
+    for (uint64_t kk = k; kk; kk &= kk - 1) {
+      const uint64_t* t = &powers[size_t(__builtin_ctzll(kk)) * 256];
+      uint64_t y = 0;
+      for (int q = 0; q < 16; ++q) y ^= t[q * 16 + ((x >> (4 * q)) & 0xF)];
+      x = y;
     }
-    for (int i = 0; i < 64; ++i) N[i] = apply(M, M[i]);  // M <- M M
-    M.swap(N);
+    cols[i] = x;
   }
   std::vector<uint64_t> tab(256, 0ull);
   for (int q = 0; q < 16; ++q)
     for (int v = 0; v < 16; ++v)
       for (int j = 0; j < 4; ++j)
-        if ((v >> j) & 1) tab[q * 16 + v] ^= S[4 * q + j];
+        if ((v >> j) & 1) tab[q * 16 + v] ^= cols[4 * q + j];
+  if (cache.size() >= 256) cache.clear();
+  cache.emplace(k, tab);
   return tab;
 }
 
