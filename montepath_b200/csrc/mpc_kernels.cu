@@ -2384,7 +2384,8 @@ __device__ __forceinline__ bool lsm_ok(const LsmArgs& a, uint64_t index, uint64_
 // value.  Lane l ends with the warp sum of value brev4(l >> 1) (lanes l and
 // l ^ 1 hold the same bits): 16 double shuffles instead of 80 for 16 separate
 // butterflies, in a fixed order.
-__device__ __forceinline__ double warp_reduce_scatter16(double (&v)[16]) {
+template <class T>
+__device__ __forceinline__ T warp_reduce_scatter16(T (&v)[16]) {
   const uint32_t lane = threadIdx.x & 31u;
 #pragma unroll
   for (int r = 0; r < 4; ++r) {
@@ -2392,8 +2393,8 @@ __device__ __forceinline__ double warp_reduce_scatter16(double (&v)[16]) {
     const bool up = (lane & (uint32_t)o) != 0;
 #pragma unroll
     for (int i = 0; i < c; ++i) {
-      const double send = up ? v[i] : v[i + c];
-      const double keep = up ? v[i + c] : v[i];
+      const T send = up ? v[i] : v[i + c];
+      const T keep = up ? v[i + c] : v[i];
       v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
     }
   }
@@ -2626,8 +2627,9 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
     double m[kLsmMom];
 #pragma unroll
     for (int i = 0; i < kLsmMom; ++i) m[i] = 0.0;
-    // FP32 path: each thread first sums its own <= kLsmMaxP paths in FP32;
-    // FP64 takes over from the thread's sums (warp, block, cross-block)
+    // FP32 path: each thread sums its own <= kLsmMaxP paths in FP32 and the
+    // warp sums them in FP32; FP64 takes over from the warp sums (block,
+    // cross-block)
     float mf[kLsmMom];
 #pragma unroll
     for (int i = 0; i < kLsmMom; ++i) mf[i] = 0.0f;
@@ -2670,18 +2672,23 @@ __global__ void __launch_bounds__(kLsmBlock, 1) lsm_kernel(const LsmArgs* __rest
         m[14] += 1.0;
       }
     }
-    if constexpr (sizeof(Real) == 4) {
-#pragma unroll
-      for (int i = 0; i < kLsmMom; ++i) m[i] = (double)mf[i];
-    }
-    // block reduction of the 15 moments: warp sums by reduce-scatter, then
-    // one thread per moment folds the warps in order
+    // block reduction of the 15 moments: warp sums by reduce-scatter (the
+    // FP32 path reduces the thread sums in FP32 across the warp, and FP64
+    // takes over from the warp sums), then a fixed tree folds the warps
     const uint64_t part_at = ((uint64_t)round * nb + lb) * 16;
     {
-      double mv[16];
+      double w;
+      if constexpr (sizeof(Real) == 4) {
+        float mv[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) mv[i] = i < kLsmMom ? m[i] : 0.0;
-      const double w = warp_reduce_scatter16(mv);
+        for (int i = 0; i < 16; ++i) mv[i] = i < kLsmMom ? mf[i] : 0.0f;
+        w = (double)warp_reduce_scatter16(mv);
+      } else {
+        double mv[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) mv[i] = i < kLsmMom ? m[i] : 0.0;
+        w = warp_reduce_scatter16(mv);
+      }
       const uint32_t lane = threadIdx.x & 31u;
       if ((lane & 1u) == 0) s_red15[threadIdx.x >> 5][reduce_scatter16_index(lane)] = w;
     }
