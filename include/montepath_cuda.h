@@ -345,7 +345,9 @@ int mpc_estimate_cost_ctx(mpc_context_t* ctx, const mpc_request_t* req, mpc_cost
 /* Measures this device's rates for the cost model: one request of 1,048,576
  * paths x 64 steps (1 step for terminal workloads) per model row, sampler
  * column (pseudorandom, counter hash, scrambled Sobol, Halton) and
- * precision, priced twice, the second call's device time kept.  Replaces the
+ * precision, priced twice, the second call's device time kept (the terminal
+ * GBM row is priced at 4,194,304 paths too, which separates a per-call
+ * intercept from its per-path rate).  Replaces the
  * single-B200 table that cuda.rs:121-152's estimate would otherwise read;
  * combinations the backend does not run, or past the context's byte budget,
  * keep the built-in rate.  `seconds` (optional) receives the wall time it
