@@ -604,7 +604,12 @@ Shape choose_shape(mpc_context* ctx, const Prepared& p) {
   s.block = block;
   int occ = std::max(1, fused_max_blocks_per_sm(p.family, p.sampler, int(block)));
   uint64_t resident = uint64_t(ctx->sm_count) * occ * block;
-  uint64_t want = p.q.n_units / std::max<uint64_t>(resident * 4, 1);
+  // About four tiles per resident thread, except for the pseudorandom
+  // stream, whose later units in a thread's tile start by one table jump
+  // instead of a full seek: there fewer, longer tiles pay (1,048,576 GBM
+  // paths x 64 steps: 0.244 ms at 1 unit per thread and tile, 0.172 ms at 4)
+  const uint64_t tiles_per_thread = p.sampler == SMP_XORSHIFT ? 1 : 4;
+  uint64_t want = p.q.n_units / std::max<uint64_t>(resident * tiles_per_thread, 1);
   uint32_t ppt = 1;
   while (ppt < 8 && uint64_t(ppt) * 2 <= want) ppt *= 2;
   s.ppt = ppt;
@@ -1764,10 +1769,10 @@ enum CostRow : int {
   ROW_COUNT
 };
 const RateRow kRates[ROW_COUNT] = {
-    {{2.24e11, 3.25e11, 3.85e11, 9.05e10}, {1.31e11, 1.35e11, 5.96e10, 5.38e10}},  // GBM stepwise
-    {{2.12e11, 2.93e11, 3.50e11, 8.84e10}, {1.12e11, 1.16e11, 5.59e10, 5.02e10}},  // arithmetic Asian
-    {{8.7e10, 1.83e10, 1.53e10, 1.11e10}, {7.38e9, 2.45e10, 1.98e10, 1.12e10}},    // GBM terminal (pseudorandom FP32: + kTerminalFixedMs)
-    {{1.45e11, 1.93e11, 2.23e11, 5.37e10}, {7.09e10, 6.85e10, 3.02e10, 3.14e10}},  // Heston
+    {{3.72e11, 3.25e11, 3.85e11, 9.05e10}, {1.31e11, 1.35e11, 5.96e10, 5.38e10}},  // GBM stepwise
+    {{3.48e11, 2.93e11, 3.50e11, 8.84e10}, {1.12e11, 1.16e11, 5.59e10, 5.02e10}},  // arithmetic Asian
+    {{5.4e10, 1.83e10, 1.53e10, 1.11e10}, {7.38e9, 2.45e10, 1.98e10, 1.12e10}},    // GBM terminal (pseudorandom FP32: + kTerminalFixedMs)
+    {{2.51e11, 1.93e11, 2.23e11, 5.37e10}, {7.09e10, 6.85e10, 3.02e10, 3.14e10}},  // Heston
     {{1.05e11, 1.05e11, 1.97e11, 4.30e10}, {4.16e10, 4.16e10, 2.65e10, 2.63e10}},  // Merton stepwise
     {{1.70e10, 1.70e10, 1.44e10, 7.09e9}, {1.83e10, 1.83e10, 1.30e10, 6.60e9}},    // Merton terminal
     {{5.46e9, 1.53e10, 1.28e10, 7.74e9}, {5.49e9, 1.58e10, 1.13e10, 6.77e9}},      // 2-asset basket
@@ -1777,8 +1782,8 @@ const RateRow kRates[ROW_COUNT] = {
 // full stream seek and its later paths one table jump each, so the time has
 // an intercept (about one full seek per resident thread, scaled down for
 // requests with fewer paths than resident threads) beside the per-path
-// rate (fit to 2,097,152 and 4,194,304 paths on a B200: 0.157 and 0.180 ms).
-const double kTerminalFixedMs = 0.134;
+// rate (fit to 2,097,152 and 4,194,304 paths on a B200: 0.082 and 0.119 ms).
+const double kTerminalFixedMs = 0.046;
 const double kLsmFixedMs = 0.22, kLsmRate = 1.7e11; // 49 cross-block date rounds, then path-steps
                                                       // (fit to 524,288 paths x 50 dates, FP32: 0.37 ms)
 const double kCallOverheadMs = 0.035;               // events, copies, one launch
